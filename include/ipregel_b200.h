@@ -1,0 +1,168 @@
+/*
+ * ipregel_b200.h -- C ABI of libipregel_b200.so, the type-independent runtime
+ * under the drop-in iPregel headers (include/iPregel.h).
+ *
+ * The reference is a header-only C library: every ip_* function is compiled
+ * into the user's program, and the graph loader, vertex storage and the
+ * OpenMP superstep loop live in its headers.  Here the typed part (the user's
+ * ip_compute / ip_combine inlined into sm_100a kernels, and the superstep
+ * loop of each version) stays in headers compiled by nvcc with the
+ * application, while everything that does not depend on the user's types sits
+ * behind this C ABI: graph loading and device-resident CSR/CSC, seeded graph
+ * generators, frontier compaction, bitmap reductions and error reporting.
+ *
+ * Every function returns 0 on success or a negative IPG_E* code; the message
+ * is available from ipg_last_error().  No function exits the process: the
+ * drop-in header layer turns errors into the reference's print-and-exit(-1)
+ * behaviour (src/iPregel_postamble.h:117-174).  Pointers named d_* are device
+ * pointers; "stream" is a cudaStream_t passed as void*.
+ */
+#ifndef IPREGEL_B200_RUNTIME_H
+#define IPREGEL_B200_RUNTIME_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IPG_ABI_VERSION 1
+
+enum ipg_status {
+    IPG_OK = 0,
+    IPG_EINVAL = -1,     /* bad argument */
+    IPG_ENOMEM = -2,     /* host or device allocation failed */
+    IPG_EIO = -3,        /* file missing, short or malformed */
+    IPG_ECUDA = -4,      /* CUDA runtime error */
+    IPG_EDEVICE = -5,    /* a kernel reported an error word */
+    IPG_EBUDGET = -6     /* request exceeds the configured HBM budget */
+};
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ipg_last_error(void);
+int ipg_abi_version(void);
+/* Name and HBM capacity of the current device; 0 when a device is usable. */
+int ipg_device_info(char* name, size_t name_len, uint64_t* hbm_bytes, int* sm_count);
+
+/* Device memory accounting.  Every device allocation of the runtime and of
+ * the engine state goes through ipg_dev_alloc, which refuses (IPG_EBUDGET)
+ * any request that would take the bytes held above the budget (0 = no
+ * budget; the IPG_HBM_BUDGET environment variable sets it at first use). */
+int ipg_dev_alloc(void** d_ptr, uint64_t bytes);
+int ipg_dev_free(void* d_ptr, uint64_t bytes);
+int ipg_set_hbm_budget(uint64_t bytes);
+uint64_t ipg_hbm_in_use(void);
+/* Page-locked host buffers, for host<->device copies at full link speed. */
+int ipg_host_alloc(void** ptr, uint64_t bytes);
+int ipg_host_free(void* ptr);
+
+/* ------------------------------------------------------------------------
+ * Graphs.  A graph is the reference loader's CSR (src/iPregel_postamble.h:
+ * 244-421) made resident on the device: row[V+1] (u64, row[V] = E), adj[E]
+ * (id_bytes each) and optional weights.  For directed graphs whose in-lists
+ * are needed, the in-CSR (CSC) is built on the device in the order of the
+ * reference's mirror loop (iPregel_postamble.h:429-487): each in-list sorted
+ * by source vertex, ties in edge order.  For undirected graphs the in-lists
+ * alias the rows, as in the reference (iPregel_postamble.h:368-372).
+ * ------------------------------------------------------------------------ */
+typedef struct ipg_graph ipg_graph;
+
+typedef struct ipg_graph_view {
+    uint64_t V;
+    uint64_t E;
+    int id_bytes;            /* 4 or 8 */
+    int weight_bytes;        /* 0 when unweighted, else 1, 2, 4 or 8 */
+    int directed;
+    int has_in;              /* in_* are valid */
+    const uint64_t* d_row;   /* V+1 */
+    const void* d_adj;       /* E ids */
+    const void* d_wgt;       /* E weights or NULL */
+    const uint64_t* d_in_row;
+    const void* d_in_adj;
+    const void* d_in_wgt;
+    uint64_t max_out_degree;
+    uint64_t max_in_degree;
+    uint64_t device_bytes;   /* HBM held by the graph */
+} ipg_graph_view;
+
+/* Replaces ip_load_graph (src/iPregel_postamble.h:508-546): reads
+ * <path>.config ("V E"), <path>.idx (V x idx_bytes row starts, no trailing E),
+ * <path>.adj (E x id_bytes) and, when weighted, <path>.wgt (E x weight_bytes,
+ * an extension: the reference never loads weights). */
+int ipg_graph_load(const char* path, int id_bytes, int idx_bytes, int directed,
+                   int weighted, int weight_bytes, int need_in, ipg_graph** out);
+
+/* Same, from host buffers laid out as the files are (idx without trailing E). */
+int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int idx_bytes,
+                        const void* adj, int id_bytes, const void* wgt,
+                        int weight_bytes, int directed, int need_in,
+                        ipg_graph** out);
+
+/* Wraps device buffers (row with V+1 entries) without copying; the caller
+ * keeps them alive until ipg_graph_free. */
+int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_row,
+                          const void* d_adj, int id_bytes, const void* d_wgt,
+                          int weight_bytes, int directed, int need_in,
+                          ipg_graph** out);
+
+/* Seeded generators on the device (counter-based SplitMix64, self-loops and
+ * duplicates removed, vertex ids not permuted).  R-MAT: 2^scale vertices,
+ * edge_factor * 2^scale sampled edges with quadrant probabilities a, b, c,
+ * 1-a-b-c.  Erdos-Renyi: n vertices, m sampled edges.  undirected adds every
+ * reverse edge.  wmax > 0 attaches u32 weights in [1, wmax], symmetric in
+ * (u, v).  The CPU oracle produces the identical CSR for the same arguments. */
+int ipg_graph_generate_rmat(uint32_t scale, uint32_t edge_factor, double a,
+                            double b, double c, uint64_t seed, int undirected,
+                            uint32_t wmax, int need_in, ipg_graph** out);
+int ipg_graph_generate_er(uint64_t n, uint64_t m, uint64_t seed, int undirected,
+                          uint32_t wmax, int need_in, ipg_graph** out);
+
+int ipg_graph_view_get(const ipg_graph* g, ipg_graph_view* view);
+/* Builds the in-CSR if it is missing (no-op for undirected graphs). */
+int ipg_graph_build_in(ipg_graph* g);
+/* Copies the CSR back to host buffers in the file layout (idx: V x u64). */
+int ipg_graph_to_host(const ipg_graph* g, uint64_t* idx, void* adj, void* wgt);
+/* Writes <path>.config/.idx/.adj(/.wgt) in the reference loader's format. */
+int ipg_graph_write(const ipg_graph* g, const char* path);
+void ipg_graph_free(ipg_graph* g);
+
+/* Static degree classes of all vertices (cached on the graph): list k holds
+ * the vertices whose (in- or out-) degree d satisfies d <= t0 (k=0),
+ * t0 < d <= t1 (k=1), d > t1 (k=2), each sorted by id.  Used by the
+ * all-vertex gather of the single-broadcast version. */
+typedef struct ipg_bins {
+    const uint32_t* d_list[3];
+    uint64_t count[3];
+    uint64_t t0, t1;
+} ipg_bins;
+int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1,
+                   ipg_bins* bins);
+
+/* ------------------------------------------------------------------------
+ * Frontier primitives (stream-ordered, no host synchronisation, safe to
+ * capture in a CUDA graph).
+ * ------------------------------------------------------------------------ */
+
+/* Compacts the set bits of d_bitmap (NULL = all of [0, V)) into up to three
+ * degree-class lists, as ipg_graph_bins does, appending at d_counts[k]
+ * (u32, device, not reset here).  d_row gives degrees (NULL puts every vertex
+ * in list 0).  d_edges (nullable, u64, device) accumulates the sum of degrees.
+ * clear != 0 zeroes the bitmap words it read. */
+int ipg_compact(uint32_t* d_bitmap, uint64_t V, const uint64_t* d_row,
+                uint64_t t0, uint64_t t1, uint32_t* d_list0, uint32_t* d_list1,
+                uint32_t* d_list2, uint32_t* d_counts, uint64_t* d_edges,
+                int clear, void* stream);
+
+/* d_out (u64, device) += popcount(a | b) over nwords words (b nullable). */
+int ipg_bitmap_popc_or(const uint32_t* d_a, const uint32_t* d_b, uint64_t nwords,
+                       uint64_t* d_out, void* stream);
+
+/* SM count of the current device (cached). */
+int ipg_sm_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IPREGEL_B200_RUNTIME_H */

@@ -1,0 +1,956 @@
+/*
+ * engine.cuh -- the typed superstep engine: sm_100a kernels instantiated with
+ * the application's IP_* types, its ip_compute and its ip_combine.
+ *
+ * Versions (selected as in src/iPregel_preamble.h:319-331):
+ *   combiner (push)                src/combiner_postamble.h:123-199
+ *   single_broadcast (pull)        src/combiner_single_broadcast_postamble.h:125-259
+ *   spread (frontier push)         src/combiner_spread_postamble.h:160-431
+ *   spread + single_broadcast      src/combiner_spread_single_broadcast_postamble.h:145-399
+ *
+ * Device layout (structure of arrays, all resident in HBM):
+ *   value[V]                       IP_VALUE_TYPE
+ *   CSR row[V+1] (u64), adj[E]     the loader's layout; in-CSR for pulls
+ *   active / has_message           bitmaps (combiner, written by warp ballot)
+ *                                  or bytes (pulls, written by any thread)
+ *   mailbox[2][V]                  push: combined message of the superstep,
+ *                                  double-buffered by superstep parity
+ *   received[2]                    push: bitmap of mailboxes that got mail
+ *   outbox[V] + broadcaster bitmap push: ip_broadcast records here; delivery
+ *                                  is a separate edge-parallel kernel
+ *   bval[V] + has_bcast bitmap     pull: the externalised broadcast slot of
+ *                                  combiner_single_broadcast_preamble.h:42-50
+ * Messages become visible only at the next superstep in every version
+ * (combiner_postamble.h:168-183), so recording broadcasts in an outbox and
+ * delivering them after the compute kernel gives the reference's results;
+ * ip_combine is associative and commutative by contract
+ * (iPregel_preamble.h:256-262), so combining in a different order is allowed.
+ */
+#ifndef IPREGEL_B200_ENGINE_CUH
+#define IPREGEL_B200_ENGINE_CUH
+
+#include <cuda_runtime.h>
+
+#include <limits>
+#include <type_traits>
+
+typedef IP_VERTEX_ID_TYPE ipx_vid;
+typedef IP_MESSAGE_TYPE ipx_msg;
+typedef IP_VALUE_TYPE ipx_val;
+
+#ifdef IP_NEEDS_OUT_NEIGHBOUR_WEIGHTS
+#define IPX_OUT_WEIGHTS 1
+#else
+#define IPX_OUT_WEIGHTS 0
+#endif
+#ifdef IP_NEEDS_IN_NEIGHBOUR_WEIGHTS
+#define IPX_IN_WEIGHTS 1
+#else
+#define IPX_IN_WEIGHTS 0
+#endif
+#if IPX_OUT_WEIGHTS || IPX_IN_WEIGHTS
+typedef IP_EDGE_WEIGHT_TYPE ipx_wgt;
+#define IPX_WEIGHT_BYTES ((int)sizeof(IP_EDGE_WEIGHT_TYPE))
+#else
+typedef unsigned int ipx_wgt;
+#define IPX_WEIGHT_BYTES 0
+#endif
+
+/* Weighted broadcast (extension, no reference counterpart): an application
+ * that defines IP_BROADCAST_EDGE_MESSAGE(m, w) before including iPregel.h
+ * makes ip_broadcast deliver IP_BROADCAST_EDGE_MESSAGE(m, weight) along each
+ * out-edge (e.g. m + w for SSSP).  The transform must distribute over
+ * ip_combine, because two broadcasts of one vertex in one superstep are
+ * combined before delivery. */
+#ifdef IP_BROADCAST_EDGE_MESSAGE
+#define IPX_EDGE_MSG 1
+#if !IPX_OUT_WEIGHTS
+#error "IP_BROADCAST_EDGE_MESSAGE needs IP_NEEDS_OUT_NEIGHBOUR_WEIGHTS"
+#endif
+#if IPX_PULL
+#error "IP_BROADCAST_EDGE_MESSAGE applies to the combiner and spread versions"
+#endif
+#else
+#define IPX_EDGE_MSG 0
+#endif
+
+static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at most 8 bytes");
+
+#define IPX_FULL 0xffffffffu
+#define IPX_THREADS 256
+#define IPX_ERR_SEND_IN_BROADCAST 1u
+#define IPX_ERR_COMBINE_HINT 2u
+
+/* Degree-class thresholds for the thread / warp / block kernels. */
+#ifndef IPX_T0
+#define IPX_T0 16
+#endif
+#ifndef IPX_T1
+#define IPX_T1 4096
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Mailbox policies: how a push delivers a message into mailbox[w].          */
+/* deliver() returns true when this call filled an empty mailbox (so the     */
+/* caller sets the received bit once per vertex); kFirstKnown = false means  */
+/* the policy cannot tell and the caller tests the bit itself.               */
+/* ------------------------------------------------------------------------ */
+template <class T>
+struct ipx_word {
+    typedef typename std::conditional<(sizeof(T) <= 4), unsigned int, unsigned long long>::type type;
+};
+
+template <class T>
+__device__ __forceinline__ typename ipx_word<T>::type ipx_to_word(const T& x)
+{
+    typename ipx_word<T>::type w = 0;
+    memcpy(&w, &x, sizeof(T));
+    return w;
+}
+
+template <class T>
+__device__ __forceinline__ T ipx_from_word(typename ipx_word<T>::type w)
+{
+    T x;
+    memcpy(&x, &w, sizeof(T));
+    return x;
+}
+
+template <class T>
+__device__ __forceinline__ T ipx_shfl_down(T x, int o)
+{
+    typedef typename ipx_word<T>::type W;
+    W w = ipx_to_word(x);
+    w = __shfl_down_sync(IPX_FULL, w, o);
+    return ipx_from_word<T>(w);
+}
+
+/* Read-modify-write by compare-and-swap on the message's bits, for operand
+ * types without a hardware atomic of the operator. */
+template <class T, class Op>
+__device__ __forceinline__ void ipx_atomic_cas_op(T* a, T v, Op op)
+{
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "combiner hints need a 4- or 8-byte message type");
+    typedef typename std::conditional<sizeof(T) == 4, unsigned int, unsigned long long>::type W;
+    W* p = reinterpret_cast<W*>(a);
+    W old = *p;
+    for (;;) {
+        T cur;
+        memcpy(&cur, &old, sizeof(T));
+        T nv = op(cur, v);
+        W nw;
+        memcpy(&nw, &nv, sizeof(T));
+        if (nw == old) return;
+        W prev = atomicCAS(p, old, nw);
+        if (prev == old) return;
+        old = prev;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void ipx_atomic_min(T* a, T v)
+{
+    if constexpr (std::is_unsigned<T>::value && sizeof(T) == 4) atomicMin((unsigned int*)a, (unsigned int)v);
+    else if constexpr (std::is_unsigned<T>::value && sizeof(T) == 8) atomicMin((unsigned long long*)a, (unsigned long long)v);
+    else if constexpr (std::is_signed<T>::value && std::is_integral<T>::value && sizeof(T) == 4) atomicMin((int*)a, (int)v);
+    else if constexpr (std::is_signed<T>::value && std::is_integral<T>::value && sizeof(T) == 8) atomicMin((long long*)a, (long long)v);
+    else ipx_atomic_cas_op(a, v, [](T x, T y) { return y < x ? y : x; });
+}
+
+template <class T>
+__device__ __forceinline__ void ipx_atomic_max(T* a, T v)
+{
+    if constexpr (std::is_unsigned<T>::value && sizeof(T) == 4) atomicMax((unsigned int*)a, (unsigned int)v);
+    else if constexpr (std::is_unsigned<T>::value && sizeof(T) == 8) atomicMax((unsigned long long*)a, (unsigned long long)v);
+    else if constexpr (std::is_signed<T>::value && std::is_integral<T>::value && sizeof(T) == 4) atomicMax((int*)a, (int)v);
+    else if constexpr (std::is_signed<T>::value && std::is_integral<T>::value && sizeof(T) == 8) atomicMax((long long*)a, (long long)v);
+    else ipx_atomic_cas_op(a, v, [](T x, T y) { return y > x ? y : x; });
+}
+
+template <class T>
+__device__ __forceinline__ void ipx_atomic_add(T* a, T v)
+{
+    if constexpr (std::is_same<T, double>::value || std::is_same<T, float>::value) atomicAdd(a, v);
+    else if constexpr (std::is_integral<T>::value && sizeof(T) == 4) atomicAdd((unsigned int*)a, (unsigned int)v);
+    else if constexpr (std::is_integral<T>::value && sizeof(T) == 8) atomicAdd((unsigned long long*)a, (unsigned long long)v);
+    else ipx_atomic_cas_op(a, v, [](T x, T y) { return x + y; });
+}
+
+/* 128-bit compare-and-swap (sm_90+ atom.cas.b128) for the generic 8-byte path. */
+struct __align__(16) ipx_slot128 {
+    unsigned long long flag;
+    unsigned long long bits;
+};
+
+__device__ __forceinline__ void ipx_cas128(ipx_slot128* addr, unsigned long long cmp_f, unsigned long long cmp_b,
+                                           unsigned long long new_f, unsigned long long new_b,
+                                           unsigned long long& old_f, unsigned long long& old_b)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .b128 c, n, o;\n\t"
+        "mov.b128 c, {%2, %3};\n\t"
+        "mov.b128 n, {%4, %5};\n\t"
+        "atom.global.cas.b128 o, [%6], c, n;\n\t"
+        "mov.b128 {%0, %1}, o;\n\t"
+        "}"
+        : "=l"(old_f), "=l"(old_b)
+        : "l"(cmp_f), "l"(cmp_b), "l"(new_f), "l"(new_b), "l"(addr)
+        : "memory");
+}
+
+template <int KIND, int MSGBYTES>
+struct ipx_mailbox;
+
+/* Hardware min on a packed word: the high half is 0 for a message and the
+ * empty mailbox is all ones, so a delivered UINT_MAX is still "received", and
+ * the atomic's old value tells which sender was first. */
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 4> {
+    typedef unsigned long long slot;
+    static constexpr bool kFirstKnown = true;
+    static constexpr bool kNeedsRMWCheck = true;
+    __device__ static slot empty() { return ~0ULL; }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        const unsigned long long w = (unsigned long long)ipx_to_word(m);
+        if constexpr (std::is_signed<ipx_msg>::value) {
+            // signed order: bias into unsigned order
+            const unsigned long long b = (unsigned long long)(ipx_to_word(m) ^ 0x80000000u);
+            if (b >= __ldcg(s)) return false;
+            return atomicMin(s, b) == ~0ULL;
+        } else {
+            if (w >= __ldcg(s)) return false;
+            return atomicMin(s, w) == ~0ULL;
+        }
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        unsigned long long w = *s;
+        *s = ~0ULL;
+        unsigned int b = (unsigned int)w;
+        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
+        return ipx_from_word<ipx_msg>(b);
+    }
+};
+
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 4> {
+    typedef unsigned long long slot;
+    static constexpr bool kFirstKnown = true;
+    __device__ static slot empty() { return 0ULL; }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        unsigned int b = ipx_to_word(m);
+        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
+        const unsigned long long w = (1ULL << 32) | b;
+        if (w <= __ldcg(s)) return false;
+        return atomicMax(s, w) == 0ULL;
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        unsigned long long w = *s;
+        *s = 0ULL;
+        unsigned int b = (unsigned int)w;
+        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
+        return ipx_from_word<ipx_msg>(b);
+    }
+};
+
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 8> {
+    typedef ipx_msg slot;
+    static constexpr bool kFirstKnown = false;
+    __device__ static slot empty() { return std::numeric_limits<ipx_msg>::max(); }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        if (m < __ldcg(s)) ipx_atomic_min(s, m);
+        return false;
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        ipx_msg m = *s;
+        *s = empty();
+        return m;
+    }
+};
+
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 8> {
+    typedef ipx_msg slot;
+    static constexpr bool kFirstKnown = false;
+    __device__ static slot empty() { return std::numeric_limits<ipx_msg>::lowest(); }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        if (m > __ldcg(s)) ipx_atomic_max(s, m);
+        return false;
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        ipx_msg m = *s;
+        *s = empty();
+        return m;
+    }
+};
+
+template <int MSGBYTES>
+struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
+    typedef ipx_msg slot;
+    static constexpr bool kFirstKnown = false;
+    __device__ static slot empty() { return (ipx_msg)0; }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        ipx_atomic_add(s, m);
+        return false;
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        ipx_msg m = *s;
+        *s = (ipx_msg)0;
+        return m;
+    }
+};
+
+/* Generic, up to 4 bytes: {flag, bits} in one 64-bit word, CAS loop around
+ * the user's ip_combine with the early exit of ip_cas (combiner_postamble.h:
+ * 41-52): no write when combining leaves the mailbox unchanged. */
+template <int MSGBYTES>
+struct ipx_mailbox_generic32 {
+    typedef unsigned long long slot;
+    static constexpr bool kFirstKnown = true;
+    __device__ static slot empty() { return 0ULL; }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        unsigned long long old = __ldcg(s);
+        for (;;) {
+            unsigned long long nw;
+            if (old >> 32) {
+                ipx_msg cur = ipx_from_word<ipx_msg>((unsigned int)old);
+                ipx_msg nv = cur;
+                ip_combine(&nv, m);
+                unsigned int nb = ipx_to_word(nv);
+                if (nb == (unsigned int)old) return false;
+                nw = (1ULL << 32) | nb;
+            } else {
+                nw = (1ULL << 32) | ipx_to_word(m);
+            }
+            unsigned long long prev = atomicCAS(s, old, nw);
+            if (prev == old) return (old >> 32) == 0;
+            old = prev;
+        }
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        unsigned long long w = *s;
+        *s = 0ULL;
+        return ipx_from_word<ipx_msg>((unsigned int)w);
+    }
+};
+
+template <>
+struct ipx_mailbox<IP_COMBINE_GENERIC, 1> : ipx_mailbox_generic32<1> {};
+template <>
+struct ipx_mailbox<IP_COMBINE_GENERIC, 2> : ipx_mailbox_generic32<2> {};
+template <>
+struct ipx_mailbox<IP_COMBINE_GENERIC, 4> : ipx_mailbox_generic32<4> {};
+
+/* Generic, 8 bytes: {flag, bits} in a 16-byte slot with a 128-bit CAS. */
+template <>
+struct ipx_mailbox<IP_COMBINE_GENERIC, 8> {
+    typedef ipx_slot128 slot;
+    static constexpr bool kFirstKnown = true;
+    __device__ static slot empty() { return slot{0ULL, 0ULL}; }
+    __device__ static bool deliver(slot* s, ipx_msg m)
+    {
+        unsigned long long of = __ldcg(&s->flag), ob = __ldcg(&s->bits);
+        for (;;) {
+            unsigned long long nb;
+            if (of) {
+                ipx_msg cur = ipx_from_word<ipx_msg>(ob);
+                ipx_msg nv = cur;
+                ip_combine(&nv, m);
+                nb = ipx_to_word(nv);
+                if (nb == ob) return false;
+            } else {
+                nb = ipx_to_word(m);
+            }
+            unsigned long long pf, pb;
+            ipx_cas128(s, of, ob, 1ULL, nb, pf, pb);
+            if (pf == of && pb == ob) return of == 0;
+            of = pf;
+            ob = pb;
+        }
+    }
+    __device__ static ipx_msg take(slot* s)
+    {
+        slot w = *s;
+        *s = slot{0ULL, 0ULL};
+        return ipx_from_word<ipx_msg>(w.bits);
+    }
+};
+
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 1> : ipx_mailbox_generic32<1> {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 2> : ipx_mailbox_generic32<2> {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 1> : ipx_mailbox_generic32<1> {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 2> : ipx_mailbox_generic32<2> {};
+
+typedef ipx_mailbox<IP_COMBINE_KIND, (int)sizeof(ipx_msg)> ipx_mb;
+typedef typename ipx_mb::slot ipx_slot;
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident engine state, read through the constant bank.            */
+/* ------------------------------------------------------------------------ */
+struct ipx_consts {
+    uint64_t V, E, W;  /* W = bitmap words */
+    const uint64_t* row;
+    const ipx_vid* adj;
+    const ipx_wgt* wgt;
+    const uint64_t* in_row;
+    const ipx_vid* in_adj;
+    const ipx_wgt* in_wgt;
+    ipx_val* value;
+    /* combiner */
+    uint32_t* active_bm;
+    uint32_t* hasmsg_bm;
+    /* pulls */
+    uint8_t* active_b;
+    uint8_t* hasmsg_b;
+    ipx_msg* msg;
+    /* push mail */
+    ipx_slot* mbox[2];
+    uint32_t* recv[2];
+    ipx_msg* outbox;
+    uint32_t* bcaster;
+    /* pull broadcast slots */
+    ipx_msg* bval;
+    uint32_t* has_b;
+    uint32_t* bt;
+    /* counters: [0..3] active counts ring, [4] edges, [5] error word */
+    unsigned long long* ctr;
+    uint32_t* err;
+};
+
+__constant__ ipx_consts ipx_c;
+
+#define IPX_CTR_EDGES 4
+
+__device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+__device__ __forceinline__ bool ipx_test(const uint32_t* bm, uint64_t v) { return (bm[v >> 5] >> (v & 31)) & 1u; }
+
+/* Sets bit v of a shared bitmap; lanes that hit the same word combine first. */
+__device__ __forceinline__ void ipx_set_bit_agg(uint32_t* bm, uint64_t v)
+{
+    const unsigned act = __activemask();
+    const unsigned long long word = v >> 5;
+    const unsigned peers = __match_any_sync(act, word);
+    const unsigned bits = __reduce_or_sync(peers, 1u << (v & 31));
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicOr(&bm[word], bits);
+}
+
+/* Sets bit v if it is clear; returns nothing (idempotent). */
+__device__ __forceinline__ void ipx_mark(uint32_t* bm, uint64_t v)
+{
+    const uint32_t bit = 1u << (v & 31);
+    if (!(__ldcg(&bm[v >> 5]) & bit)) atomicOr(&bm[v >> 5], bit);
+}
+
+/* Warp + block sum into a global counter (all threads of the block call). */
+__device__ __forceinline__ void ipx_block_count(unsigned long long c, unsigned long long* dst)
+{
+    __shared__ unsigned long long s_part[IPX_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(IPX_FULL, c, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < IPX_THREADS / 32; w++) t += s_part[w];
+        if (t) atomicAdd(dst, t);
+    }
+}
+
+/* Delivery of one message into mailbox parity p of vertex w. */
+__device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
+{
+    const bool first = ipx_mb::deliver(&ipx_c.mbox[p][w], m);
+    if constexpr (ipx_mb::kFirstKnown) {
+        if (first) atomicOr(&ipx_c.recv[p][w >> 5], 1u << (w & 31));
+    } else {
+        ipx_mark(ipx_c.recv[p], w);
+    }
+}
+
+/* ---- the vertex functions that depend on the version ---- */
+__device__ inline void ip_broadcast(struct ip_vertex_t* v, IP_MESSAGE_TYPE message)
+{
+#if IPX_PULL
+    /* single_broadcast: write the vertex's own slot (combiner_single_broadcast_
+     * postamble.h:51-55); spread+single_broadcast also flags the out-neighbours
+     * as targets (combiner_spread_single_broadcast_postamble.h:64-76), which the
+     * engine does after the compute kernel. */
+    v->ipx_has_out = true;
+    v->ipx_out = message;
+#else
+    /* combiner / spread: every out-neighbour receives the message
+     * (combiner_postamble.h:81-87); two broadcasts in one call are combined. */
+    if (v->ipx_has_out) {
+        ip_combine(&v->ipx_out, message);
+    } else {
+        v->ipx_has_out = true;
+        v->ipx_out = message;
+    }
+#endif
+}
+
+__device__ inline void ip_send_message(IP_VERTEX_ID_TYPE id, IP_MESSAGE_TYPE message)
+{
+#if IPX_PULL
+    /* Fatal in the single-broadcast versions (combiner_single_broadcast_
+     * postamble.h:42-49): flagged here, reported and exited on the host. */
+    (void)id;
+    (void)message;
+    atomicOr(ipx_c.err, IPX_ERR_SEND_IN_BROADCAST);
+#else
+    ipx_deliver((int)(ip_get_superstep() & 1), (uint64_t)id, message);
+#endif
+}
+
+__device__ inline void ip_vote_to_halt(struct ip_vertex_t* v)
+{
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    v->active = false;
+#else
+    (void)v; /* spread versions ignore it (combiner_spread_postamble.h:433-436) */
+#endif
+}
+
+/* Fills the neighbour fields of the proxy (loads the compiler drops when
+ * ip_compute does not read them). */
+__device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_t v)
+{
+#if defined(IP_NEEDS_OUT_NEIGHBOUR_IDS) || defined(IP_NEEDS_OUT_NEIGHBOUR_COUNT) || IPX_OUT_WEIGHTS
+    const uint64_t r0 = ipx_c.row[v], r1 = ipx_c.row[v + 1];
+#endif
+#ifdef IP_NEEDS_OUT_NEIGHBOUR_IDS
+    x.out_neighbours = const_cast<ipx_vid*>(ipx_c.adj + r0);
+#endif
+#ifdef IP_NEEDS_OUT_NEIGHBOUR_COUNT
+    x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(r1 - r0);
+#endif
+#if IPX_OUT_WEIGHTS
+    x.out_neighbour_weights = const_cast<ipx_wgt*>(ipx_c.wgt + r0);
+#endif
+#if defined(IP_NEEDS_IN_NEIGHBOUR_IDS) || defined(IP_NEEDS_IN_NEIGHBOUR_COUNT) || IPX_IN_WEIGHTS
+    const uint64_t q0 = ipx_c.in_row[v], q1 = ipx_c.in_row[v + 1];
+#endif
+#ifdef IP_NEEDS_IN_NEIGHBOUR_IDS
+    x.in_neighbours = const_cast<ipx_vid*>(ipx_c.in_adj + q0);
+#endif
+#ifdef IP_NEEDS_IN_NEIGHBOUR_COUNT
+    x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(q1 - q0);
+#endif
+#if IPX_IN_WEIGHTS
+    x.in_neighbour_weights = const_cast<ipx_wgt*>(ipx_c.in_wgt + q0);
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Push delivery over degree-class lists of broadcasters.                   */
+/* MODE 0: a thread per broadcaster; 1: a warp; 2: a block.                 */
+/* ------------------------------------------------------------------------ */
+template <int MODE>
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_push(const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ count, int p)
+{
+    const uint64_t n = *count;
+    const ipx_vid* __restrict__ adj = ipx_c.adj;
+    const uint64_t* __restrict__ row = ipx_c.row;
+    if constexpr (MODE == 0) {
+        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+            const uint64_t u = list[i];
+            const ipx_msg m = ipx_c.outbox[u];
+            const uint64_t e1 = row[u + 1];
+            for (uint64_t e = row[u]; e < e1; e++) {
+#if IPX_EDGE_MSG
+                ipx_deliver(p, (uint64_t)adj[e], IP_BROADCAST_EDGE_MESSAGE(m, ipx_c.wgt[e]));
+#else
+                ipx_deliver(p, (uint64_t)adj[e], m);
+#endif
+            }
+        }
+    } else {
+        const uint64_t lanes = (MODE == 1) ? 32 : IPX_THREADS;
+        const uint64_t lane = (MODE == 1) ? (threadIdx.x & 31) : threadIdx.x;
+        const uint64_t unit = (MODE == 1) ? (ipx_gtid() >> 5) : blockIdx.x;
+        const uint64_t units = (MODE == 1) ? (ipx_gstride() >> 5) : gridDim.x;
+        for (uint64_t i = unit; i < n; i += units) {
+            const uint64_t u = list[i];
+            const ipx_msg m = ipx_c.outbox[u];
+            const uint64_t e1 = row[u + 1];
+            for (uint64_t e = row[u] + lane; e < e1; e += lanes) {
+#if IPX_EDGE_MSG
+                ipx_deliver(p, (uint64_t)adj[e], IP_BROADCAST_EDGE_MESSAGE(m, ipx_c.wgt[e]));
+#else
+                ipx_deliver(p, (uint64_t)adj[e], m);
+#endif
+            }
+        }
+    }
+}
+
+/* Marks the out-neighbours of broadcasters as targets (spread+single_broadcast). */
+template <int MODE>
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_mark(const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ count)
+{
+    const uint64_t n = *count;
+    const ipx_vid* __restrict__ adj = ipx_c.adj;
+    const uint64_t* __restrict__ row = ipx_c.row;
+    const uint64_t lanes = (MODE == 0) ? 1 : (MODE == 1 ? 32 : IPX_THREADS);
+    const uint64_t lane = (MODE == 0) ? 0 : (MODE == 1 ? (threadIdx.x & 31) : threadIdx.x);
+    const uint64_t unit = (MODE == 0) ? ipx_gtid() : (MODE == 1 ? (ipx_gtid() >> 5) : blockIdx.x);
+    const uint64_t units = (MODE == 0) ? ipx_gstride() : (MODE == 1 ? (ipx_gstride() >> 5) : gridDim.x);
+    for (uint64_t i = unit; i < n; i += units) {
+        const uint64_t u = list[i];
+        const uint64_t e1 = row[u + 1];
+        for (uint64_t e = row[u] + lane; e < e1; e += lanes) ipx_mark(ipx_c.bt, (uint64_t)adj[e]);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Pull gather (ip_fetch_broadcast_messages, combiner_single_broadcast_      */
+/* postamble.h:57-89): fold ip_combine over the in-neighbours that           */
+/* broadcast.  MODE 0 folds in adjacency order, as the reference does; the   */
+/* warp and block modes fold lane-strided runs in order and then combine the */
+/* partial results in a tree.                                                */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ void ipx_fold(bool& has, ipx_msg& acc, bool oh, ipx_msg om)
+{
+    if (oh) {
+        if (has) {
+            ip_combine(&acc, om);
+        } else {
+            acc = om;
+            has = true;
+        }
+    }
+}
+
+__device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        bool oh = __shfl_down_sync(IPX_FULL, has, o);
+        ipx_msg om = ipx_shfl_down(acc, o);
+        ipx_fold(has, acc, oh, om);
+    }
+}
+
+/* REACT: reactivate and count (single_broadcast) or not (spread+single_broadcast). */
+template <int MODE, bool REACT>
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_gather(const uint32_t* __restrict__ list,
+                                                            const uint32_t* __restrict__ count_dev,
+                                                            uint64_t count_host, int ctr_slot)
+{
+    const uint64_t n = count_dev ? (uint64_t)*count_dev : count_host;
+    const ipx_vid* __restrict__ adj = ipx_c.in_adj;
+    const uint64_t* __restrict__ row = ipx_c.in_row;
+    const uint32_t* __restrict__ hb = ipx_c.has_b;
+    const ipx_msg* __restrict__ bv = ipx_c.bval;
+    unsigned long long react = 0;
+    if constexpr (MODE == 0) {
+        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            const uint64_t e1 = row[v + 1];
+            for (uint64_t e = row[v]; e < e1; e++) {
+                const uint64_t u = adj[e];
+                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
+            }
+            ipx_c.hasmsg_b[v] = has;
+            if (has) {
+                ipx_c.msg[v] = acc;
+                if constexpr (REACT) {
+                    if (!ipx_c.active_b[v]) {
+                        ipx_c.active_b[v] = 1;
+                        react++;
+                    }
+                }
+            }
+        }
+    } else if constexpr (MODE == 1) {
+        const int lane = threadIdx.x & 31;
+        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            const uint64_t e1 = row[v + 1];
+            for (uint64_t e = row[v] + lane; e < e1; e += 32) {
+                const uint64_t u = adj[e];
+                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
+            }
+            ipx_warp_fold(has, acc);
+            if (lane == 0) {
+                ipx_c.hasmsg_b[v] = has;
+                if (has) {
+                    ipx_c.msg[v] = acc;
+                    if constexpr (REACT) {
+                        if (!ipx_c.active_b[v]) {
+                            ipx_c.active_b[v] = 1;
+                            react++;
+                        }
+                    }
+                }
+            }
+        }
+    } else {
+        __shared__ bool s_has[IPX_THREADS / 32];
+        __shared__ ipx_msg s_acc[IPX_THREADS / 32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (uint64_t i = blockIdx.x; i < n; i += gridDim.x) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            const uint64_t e1 = row[v + 1];
+            for (uint64_t e = row[v] + threadIdx.x; e < e1; e += IPX_THREADS) {
+                const uint64_t u = adj[e];
+                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
+            }
+            ipx_warp_fold(has, acc);
+            if (lane == 0) {
+                s_has[warp] = has;
+                s_acc[warp] = acc;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                has = false;
+                for (int w = 0; w < IPX_THREADS / 32; w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+                ipx_c.hasmsg_b[v] = has;
+                if (has) {
+                    ipx_c.msg[v] = acc;
+                    if constexpr (REACT) {
+                        if (!ipx_c.active_b[v]) {
+                            ipx_c.active_b[v] = 1;
+                            react++;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if constexpr (REACT) ipx_block_count(react, &ipx_c.ctr[ctr_slot]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Compute kernels.                                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Combiner (push): src/combiner_postamble.h:151-183.  One thread per vertex,
+ * warp-aligned so that each warp owns whole bitmap words.  The mailbox swap
+ * of the previous superstep (:168-183) happens here, for the vertex about to
+ * run: a received message becomes the vertex's message and reactivates it. */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner(uint64_t s)
+{
+    const uint64_t V = ipx_c.V;
+    const uint64_t Vp = (V + 31) & ~31ULL;
+    const int pprev = (int)((s + 1) & 1);  /* parity of superstep s-1 */
+    const int lane = threadIdx.x & 31;
+    for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
+        const uint64_t wi = v >> 5;
+        const uint32_t aw = ipx_c.active_bm[wi];
+        const uint32_t hw = ipx_c.hasmsg_bm[wi];
+        const uint32_t rw = s ? ipx_c.recv[pprev][wi] : 0u;
+        if ((aw | hw | rw) == 0u) continue; /* warp-uniform */
+        const uint32_t bit = 1u << lane;
+        bool a = aw & bit, h = hw & bit, out = false;
+        const bool r = rw & bit;
+        if (v < V && (a || h || r)) {
+            struct ip_vertex_t x;
+            x.id = (ipx_vid)v;
+            x.active = true;
+            if (r) {
+                x.has_message = true;
+                x.message = ipx_mb::take(&ipx_c.mbox[pprev][v]);
+            } else {
+                x.has_message = h;
+                if (h) x.message = ipx_c.msg[v];
+            }
+            x.value = ipx_c.value[v];
+            x.ipx_has_out = false;
+            ipx_fill_topology(x, v);
+            ip_compute(&x);
+            ipx_c.value[v] = x.value;
+            a = x.active;
+            h = x.has_message;
+            if (h) ipx_c.msg[v] = x.message;
+            if (x.ipx_has_out) {
+                ipx_c.outbox[v] = x.ipx_out;
+                out = true;
+            }
+        }
+        const uint32_t na = __ballot_sync(IPX_FULL, a), nh = __ballot_sync(IPX_FULL, h);
+        const uint32_t no = __ballot_sync(IPX_FULL, out);
+        if (lane == 0) {
+            if (na != aw) ipx_c.active_bm[wi] = na;
+            if (nh != hw) ipx_c.hasmsg_bm[wi] = nh;
+            if (no) ipx_c.bcaster[wi] = no;
+            if (rw) ipx_c.recv[pprev][wi] = 0u;
+        }
+    }
+}
+
+/* Spread (frontier push): src/combiner_spread_postamble.h:235-272 and the
+ * mailbox update :331-342.  Superstep 0 runs every vertex, later supersteps
+ * the vertices that received mail; a frontier vertex always has a message. */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(uint64_t s, const uint32_t* __restrict__ frontier,
+                                                                    const uint32_t* __restrict__ fcount)
+{
+    const uint64_t n = s ? (uint64_t)*fcount : ipx_c.V;
+    const int pprev = (int)((s + 1) & 1);
+    for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+        const uint64_t v = s ? frontier[i] : i;
+        struct ip_vertex_t x;
+        x.id = (ipx_vid)v;
+        x.active = true;
+        x.has_message = s != 0;
+        if (s) x.message = ipx_mb::take(&ipx_c.mbox[pprev][v]);
+        x.value = ipx_c.value[v];
+        x.ipx_has_out = false;
+        ipx_fill_topology(x, v);
+        ip_compute(&x);
+        ipx_c.value[v] = x.value;
+        if (x.ipx_has_out) {
+            ipx_c.outbox[v] = x.ipx_out;
+            ipx_set_bit_agg(ipx_c.bcaster, v);
+        }
+    }
+}
+
+/* Single broadcast (pull) compute phase: combiner_single_broadcast_postamble.h:
+ * 185-201.  Each warp rewrites whole has_broadcast words, which also clears
+ * last superstep's flags. */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb(uint64_t s, int ctr_slot)
+{
+    (void)s;
+    const uint64_t V = ipx_c.V;
+    const uint64_t Vp = (V + 31) & ~31ULL;
+    const int lane = threadIdx.x & 31;
+    unsigned long long cnt = 0;
+    for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
+        bool a = (v < V) && ipx_c.active_b[v];
+        bool out = false;
+        if (a) {
+            struct ip_vertex_t x;
+            x.id = (ipx_vid)v;
+            x.active = true;
+            x.has_message = ipx_c.hasmsg_b[v];
+            if (x.has_message) x.message = ipx_c.msg[v];
+            x.value = ipx_c.value[v];
+            x.ipx_has_out = false;
+            ipx_fill_topology(x, v);
+            ip_compute(&x);
+            ipx_c.value[v] = x.value;
+            if (!x.active) ipx_c.active_b[v] = 0;
+            a = x.active;
+            if (x.ipx_has_out) {
+                ipx_c.bval[v] = x.ipx_out;
+                out = true;
+            }
+        }
+        const uint32_t ob = __ballot_sync(IPX_FULL, out);
+        const uint32_t ab = __ballot_sync(IPX_FULL, a);
+        if (lane == 0) {
+            ipx_c.has_b[v >> 5] = ob;
+            cnt += __popc(ab);
+        }
+    }
+    ipx_block_count(cnt, &ipx_c.ctr[ctr_slot]);
+}
+
+/* Spread + single broadcast compute phase: combiner_spread_single_broadcast_
+ * postamble.h:228-237, over the targets (all vertices at superstep 0). */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(uint64_t s, const uint32_t* __restrict__ l0,
+                                                                 const uint32_t* __restrict__ l1,
+                                                                 const uint32_t* __restrict__ l2,
+                                                                 const uint32_t* __restrict__ cnt)
+{
+    const uint64_t c0 = s ? cnt[0] : ipx_c.V, c1 = s ? cnt[1] : 0, c2 = s ? cnt[2] : 0;
+    const uint64_t n = c0 + c1 + c2;
+    for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+        const uint64_t v = !s ? i : (i < c0 ? l0[i] : (i < c0 + c1 ? l1[i - c0] : l2[i - c0 - c1]));
+        struct ip_vertex_t x;
+        x.id = (ipx_vid)v;
+        x.active = true;
+        x.has_message = ipx_c.hasmsg_b[v];
+        if (x.has_message) x.message = ipx_c.msg[v];
+        x.value = ipx_c.value[v];
+        x.ipx_has_out = false;
+        ipx_fill_topology(x, v);
+        ip_compute(&x);
+        ipx_c.value[v] = x.value;
+        if (x.ipx_has_out) {
+            ipx_c.bval[v] = x.ipx_out;
+            ipx_set_bit_agg(ipx_c.has_b, v);
+            ipx_set_bit_agg(ipx_c.bcaster, v);
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Initialisation kernels (ip_init_vertex_range of each version).           */
+/* ------------------------------------------------------------------------ */
+__global__ void ipx_k_init_values(uint64_t first, uint64_t last)
+{
+    for (uint64_t v = first + ipx_gtid(); v <= last && v < ipx_c.V; v += ipx_gstride()) {
+        ipx_c.value[v] = ipx_val();
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+        ipx_c.active_b[v] = 1;
+#endif
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
+        ipx_c.mbox[0][v] = ipx_mb::empty();
+        ipx_c.mbox[1][v] = ipx_mb::empty();
+#endif
+    }
+}
+
+__global__ void ipx_k_fill_bits(uint32_t* bm, uint64_t V, uint64_t W)
+{
+    for (uint64_t w = ipx_gtid(); w < W; w += ipx_gstride()) {
+        uint32_t x = IPX_FULL;
+        if (w == W - 1 && (V & 31)) x = (1u << (V & 31)) - 1u;
+        bm[w] = x;
+    }
+}
+
+/* Checks an IP_COMBINE_KIND hint against the user's ip_combine on sample
+ * pairs before the hint is trusted. */
+__global__ void ipx_k_check_hint(int kind)
+{
+    for (uint64_t i = ipx_gtid(); i < 4096; i += ipx_gstride()) {
+        unsigned long long ra = (i * 0x9E3779B97F4A7C15ULL) ^ (i >> 3), rb = (i * 0xC2B2AE3D27D4EB4FULL) + 7;
+        ipx_msg a, b;
+        if constexpr (std::is_floating_point<ipx_msg>::value) {
+            a = (ipx_msg)((double)(ra >> 11) * (1.0 / 9007199254740992.0));
+            b = (ipx_msg)((double)(rb >> 11) * (1.0 / 9007199254740992.0));
+        } else if constexpr (std::is_integral<ipx_msg>::value) {
+            a = (ipx_msg)((i & 1) ? (ra & 0xFFFF) : ra);
+            b = (ipx_msg)((i & 2) ? (rb & 0xFFFF) : rb);
+        } else {
+            return;
+        }
+        ipx_msg c = a;
+        ip_combine(&c, b);
+        ipx_msg e;
+        if (kind == IP_COMBINE_MIN) e = (b < a) ? b : a;
+        else if (kind == IP_COMBINE_MAX) e = (b > a) ? b : a;
+        else e = a + b;
+        if (!(c == e)) atomicOr(ipx_c.err, IPX_ERR_COMBINE_HINT);
+    }
+}
+
+#endif /* IPREGEL_B200_ENGINE_CUH */

@@ -1,0 +1,715 @@
+/*
+ * host.cuh -- host half of the drop-in headers: ip_init / ip_run / ip_dump and
+ * the other host-side functions of the reference's interface
+ * (src/iPregel_postamble.h:43-546 and each version's ip_run), plus the C ABI
+ * that every application library exports (ipg_app_*), used by the Python
+ * package and the benchmark to drive the same code path without files.
+ *
+ * Errors follow the reference: a message on stdout and exit(-1)
+ * (iPregel_postamble.h:117-174).  The ipg_app_* entry points return status
+ * codes instead.
+ */
+#ifndef IPREGEL_B200_HOST_CUH
+#define IPREGEL_B200_HOST_CUH
+
+#include <sys/time.h>
+
+#include <string>
+#include <vector>
+
+#define STRINGIFY(x) STRINGIFY_LITERAL(x)
+#define STRINGIFY_LITERAL(x) #x
+
+#ifdef IPG_APP_SHARED
+/* The application's main, renamed by -Dmain=ipg_app_main, keeps C linkage. */
+extern "C" int ipg_app_main(int argc, char* argv[]);
+#endif
+#ifdef IP_APP_PARAMS
+/* Optional application hook: set a named parameter before ip_run. */
+extern "C" int ip_app_set_param(const char* key, double value);
+#endif
+
+static double ipx_wtime()
+{
+    struct timeval tv;
+    gettimeofday(&tv, NULL);
+    return (double)tv.tv_sec + 1e-6 * (double)tv.tv_usec;
+}
+
+/* ---- engine host state ---- */
+struct ipx_host_state {
+    ipg_graph* g = nullptr;
+    bool own_graph = false;
+    ipg_graph_view gv;
+    ipx_consts c;
+    std::vector<std::pair<void*, uint64_t>> allocs;
+    uint32_t* blist[3] = {nullptr, nullptr, nullptr};  /* broadcaster classes */
+    uint32_t* tlist[3] = {nullptr, nullptr, nullptr};  /* frontier / target classes */
+    uint32_t* lcnt = nullptr;                          /* [0..2] broadcaster, [4..6] targets */
+    unsigned long long* h_ctr = nullptr;               /* pinned mirror of ctr */
+    uint32_t* h_lcnt = nullptr;                        /* pinned mirror of lcnt */
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ipg_bins gbins;                                    /* static in-degree classes (pull) */
+    std::vector<uint64_t> counts;
+    double total_seconds = 0.0;
+    uint64_t edges = 0;
+    bool quiet = false;
+    bool ready = false;
+    bool dirty = false;
+    int grid = 0;
+    std::vector<struct ip_vertex_t> host_vertices;
+    bool host_valid = false;
+    char err[512] = {0};
+};
+static ipx_host_state ipx_h;
+
+static int ipx_fail(int code, const char* msg)
+{
+    snprintf(ipx_h.err, sizeof ipx_h.err, "%s", msg);
+    return code;
+}
+
+#define IPX_CU(call)                                                                   \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            snprintf(ipx_h.err, sizeof ipx_h.err, "%s: %s", #call, cudaGetErrorString(e_)); \
+            return IPG_ECUDA;                                                          \
+        }                                                                              \
+    } while (0)
+
+#define IPX_OK(call)                                                                   \
+    do {                                                                               \
+        int r_ = (call);                                                               \
+        if (r_ != IPG_OK) {                                                            \
+            if (!ipx_h.err[0]) snprintf(ipx_h.err, sizeof ipx_h.err, "%s", ipg_last_error()); \
+            return r_;                                                                 \
+        }                                                                              \
+    } while (0)
+
+template <class T>
+static int ipx_alloc(T** p, uint64_t n)
+{
+    void* d = nullptr;
+    uint64_t bytes = (n ? n : 1) * sizeof(T);
+    int r = ipg_dev_alloc(&d, bytes);
+    if (r != IPG_OK) {
+        snprintf(ipx_h.err, sizeof ipx_h.err, "%s", ipg_last_error());
+        return r;
+    }
+    ipx_h.allocs.push_back({d, bytes});
+    *p = (T*)d;
+    return IPG_OK;
+}
+
+static void ipx_release_state()
+{
+    for (auto& a : ipx_h.allocs) ipg_dev_free(a.first, a.second);
+    ipx_h.allocs.clear();
+    if (ipx_h.h_ctr) cudaFreeHost(ipx_h.h_ctr);
+    if (ipx_h.h_lcnt) cudaFreeHost(ipx_h.h_lcnt);
+    ipx_h.h_ctr = nullptr;
+    ipx_h.h_lcnt = nullptr;
+    if (ipx_h.ev0) cudaEventDestroy(ipx_h.ev0);
+    if (ipx_h.ev1) cudaEventDestroy(ipx_h.ev1);
+    if (ipx_h.st) cudaStreamDestroy(ipx_h.st);
+    ipx_h.ev0 = ipx_h.ev1 = nullptr;
+    ipx_h.st = nullptr;
+    if (ipx_h.g && ipx_h.own_graph) ipg_graph_free(ipx_h.g);
+    ipx_h.g = nullptr;
+    ipx_h.ready = false;
+    ipx_h.host_valid = false;
+    ipx_h.host_vertices.clear();
+    ipx_h.host_vertices.shrink_to_fit();
+}
+
+static uint32_t ipx_grid(int per_sm = 8) { return (uint32_t)(ipg_sm_count() * per_sm); }
+
+/* ip_init_vertex_range (combiner_postamble.h:89-117 and the other versions):
+ * every per-vertex flag back to its initial value. */
+static int ipx_reset_vertex_state()
+{
+    const ipx_consts& c = ipx_h.c;
+    const uint64_t V = c.V, W = c.W;
+    cudaStream_t st = ipx_h.st;
+    if (V) {
+        ipx_k_init_values<<<ipx_grid(), IPX_THREADS, 0, st>>>(0, V - 1);
+        IPX_CU(cudaGetLastError());
+    }
+#if IPX_VERSION == IPX_COMBINER
+    if (W) ipx_k_fill_bits<<<ipx_grid(), IPX_THREADS, 0, st>>>(c.active_bm, V, W);
+    IPX_CU(cudaMemsetAsync(c.hasmsg_bm, 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.recv[0], 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.recv[1], 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
+#elif IPX_VERSION == IPX_SPREAD
+    IPX_CU(cudaMemsetAsync(c.recv[0], 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.recv[1], 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
+#elif IPX_VERSION == IPX_SINGLE_BROADCAST
+    IPX_CU(cudaMemsetAsync(c.hasmsg_b, 0, V + 1, st));
+    IPX_CU(cudaMemsetAsync(c.has_b, 0, W * 4 + 4, st));
+#else
+    IPX_CU(cudaMemsetAsync(c.hasmsg_b, 0, V + 1, st));
+    IPX_CU(cudaMemsetAsync(c.has_b, 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.bt, 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
+#endif
+    IPX_CU(cudaMemsetAsync(c.ctr, 0, 8 * sizeof(unsigned long long), st));
+    IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
+    IPX_CU(cudaStreamSynchronize(st));
+    ip_superstep = 0;
+    ip_active_vertices = V;
+    ipx_h.counts.clear();
+    ipx_h.total_seconds = 0.0;
+    ipx_h.edges = 0;
+    ipx_h.dirty = false;
+    ipx_h.host_valid = false;
+    return IPG_OK;
+}
+
+/* Allocates the version's device state for the attached graph. */
+static int ipx_setup_state()
+{
+    ipx_consts& c = ipx_h.c;
+    memset(&c, 0, sizeof c);
+    const ipg_graph_view& gv = ipx_h.gv;
+    if (gv.id_bytes != (int)sizeof(ipx_vid)) return ipx_fail(IPG_EINVAL, "graph id width differs from IP_VERTEX_ID_TYPE");
+    const uint64_t V = gv.V, W = (V + 31) / 32;
+    c.V = V;
+    c.E = gv.E;
+    c.W = W;
+    c.row = gv.d_row;
+    c.adj = (const ipx_vid*)gv.d_adj;
+    c.wgt = (const ipx_wgt*)gv.d_wgt;
+    c.in_row = gv.has_in ? gv.d_in_row : gv.d_row;
+    c.in_adj = (const ipx_vid*)(gv.has_in ? gv.d_in_adj : gv.d_adj);
+    c.in_wgt = (const ipx_wgt*)(gv.has_in ? gv.d_in_wgt : gv.d_wgt);
+    if (IPX_WEIGHT_BYTES && !gv.d_wgt)
+        return ipx_fail(IPG_EINVAL, "the application needs edge weights: load the graph with weighted = true");
+    if (IPX_WEIGHT_BYTES && gv.weight_bytes != IPX_WEIGHT_BYTES)
+        return ipx_fail(IPG_EINVAL, "graph weight width differs from IP_EDGE_WEIGHT_TYPE");
+    IPX_CU(cudaStreamCreateWithFlags(&ipx_h.st, cudaStreamNonBlocking));
+    IPX_CU(cudaEventCreate(&ipx_h.ev0));
+    IPX_CU(cudaEventCreate(&ipx_h.ev1));
+    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, 8 * sizeof(unsigned long long), cudaHostAllocDefault));
+    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_lcnt, 8 * sizeof(uint32_t), cudaHostAllocDefault));
+    IPX_OK(ipx_alloc(&c.value, V));
+    IPX_OK(ipx_alloc(&c.ctr, 8));
+    c.err = (uint32_t*)(c.ctr + 5);
+    IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
+#if IPX_VERSION == IPX_COMBINER
+    IPX_OK(ipx_alloc(&c.active_bm, W + 1));
+    IPX_OK(ipx_alloc(&c.hasmsg_bm, W + 1));
+    IPX_OK(ipx_alloc(&c.msg, V));
+#endif
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
+    IPX_OK(ipx_alloc(&c.mbox[0], V));
+    IPX_OK(ipx_alloc(&c.mbox[1], V));
+    IPX_OK(ipx_alloc(&c.recv[0], W + 1));
+    IPX_OK(ipx_alloc(&c.recv[1], W + 1));
+    IPX_OK(ipx_alloc(&c.outbox, V));
+    IPX_OK(ipx_alloc(&c.bcaster, W + 1));
+    for (int k = 0; k < 3; k++) IPX_OK(ipx_alloc(&ipx_h.blist[k], V));
+#endif
+#if IPX_VERSION == IPX_SPREAD
+    IPX_OK(ipx_alloc(&ipx_h.tlist[0], V));
+#endif
+#if IPX_PULL
+    IPX_OK(ipx_alloc(&c.hasmsg_b, V + 1));
+    IPX_OK(ipx_alloc(&c.msg, V));
+    IPX_OK(ipx_alloc(&c.bval, V));
+    IPX_OK(ipx_alloc(&c.has_b, W + 1));
+#endif
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    IPX_OK(ipx_alloc(&c.active_b, V + 1));
+    IPX_OK(ipg_graph_bins(ipx_h.g, 1, IPX_T0, IPX_T1, &ipx_h.gbins));
+#endif
+#if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
+    IPX_OK(ipx_alloc(&c.bt, W + 1));
+    IPX_OK(ipx_alloc(&c.bcaster, W + 1));
+    for (int k = 0; k < 3; k++) IPX_OK(ipx_alloc(&ipx_h.blist[k], V));
+    for (int k = 0; k < 3; k++) IPX_OK(ipx_alloc(&ipx_h.tlist[k], V));
+#endif
+    IPX_CU(cudaMemcpyToSymbol(ipx_c, &c, sizeof c));
+    size_t vc = V, ec = gv.E;
+    IPX_CU(cudaMemcpyToSymbol(ipd_vertices_count, &vc, sizeof vc));
+    IPX_CU(cudaMemcpyToSymbol(ipd_edges_count, &ec, sizeof ec));
+#if IP_COMBINE_KIND != IP_COMBINE_GENERIC
+    IPX_CU(cudaMemset(c.err, 0, 4));
+    ipx_k_check_hint<<<16, IPX_THREADS>>>(IP_COMBINE_KIND);
+    IPX_CU(cudaGetLastError());
+    uint32_t herr = 0;
+    IPX_CU(cudaMemcpy(&herr, c.err, 4, cudaMemcpyDeviceToHost));
+    if (herr & IPX_ERR_COMBINE_HINT)
+        return ipx_fail(IPG_EINVAL, "IP_COMBINE_KIND disagrees with ip_combine on sample messages");
+#endif
+    ipx_h.ready = true;
+    return ipx_reset_vertex_state();
+}
+
+static int ipx_attach(ipg_graph* g, bool own)
+{
+    ipx_release_state();
+    ipx_h.err[0] = 0;
+    ipx_h.g = g;
+    ipx_h.own_graph = own;
+    IPX_OK(ipg_graph_view_get(g, &ipx_h.gv));
+    bool need_in = IPX_PULL
+#if defined(IP_NEEDS_IN_NEIGHBOUR_IDS) || defined(IP_NEEDS_IN_NEIGHBOUR_COUNT) || IPX_IN_WEIGHTS
+                   || true
+#endif
+        ;
+    if (need_in && !ipx_h.gv.has_in) {
+        IPX_OK(ipg_graph_build_in(g));
+        IPX_OK(ipg_graph_view_get(g, &ipx_h.gv));
+    }
+    ip_set_vertices_count(ipx_h.gv.V);
+    ip_set_edges_count(ipx_h.gv.E);
+    int r = ipx_setup_state();
+    if (r != IPG_OK) {
+        ipx_h.own_graph = own;
+        ipx_release_state();
+    }
+    return r;
+}
+
+/* ---- superstep loop ---- */
+static int ipx_set_superstep(uint64_t s)
+{
+    size_t v = s;
+    IPX_CU(cudaMemcpyToSymbolAsync(ipd_superstep, &v, sizeof v, 0, cudaMemcpyHostToDevice, ipx_h.st));
+    return IPG_OK;
+}
+
+static int ipx_end_superstep(uint64_t s, uint64_t* count)
+{
+    cudaStream_t st = ipx_h.st;
+    IPX_CU(cudaMemcpyAsync(ipx_h.h_ctr, ipx_h.c.ctr, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    IPX_CU(cudaMemcpyAsync(ipx_h.h_lcnt, ipx_h.lcnt, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    IPX_CU(cudaEventRecord(ipx_h.ev1, st));
+    IPX_CU(cudaEventSynchronize(ipx_h.ev1));
+    IPX_CU(cudaGetLastError());
+    uint32_t err = (uint32_t)(ipx_h.h_ctr[5] & 0xffffffffu);
+    if (err & IPX_ERR_SEND_IN_BROADCAST)
+        return ipx_fail(IPG_EDEVICE,
+                        "The function send_message should not be used in the SINGLE_BROADCAST version; only "
+                        "broadcast() should be called, and once per superstep maximum.");
+    if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    *count = ipx_h.h_ctr[s & 3];
+#elif IPX_VERSION == IPX_SPREAD
+    *count = ipx_h.h_lcnt[4];
+#else
+    *count = (uint64_t)ipx_h.h_lcnt[4] + ipx_h.h_lcnt[5] + ipx_h.h_lcnt[6];
+#endif
+    float ms = 0.f;
+    IPX_CU(cudaEventElapsedTime(&ms, ipx_h.ev0, ipx_h.ev1));
+    double sec = ms * 1e-3;
+    ipx_h.total_seconds += sec;
+    ipx_h.counts.push_back(*count);
+    ip_active_vertices = *count;
+    if (!ipx_h.quiet) {
+        printf("Superstep%zuDuration:%f\n", (size_t)s, sec);
+        printf("Superstep%zuActiveVertexCount:%zu\n", (size_t)s, (size_t)*count);
+    }
+    return IPG_OK;
+}
+
+static int ipx_push_lists(int p)
+{
+    const uint32_t g = ipx_grid();
+    cudaStream_t st = ipx_h.st;
+    ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, p);
+    ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, p);
+    ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, p);
+    IPX_CU(cudaGetLastError());
+    return IPG_OK;
+}
+
+static int ipx_run_impl()
+{
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
+    if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
+    ipx_h.dirty = true;
+    const ipx_consts& c = ipx_h.c;
+    cudaStream_t st = ipx_h.st;
+    const uint32_t g = ipx_grid();
+    const uint64_t V = c.V;
+    uint64_t count = ip_active_vertices;
+    unsigned long long* edges = c.ctr + IPX_CTR_EDGES;
+    (void)V;
+    (void)edges;
+    for (uint64_t s = 0;; s++) {
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+        if (count == 0) break; /* while(ip_active_vertices != 0), combiner_postamble.h:134 */
+#else
+        if (s > 0 && count == 0) break; /* while(first || count > 0), combiner_spread_postamble.h:212 */
+#endif
+        IPX_OK(ipx_set_superstep(s));
+        IPX_CU(cudaEventRecord(ipx_h.ev0, st));
+        IPX_CU(cudaMemsetAsync(c.ctr + (s & 3), 0, sizeof(unsigned long long), st));
+#if IPX_VERSION == IPX_COMBINER
+        ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>(s);
+        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
+        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
+                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
+        IPX_OK(ipx_push_lists((int)(s & 1)));
+        IPX_OK(ipg_bitmap_popc_or(c.active_bm, c.recv[s & 1], c.W, (uint64_t*)(c.ctr + (s & 3)), st));
+#elif IPX_VERSION == IPX_SPREAD
+        ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.lcnt + 4);
+        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
+        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
+                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
+        IPX_OK(ipx_push_lists((int)(s & 1)));
+        IPX_OK(ipg_compact(c.recv[s & 1], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr, nullptr, ipx_h.lcnt + 4,
+                           nullptr, 1, st));
+#elif IPX_VERSION == IPX_SINGLE_BROADCAST
+        {
+            const int slot = (int)(s & 3);
+            ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>(s, slot);
+            const ipg_bins& b = ipx_h.gbins;
+            if (b.count[0]) ipx_k_gather<0, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr, b.count[0], slot);
+            if (b.count[1]) ipx_k_gather<1, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr, b.count[1], slot);
+            if (b.count[2]) ipx_k_gather<2, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr, b.count[2], slot);
+            IPX_CU(cudaGetLastError());
+        }
+#else
+        ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.tlist[1], ipx_h.tlist[2],
+                                                      ipx_h.lcnt + 4);
+        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
+        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
+                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
+        ipx_k_mark<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0);
+        ipx_k_mark<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1);
+        ipx_k_mark<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2);
+        IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0], ipx_h.tlist[1], ipx_h.tlist[2],
+                           ipx_h.lcnt + 4, (uint64_t*)edges, 1, st));
+        ipx_k_gather<0, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0);
+        ipx_k_gather<1, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0);
+        ipx_k_gather<2, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0);
+        IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
+        IPX_CU(cudaGetLastError());
+#endif
+        IPX_OK(ipx_end_superstep(s, &count));
+        ip_superstep = s + 1;
+    }
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    ipx_h.edges = (uint64_t)ip_superstep * c.E;
+#else
+    IPX_CU(cudaMemcpy(&ipx_h.edges, edges, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+#endif
+    if (!ipx_h.quiet) printf("Total time of supersteps: %fs.\n", ipx_h.total_seconds);
+    ipx_h.host_valid = false;
+    return IPG_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The reference's host interface.                                          */
+/* ------------------------------------------------------------------------ */
+static void ipx_die(const char* msg)
+{
+    printf("%s\n", msg);
+    exit(-1);
+}
+
+void ip_increment_superstep() { ip_superstep++; }
+void ip_set_vertices_count(size_t vertices_count) { ip_vertices_count = vertices_count; }
+void ip_set_edges_count(size_t edges_count) { ip_edges_count = edges_count; }
+
+/* Host copies of the vertices, filled from the device on first use. */
+static int ipx_materialise()
+{
+    if (ipx_h.host_valid) return IPG_OK;
+    const uint64_t V = ipx_h.c.V;
+    std::vector<ipx_val> vals(V);
+    std::vector<uint64_t> row(V + 1), in_row(V + 1);
+    if (V) {
+        IPX_CU(cudaMemcpy(vals.data(), ipx_h.c.value, V * sizeof(ipx_val), cudaMemcpyDeviceToHost));
+        IPX_CU(cudaMemcpy(row.data(), ipx_h.c.row, (V + 1) * 8, cudaMemcpyDeviceToHost));
+        IPX_CU(cudaMemcpy(in_row.data(), ipx_h.c.in_row, (V + 1) * 8, cudaMemcpyDeviceToHost));
+    }
+    ipx_h.host_vertices.resize(V);
+    for (uint64_t i = 0; i < V; i++) {
+        struct ip_vertex_t& x = ipx_h.host_vertices[i];
+        memset(&x, 0, sizeof x);
+        x.id = (ipx_vid)i;
+        x.value = vals[i];
+#ifdef IP_NEEDS_OUT_NEIGHBOUR_COUNT
+        x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(row[i + 1] - row[i]);
+#endif
+#ifdef IP_NEEDS_IN_NEIGHBOUR_COUNT
+        x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(in_row[i + 1] - in_row[i]);
+#endif
+    }
+    ip_all_vertices = ipx_h.host_vertices.data();
+    ipx_h.host_valid = true;
+    return IPG_OK;
+}
+
+struct ip_vertex_t* ip_get_vertex_by_location(size_t location)
+{
+    if (ipx_materialise() != IPG_OK) ipx_die(ipx_h.err);
+    return &ip_all_vertices[location];
+}
+
+struct ip_vertex_t* ip_get_vertex_by_id(IP_VERTEX_ID_TYPE id) { return ip_get_vertex_by_location((size_t)id); }
+
+void ip_dump(FILE* f)
+{
+    double t0 = ipx_wtime();
+    if (ipx_materialise() != IPG_OK) ipx_die(ipx_h.err);
+    for (size_t i = 0; i < ip_get_vertices_count(); i++) ip_serialise_vertex(f, &ip_all_vertices[i]);
+    printf("DumpingTime:%f\n", ipx_wtime() - t0);
+}
+
+void* ip_safe_malloc(size_t size_to_malloc)
+{
+    void* ptr = malloc(size_to_malloc);
+    if (ptr == NULL) {
+        printf("Failed to allocate %zu bytes.\n", size_to_malloc);
+        exit(-1);
+    }
+    return ptr;
+}
+
+void* ip_safe_realloc(void* ptr, size_t size_to_realloc)
+{
+    ptr = realloc(ptr, size_to_realloc);
+    if (ptr == NULL) {
+        printf("Failed to reallocate to %zu bytes.\n", size_to_realloc);
+        exit(-1);
+    }
+    return ptr;
+}
+
+void ip_safe_free(void* ptr)
+{
+    if (ptr != NULL) free(ptr);
+}
+
+FILE* ip_safe_fopen(const char* file_path, const char* mode)
+{
+    FILE* f = fopen(file_path, mode);
+    if (f == NULL) {
+        printf("Cannot open the file \"%s\" in mode \"%s\".\n", file_path, mode);
+        exit(-1);
+    }
+    return f;
+}
+
+void ip_safe_fread(void* ptr, size_t size, size_t count, FILE* stream)
+{
+    if (fread(ptr, size, count, stream) != count) {
+        printf("Failed to read %zu elements of %zu bytes each.\n", count, size);
+        exit(-1);
+    }
+}
+
+void ip_safe_fwrite(void* ptr, size_t size, size_t count, FILE* stream)
+{
+    if (fwrite(ptr, size, count, stream) != count) {
+        printf("Failed to write.'\n");
+        exit(-1);
+    }
+}
+
+void ip_init_vertex_range(IP_VERTEX_ID_TYPE first, IP_VERTEX_ID_TYPE last)
+{
+    if (!ipx_h.ready || last < first) return;
+    ipx_k_init_values<<<ipx_grid(), IPX_THREADS, 0, ipx_h.st>>>((uint64_t)first, (uint64_t)last);
+    cudaStreamSynchronize(ipx_h.st);
+}
+
+void ip_init_specific()
+{
+    if (ipx_h.ready && ipx_reset_vertex_state() != IPG_OK) ipx_die(ipx_h.err);
+}
+
+void ip_load_graph(const char* file_path, bool directed, bool weighted)
+{
+    double start = ipx_wtime();
+    if (!ipx_h.quiet) {
+        printf("[INFO] The application indicates that the graph must be %sdirected and %sweighted, so the graph "
+               "passed is expected to be so.\n",
+               directed ? "" : "un", weighted ? "" : "un");
+        printf("[INFO] Starting graph loading.\n");
+    }
+    const bool need_in = directed && (IPX_PULL
+#if defined(IP_NEEDS_IN_NEIGHBOUR_IDS) || defined(IP_NEEDS_IN_NEIGHBOUR_COUNT) || IPX_IN_WEIGHTS
+                                      || true
+#endif
+                                     );
+    const int wbytes = IPX_WEIGHT_BYTES ? IPX_WEIGHT_BYTES : 4;
+    ipg_graph* g = nullptr;
+    int r = ipg_graph_load(file_path, (int)sizeof(IP_VERTEX_ID_TYPE), (int)sizeof(IP_NEIGHBOUR_COUNT_TYPE),
+                           directed, weighted, wbytes, need_in, &g);
+    if (r != IPG_OK) ipx_die(ipg_last_error());
+    r = ipx_attach(g, true);
+    if (r != IPG_OK) ipx_die(ipx_h.err);
+    if (!ipx_h.quiet) {
+        printf("\t\t- %zu vertices\n\t\t- %zu edges\n", ip_get_vertices_count(), ip_get_edges_count());
+        printf("LoadingTime:%f\n", ipx_wtime() - start);
+    }
+}
+
+void ip_init(const char* file_path, int number_of_threads, const char* schedule, int chunk_size, bool directed,
+             bool weighted)
+{
+    /* The OpenMP schedule arguments are accepted and checked as in
+     * tmp_extract_runtime_schedule (iPregel_postamble.h:176-193); the GPU
+     * engine has no use for them. */
+    if (strcmp(schedule, "static") == 0) {
+        if (!ipx_h.quiet) printf("Runtime schedule set to static(%d).\n", chunk_size);
+    } else if (strcmp(schedule, "dynamic") == 0) {
+        if (!ipx_h.quiet) printf("Runtime schedule set to dynamic(%d).\n", chunk_size);
+    } else {
+        printf("The schedule %s is unknown.\n", schedule);
+        exit(-1);
+    }
+    double t0 = ipx_wtime();
+    if (!ipx_h.quiet) {
+        char dev[256] = "unknown";
+        uint64_t hbm = 0;
+        int sms = 0;
+        ipg_device_info(dev, sizeof dev, &hbm, &sms);
+        printf("Version:%s\n", VERSION);
+        printf("Software:iPregel-B200\n");
+        printf("FileCommits:%s\n", COMMITS);
+        printf("Application:%s\n", IP_APPLICATION);
+        printf("MpiProcessCount:0\n");
+        printf("Machine:%s\n", IP_MACHINE);
+        printf("Device:%s\n", dev);
+        printf("CompilationFlags:%s\n", STRINGIFY(COMPILATION_FLAGS));
+        time_t t = time(NULL);
+        struct tm tm = *localtime(&t);
+        printf("SubmissionDate:%02d/%02d/%d\n", tm.tm_mday, tm.tm_mon + 1, tm.tm_year + 1900);
+        printf("SubmissionTime:%02d:%02d:%02d\n", tm.tm_hour, tm.tm_min, tm.tm_sec);
+        const char* name = file_path;
+        const char* tmp = strchr(name, '/');
+        while (tmp != NULL) {
+            name = tmp + 1;
+            tmp = strchr(name, '/');
+        }
+        printf("Graph:%s\n", name);
+        printf("OpenmpThreadCount:%d\n", number_of_threads);
+    }
+    ip_thread_count = number_of_threads;
+    ip_load_graph(file_path, directed, weighted);
+    if (!ipx_h.quiet) printf("InitialisationTime:%f\n", ipx_wtime() - t0);
+}
+
+int ip_run()
+{
+    int r = ipx_run_impl();
+    if (r != IPG_OK) ipx_die(ipx_h.err);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* C ABI exported by every application library (no reference counterpart:  */
+/* the reference is compiled into its application; these let a host program */
+/* or a test drive the same engine with in-memory graphs).                  */
+/* ------------------------------------------------------------------------ */
+extern "C" {
+
+int ipg_app_abi_version(void) { return IPG_ABI_VERSION; }
+
+/* "key=value" pairs describing the instantiated types and version. */
+int ipg_app_describe(char* buf, int len)
+{
+    const char* kind = std::is_floating_point<ipx_val>::value ? "f" : (std::is_signed<ipx_val>::value ? "i" : "u");
+    const char* mkind = std::is_floating_point<ipx_msg>::value ? "f" : (std::is_signed<ipx_msg>::value ? "i" : "u");
+    return snprintf(buf, (size_t)len,
+                    "application=%s version=%d id_bytes=%d value_bytes=%d value_kind=%s message_bytes=%d "
+                    "message_kind=%s combine_kind=%d weight_bytes=%d",
+                    IP_APPLICATION, IPX_VERSION, (int)sizeof(ipx_vid), (int)sizeof(ipx_val), kind,
+                    (int)sizeof(ipx_msg), mkind, IP_COMBINE_KIND, IPX_WEIGHT_BYTES);
+}
+
+const char* ipg_app_last_error(void) { return ipx_h.err; }
+
+/* Attaches a resident graph (the caller keeps ownership). */
+int ipg_app_attach(ipg_graph* g)
+{
+    if (!g) return ipx_fail(IPG_EINVAL, "ipg_app_attach: null graph");
+    return ipx_attach(g, false);
+}
+
+/* ip_init from host buffers in the file layout (idx: V row starts, u64). */
+int ipg_app_load_host(uint64_t V, uint64_t E, const uint64_t* idx, const void* adj, const void* wgt, int directed)
+{
+    ipx_h.err[0] = 0;
+    const bool need_in = directed && (IPX_PULL
+#if defined(IP_NEEDS_IN_NEIGHBOUR_IDS) || defined(IP_NEEDS_IN_NEIGHBOUR_COUNT) || IPX_IN_WEIGHTS
+                                      || true
+#endif
+                                     );
+    ipg_graph* g = nullptr;
+    int r = ipg_graph_from_host(V, E, idx, 8, adj, (int)sizeof(ipx_vid), wgt, wgt ? (IPX_WEIGHT_BYTES ? IPX_WEIGHT_BYTES : 4) : 0,
+                                directed, need_in, &g);
+    if (r != IPG_OK) return ipx_fail(r, ipg_last_error());
+    return ipx_attach(g, true);
+}
+
+int ipg_app_run(void) { return ipx_run_impl(); }
+
+int ipg_app_values(void* out, uint64_t cap_bytes)
+{
+    const uint64_t bytes = ipx_h.c.V * sizeof(ipx_val);
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "no graph attached");
+    if (cap_bytes < bytes) return ipx_fail(IPG_EINVAL, "output buffer too small");
+    if (bytes) IPX_CU(cudaMemcpy(out, ipx_h.c.value, bytes, cudaMemcpyDeviceToHost));
+    return IPG_OK;
+}
+
+int ipg_app_values_device(void** ptr)
+{
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "no graph attached");
+    *ptr = ipx_h.c.value;
+    return IPG_OK;
+}
+
+uint64_t ipg_app_supersteps(void) { return ipx_h.counts.size(); }
+
+int ipg_app_counts(uint64_t* out, uint64_t cap)
+{
+    uint64_t n = ipx_h.counts.size();
+    for (uint64_t i = 0; i < n && i < cap; i++) out[i] = ipx_h.counts[i];
+    return (int)n;
+}
+
+int ipg_app_stats(double* seconds, uint64_t* edges, uint64_t* supersteps)
+{
+    if (seconds) *seconds = ipx_h.total_seconds;
+    if (edges) *edges = ipx_h.edges;
+    if (supersteps) *supersteps = ipx_h.counts.size();
+    return IPG_OK;
+}
+
+/* Launch stream of the engine (for callers timing it with their own events). */
+void* ipg_app_stream(void) { return (void*)ipx_h.st; }
+
+int ipg_app_set_quiet(int quiet)
+{
+    ipx_h.quiet = quiet != 0;
+    return IPG_OK;
+}
+
+int ipg_app_set_param(const char* key, double value)
+{
+#ifdef IP_APP_PARAMS
+    return ip_app_set_param(key, value);
+#else
+    (void)key;
+    (void)value;
+    return ipx_fail(IPG_EINVAL, "this application takes no parameters");
+#endif
+}
+
+void ipg_app_release(void) { ipx_release_state(); }
+
+} /* extern "C" */
+
+#endif /* IPREGEL_B200_HOST_CUH */

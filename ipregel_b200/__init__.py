@@ -1,0 +1,400 @@
+"""iPregel-B200: the iPregel superstep engine on an NVIDIA B200 (sm_100a).
+
+Host-side mirror of the reference's interface for Python callers.  The
+reference (a header-only C library) is driven as
+
+    ip_init(path, threads, schedule, chunk, directed, weighted)   # iPregel_preamble.h:298
+    ip_run()                                                      # :309
+    ip_dump(FILE*)                                                # :317
+
+with one application (ip_compute / ip_combine) compiled in, and the version
+chosen at compile time (IP_USE_SPREAD / IP_USE_SINGLE_BROADCAST).  Here each
+(application, version, id width) is a prebuilt library ``lib/app_*.so`` that
+exports the same ip_* functions plus the ``ipg_app_*`` C ABI; ``Engine`` wraps
+one of them, ``Graph`` wraps a device-resident graph of ``libipregel_b200.so``.
+
+There is no CPU path: if the libraries are missing or no GPU is present,
+loading raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+BIN_DIR = os.path.join(HERE, "bin")
+RUNTIME_PATH = os.path.join(LIB_DIR, "libipregel_b200.so")
+
+VERSIONS = ("combiner", "spread", "single_broadcast", "single_broadcast_spread")
+APPS = ("cc", "sssp", "pagerank", "ppr", "sssp_weighted", "sssp_weighted_send")
+
+# Every symbol of include/ipregel_b200.h.
+RUNTIME_SYMBOLS = (
+    "ipg_last_error", "ipg_abi_version", "ipg_device_info", "ipg_dev_alloc", "ipg_dev_free",
+    "ipg_set_hbm_budget", "ipg_hbm_in_use", "ipg_host_alloc", "ipg_host_free", "ipg_graph_load",
+    "ipg_graph_from_host", "ipg_graph_from_device", "ipg_graph_generate_rmat", "ipg_graph_generate_er",
+    "ipg_graph_view_get", "ipg_graph_build_in", "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
+    "ipg_graph_bins", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
+)
+# The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
+# ABI (include/ipregel_b200/host.cuh), exported by every application library.
+APP_SYMBOLS = (
+    "ip_get_superstep", "ip_is_first_superstep", "ip_increment_superstep", "ip_set_vertices_count",
+    "ip_get_vertices_count", "ip_set_edges_count", "ip_get_edges_count", "ip_get_vertex_by_location",
+    "ip_get_vertex_by_id", "ip_init_vertex_range", "ip_load_graph", "ip_safe_malloc", "ip_safe_realloc",
+    "ip_safe_free", "ip_safe_fopen", "ip_safe_fread", "ip_safe_fwrite", "ip_init", "ip_init_specific",
+    "ip_run", "ip_dump", "ip_serialise_vertex",
+    "ipg_app_abi_version", "ipg_app_describe", "ipg_app_last_error", "ipg_app_attach", "ipg_app_load_host",
+    "ipg_app_run", "ipg_app_values", "ipg_app_values_device", "ipg_app_supersteps", "ipg_app_counts",
+    "ipg_app_stats", "ipg_app_stream", "ipg_app_set_quiet", "ipg_app_set_param", "ipg_app_release",
+    "ipg_app_main",
+)
+
+
+class IPregelError(RuntimeError):
+    pass
+
+
+class _View(ctypes.Structure):
+    _fields_ = [("V", ctypes.c_uint64), ("E", ctypes.c_uint64), ("id_bytes", ctypes.c_int),
+                ("weight_bytes", ctypes.c_int), ("directed", ctypes.c_int), ("has_in", ctypes.c_int),
+                ("d_row", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("d_wgt", ctypes.c_void_p),
+                ("d_in_row", ctypes.c_void_p), ("d_in_adj", ctypes.c_void_p), ("d_in_wgt", ctypes.c_void_p),
+                ("max_out_degree", ctypes.c_uint64), ("max_in_degree", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64)]
+
+
+def build():
+    """Compiles the runtime and the application libraries in-tree (nvcc, sm_100a)."""
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}"], check=True)
+
+
+_rt = None
+
+
+def runtime():
+    """Loads libipregel_b200.so (raises if it was not built)."""
+    global _rt
+    if _rt is None:
+        if not os.path.exists(RUNTIME_PATH):
+            raise IPregelError(f"{RUNTIME_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(RUNTIME_PATH)
+        L.ipg_last_error.restype = ctypes.c_char_p
+        L.ipg_hbm_in_use.restype = ctypes.c_uint64
+        vp, u64, i32, dbl = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+        L.ipg_graph_from_host.argtypes = [u64, u64, vp, i32, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_from_device.argtypes = [u64, u64, vp, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_load.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, i32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_generate_rmat.argtypes = [ctypes.c_uint32, ctypes.c_uint32, dbl, dbl, dbl, u64, i32,
+                                              ctypes.c_uint32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_generate_er.argtypes = [u64, u64, u64, i32, ctypes.c_uint32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_view_get.argtypes = [vp, ctypes.POINTER(_View)]
+        L.ipg_graph_build_in.argtypes = [vp]
+        L.ipg_graph_to_host.argtypes = [vp, vp, vp, vp]
+        L.ipg_graph_write.argtypes = [vp, ctypes.c_char_p]
+        L.ipg_graph_free.argtypes = [vp]
+        L.ipg_graph_free.restype = None
+        L.ipg_dev_alloc.argtypes = [ctypes.POINTER(vp), u64]
+        L.ipg_dev_free.argtypes = [vp, u64]
+        L.ipg_host_alloc.argtypes = [ctypes.POINTER(vp), u64]
+        L.ipg_host_free.argtypes = [vp]
+        L.ipg_set_hbm_budget.argtypes = [u64]
+        L.ipg_device_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(u64),
+                                      ctypes.POINTER(ctypes.c_int)]
+        _rt = L
+    return _rt
+
+
+def _check(rc, lib=None, where=""):
+    if rc != 0:
+        msg = (lib or runtime()).ipg_last_error()
+        msg = msg.decode() if isinstance(msg, bytes) else str(msg)
+        raise IPregelError(f"{where} failed ({rc}): {msg}")
+
+
+def device_info():
+    name = ctypes.create_string_buffer(256)
+    hbm = ctypes.c_uint64()
+    sms = ctypes.c_int()
+    _check(runtime().ipg_device_info(name, 256, ctypes.byref(hbm), ctypes.byref(sms)), where="ipg_device_info")
+    return {"name": name.value.decode(), "hbm_bytes": hbm.value, "sm_count": sms.value}
+
+
+def set_hbm_budget(nbytes: int):
+    runtime().ipg_set_hbm_budget(int(nbytes))
+
+
+def hbm_in_use() -> int:
+    return int(runtime().ipg_hbm_in_use())
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (for host<->device copies
+    inside timed regions)."""
+
+    def __init__(self, n, dtype):
+        self.dtype = np.dtype(dtype)
+        self.n = int(n)
+        p = ctypes.c_void_p()
+        _check(runtime().ipg_host_alloc(ctypes.byref(p), max(self.n * self.dtype.itemsize, 16)),
+               where="ipg_host_alloc")
+        self._p = p
+        buf = (ctypes.c_char * max(self.n * self.dtype.itemsize, 16)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=self.n)
+
+    @property
+    def ptr(self):
+        return self._p.value
+
+    def free(self):
+        if self._p is not None and self._p.value:
+            runtime().ipg_host_free(self._p)
+        self._p = None
+        self.array = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A graph resident in HBM (the reference loader's CSR,
+    src/iPregel_postamble.h:244-421, plus the in-CSR when needed)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        self.view = _View()
+        _check(runtime().ipg_graph_view_get(handle, ctypes.byref(self.view)), where="ipg_graph_view_get")
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def V(self):
+        return int(self.view.V)
+
+    @property
+    def E(self):
+        return int(self.view.E)
+
+    def refresh(self):
+        _check(runtime().ipg_graph_view_get(self._h, ctypes.byref(self.view)), where="ipg_graph_view_get")
+
+    @classmethod
+    def from_csr(cls, V, E, idx, adj, wgt=None, directed=False, need_in=False, id_bytes=4):
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        adj = np.ascontiguousarray(adj, dtype=np.uint32 if id_bytes == 4 else np.uint64)
+        if wgt is not None:
+            wgt = np.ascontiguousarray(wgt, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        rc = runtime().ipg_graph_from_host(int(V), int(E), idx.ctypes.data if V else None, 8,
+                                           adj.ctypes.data if E else None, id_bytes,
+                                           wgt.ctypes.data if (wgt is not None and E) else None,
+                                           4 if wgt is not None else 0, int(directed), int(need_in),
+                                           ctypes.byref(h))
+        _check(rc, where="ipg_graph_from_host")
+        return cls(h.value)
+
+    @classmethod
+    def generate_rmat(cls, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, undirected=False, wmax=0,
+                      need_in=False):
+        h = ctypes.c_void_p()
+        _check(runtime().ipg_graph_generate_rmat(scale, edge_factor, a, b, c, seed, int(undirected), wmax,
+                                                 int(need_in), ctypes.byref(h)), where="ipg_graph_generate_rmat")
+        return cls(h.value)
+
+    @classmethod
+    def generate_er(cls, n, m, seed=1, undirected=False, wmax=0, need_in=False):
+        h = ctypes.c_void_p()
+        _check(runtime().ipg_graph_generate_er(n, m, seed, int(undirected), wmax, int(need_in), ctypes.byref(h)),
+               where="ipg_graph_generate_er")
+        return cls(h.value)
+
+    @classmethod
+    def load(cls, path, id_bytes=4, idx_bytes=8, directed=False, weighted=False, weight_bytes=4, need_in=False):
+        h = ctypes.c_void_p()
+        _check(runtime().ipg_graph_load(path.encode(), id_bytes, idx_bytes, int(directed), int(weighted),
+                                        weight_bytes, int(need_in), ctypes.byref(h)), where="ipg_graph_load")
+        return cls(h.value)
+
+    def build_in(self):
+        _check(runtime().ipg_graph_build_in(self._h), where="ipg_graph_build_in")
+        self.refresh()
+
+    def to_host(self):
+        """(idx, adj, wgt) numpy arrays in the file layout."""
+        V, E = self.V, self.E
+        idx = np.zeros(max(V, 1), dtype=np.uint64)
+        adj = np.zeros(max(E, 1), dtype=np.uint32 if self.view.id_bytes == 4 else np.uint64)
+        wgt = np.zeros(max(E, 1), dtype=np.uint32) if self.view.d_wgt else None
+        _check(runtime().ipg_graph_to_host(self._h, idx.ctypes.data, adj.ctypes.data,
+                                           wgt.ctypes.data if wgt is not None else None), where="ipg_graph_to_host")
+        return idx[:V], adj[:E], (wgt[:E] if wgt is not None else None)
+
+    def write(self, path):
+        _check(runtime().ipg_graph_write(self._h, path.encode()), where="ipg_graph_write")
+
+    def free(self):
+        if self._h:
+            runtime().ipg_graph_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+@dataclass
+class RunResult:
+    values: np.ndarray
+    counts: list = field(default_factory=list)   # per-superstep ActiveVertexCount
+    seconds: float = 0.0                         # sum of per-superstep device times
+    edges: int = 0                               # edges traversed by the engine
+    supersteps: int = 0
+
+
+def app_library(app: str, version: str, id_bits: int = 32, generic: bool = False) -> str:
+    prefix = "appgeneric" if generic else "app"
+    return os.path.join(LIB_DIR, f"{prefix}_{app}_{version}_{id_bits}.so")
+
+
+class Engine:
+    """One application compiled in one version: the ip_init / ip_run / ip_dump
+    life cycle of the reference, on in-memory graphs."""
+
+    _loaded = {}
+
+    def __init__(self, app: str, version: str = "combiner", id_bits: int = 32, generic: bool = False):
+        if version not in VERSIONS:
+            raise ValueError(f"unknown version {version!r}; expected one of {VERSIONS}")
+        path = app_library(app, version, id_bits, generic)
+        if not os.path.exists(path):
+            raise IPregelError(f"{path} is missing: build it with `make -C {HERE}`")
+        runtime()
+        if path not in Engine._loaded:
+            L = ctypes.CDLL(path)
+            vp, u64 = ctypes.c_void_p, ctypes.c_uint64
+            L.ipg_app_last_error.restype = ctypes.c_char_p
+            L.ipg_app_attach.argtypes = [vp]
+            L.ipg_app_load_host.argtypes = [u64, u64, vp, vp, vp, ctypes.c_int]
+            L.ipg_app_values.argtypes = [vp, u64]
+            L.ipg_app_values_device.argtypes = [ctypes.POINTER(vp)]
+            L.ipg_app_supersteps.restype = u64
+            L.ipg_app_counts.argtypes = [vp, u64]
+            L.ipg_app_stats.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(u64), ctypes.POINTER(u64)]
+            L.ipg_app_stream.restype = vp
+            L.ipg_app_set_param.argtypes = [ctypes.c_char_p, ctypes.c_double]
+            L.ipg_app_describe.argtypes = [ctypes.c_char_p, ctypes.c_int]
+            L.ipg_app_release.restype = None
+            L.ip_get_vertices_count.restype = ctypes.c_size_t
+            Engine._loaded[path] = L
+        self.lib = Engine._loaded[path]
+        self.app, self.version, self.id_bits = app, version, id_bits
+        self.info = self.describe()
+        self.graph = None
+
+    def describe(self) -> dict:
+        buf = ctypes.create_string_buffer(512)
+        self.lib.ipg_app_describe(buf, 512)
+        return dict(kv.split("=", 1) for kv in buf.value.decode().split())
+
+    def _check(self, rc, where):
+        if rc != 0:
+            raise IPregelError(f"{where} failed ({rc}): {self.lib.ipg_app_last_error().decode()}")
+
+    @property
+    def value_dtype(self):
+        kind, nbytes = self.info["value_kind"], int(self.info["value_bytes"])
+        return np.dtype({"f": "f", "i": "i", "u": "u"}[kind] + str(nbytes))
+
+    def set_quiet(self, quiet=True):
+        self.lib.ipg_app_set_quiet(int(quiet))
+
+    def set_param(self, key, value):
+        self._check(self.lib.ipg_app_set_param(key.encode(), float(value)), f"set_param({key})")
+
+    def attach(self, graph: Graph):
+        self.graph = graph
+        self._check(self.lib.ipg_app_attach(graph.handle), "ipg_app_attach")
+
+    def load_host(self, V, E, idx, adj, wgt=None, directed=False):
+        """ip_init from host buffers (idx = V row starts, u64; adj = ids)."""
+        self.graph = None
+        self._check(self.lib.ipg_app_load_host(int(V), int(E), _ptr(idx), _ptr(adj), _ptr(wgt), int(directed)),
+                    "ipg_app_load_host")
+
+    def run_only(self):
+        self._check(self.lib.ipg_app_run(), "ipg_app_run")
+
+    def vertex_count(self) -> int:
+        return int(self.lib.ip_get_vertices_count())
+
+    def values(self, out=None):
+        """Copies the vertex values to the host (the data ip_dump serialises)."""
+        n = self.vertex_count()
+        if out is None:
+            out = np.zeros(max(n, 1), dtype=self.value_dtype)
+        self._check(self.lib.ipg_app_values(_ptr(out), out.nbytes), "ipg_app_values")
+        return out[:n] if isinstance(out, np.ndarray) else out
+
+    def counts(self):
+        n = int(self.lib.ipg_app_supersteps())
+        buf = np.zeros(max(n, 1), dtype=np.uint64)
+        self.lib.ipg_app_counts(buf.ctypes.data, n)
+        return [int(x) for x in buf[:n]]
+
+    def stats(self):
+        s = ctypes.c_double()
+        e = ctypes.c_uint64()
+        n = ctypes.c_uint64()
+        self.lib.ipg_app_stats(ctypes.byref(s), ctypes.byref(e), ctypes.byref(n))
+        return s.value, int(e.value), int(n.value)
+
+    def stream(self):
+        return self.lib.ipg_app_stream()
+
+    def run(self) -> RunResult:
+        self.run_only()
+        vals = self.values()
+        sec, edges, n = self.stats()
+        return RunResult(vals, self.counts(), sec, edges, n)
+
+    def release(self):
+        self.lib.ipg_app_release()
+        self.graph = None
+
+    def main(self, argv):
+        """Calls the application's own main (ip_init from files, ip_run,
+        ip_dump) in this process."""
+        args = [a.encode() for a in argv]
+        arr = (ctypes.c_char_p * (len(args) + 1))(*args, None)
+        self.lib.ipg_app_main.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+        return self.lib.ipg_app_main(len(args), arr)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, PinnedArray):
+        return a.ptr
+    return a.ctypes.data
+
+
+def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, quiet=True) -> RunResult:
+    """Attach + set params + run, returning values and per-superstep counts."""
+    eng = Engine(app, version, id_bits, generic)
+    eng.set_quiet(quiet)
+    for k, v in (params or {}).items():
+        eng.set_param(k, v)
+    eng.attach(graph)
+    return eng.run()

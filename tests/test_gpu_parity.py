@@ -1,0 +1,153 @@
+"""CUDA engine against the oracle, through the C ABI of the application
+libraries (lib/app_*.so): integer applications bit-exact, FP64 PageRank
+within 1e-12 max abs per vertex, and the same per-superstep
+ActiveVertexCount sequence (the reference's own progress log)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import small_graphs
+
+pytestmark = pytest.mark.gpu
+
+PR_TOL = 1e-12  # max abs difference per vertex, FP64 PageRank / PPR
+
+ALL4 = ("combiner", "spread", "single_broadcast", "single_broadcast_spread")
+CASES = [("cc", v) for v in ALL4] + [("sssp", v) for v in ALL4] + \
+        [("pagerank", "single_broadcast"), ("pagerank", "combiner"), ("pagerank", "spread"),
+         ("ppr", "single_broadcast"), ("ppr", "combiner"),
+         ("sssp_weighted", "combiner"), ("sssp_weighted", "spread"),
+         ("sssp_weighted_send", "combiner"), ("sssp_weighted_send", "spread")]
+
+ORACLE_APP = {"cc": "cc", "sssp": "sssp", "pagerank": "pagerank", "ppr": "ppr",
+              "sssp_weighted": "sssp_weighted", "sssp_weighted_send": "sssp_weighted"}
+
+
+def _gpu_run(app, version, g, directed=False, id_bits=32, generic=False, params=None):
+    import ipregel_b200 as ip
+    wgt = g.wgt if app.startswith("sssp_weighted") else None
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj if id_bits == 32 else g.adj.astype(np.uint64), wgt=wgt,
+                              directed=directed, id_bytes=id_bits // 8)
+    try:
+        return ip.run_app(app, version, graph, id_bits=id_bits, generic=generic, params=params)
+    finally:
+        graph.free()
+
+
+def _compare(app, version, g, directed=False, id_bits=32, generic=False, source=0, rounds=None):
+    params = {}
+    if app in ("sssp", "sssp_weighted", "sssp_weighted_send", "ppr"):
+        params["source"] = source
+    if rounds is not None:
+        params["rounds"] = rounds
+    res = _gpu_run(app, version, g, directed, id_bits, generic, params)
+    kw = dict(source=source, directed=directed, id_bytes=id_bits // 8)
+    if rounds is not None:
+        kw["rounds"] = rounds
+    elif app == "ppr":
+        kw["rounds"] = 20
+    want, counts, _ = O.run(g, ORACLE_APP[app], version, **kw)
+    if app in ("pagerank", "ppr"):
+        assert res.values.shape == want.shape
+        err = np.max(np.abs(res.values - want)) if g.V else 0.0
+        assert err <= PR_TOL, f"max abs error {err}"
+    else:
+        np.testing.assert_array_equal(res.values.astype(np.uint64), want.astype(np.uint64))
+    assert res.counts == [int(c) for c in counts]
+    return res
+
+
+def _weighted(g):
+    return O.add_weights(g, wmax=255, seed=11)
+
+
+@pytest.mark.parametrize("app,version", CASES)
+def test_rmat_undirected(app, version):
+    g = _weighted(O.gen_rmat(12, 16, seed=1, undirected=True))
+    _compare(app, version, g)
+
+
+@pytest.mark.parametrize("app,version", CASES)
+def test_rmat_directed_file(app, version):
+    """Directed R-MAT file loaded with directed = false, as the reference's
+    applications do (in-lists alias the rows)."""
+    g = _weighted(O.gen_rmat(11, 16, seed=4, undirected=False))
+    _compare(app, version, g)
+
+
+@pytest.mark.parametrize("app,version", [("cc", "single_broadcast"), ("sssp", "single_broadcast_spread"),
+                                         ("pagerank", "single_broadcast"), ("cc", "combiner")])
+def test_directed_true_builds_in_lists(app, version):
+    """directed = true: the pull versions gather over the true in-lists, built
+    on the device in the reference's mirror order."""
+    g = O.gen_rmat(10, 16, seed=9, undirected=False)
+    _compare(app, version, g, directed=True)
+
+
+@pytest.mark.parametrize("app,version", CASES)
+def test_small_graphs(app, version):
+    for name, g in small_graphs().items():
+        g = _weighted(g)
+        _compare(app, version, g)
+
+
+@pytest.mark.parametrize("app,version", [("cc", v) for v in ALL4] + [("sssp", v) for v in ALL4])
+def test_64bit_ids(app, version):
+    g = O.gen_rmat(10, 16, seed=2, undirected=True)
+    _compare(app, version, g, id_bits=64)
+
+
+@pytest.mark.parametrize("app,version,bits", [("cc", "combiner", 32), ("cc", "spread", 32),
+                                              ("pagerank", "combiner", 32), ("pagerank", "spread", 32),
+                                              ("sssp", "combiner", 64), ("sssp", "spread", 64)])
+def test_generic_combiner_paths(app, version, bits):
+    """Builds without IP_COMBINE_KIND: delivery runs a CAS loop around the
+    user's ip_combine (packed 64-bit word for 4-byte messages, 128-bit CAS for
+    8-byte messages)."""
+    g = O.gen_rmat(11, 16, seed=6, undirected=True)
+    _compare(app, version, g, id_bits=bits, generic=True)
+
+
+def test_sssp_other_sources():
+    g = _weighted(O.gen_rmat(11, 16, seed=8, undirected=True))
+    for src in (1, 17, 1000, 2047):
+        _compare("sssp", "spread", g, source=src)
+        _compare("sssp_weighted", "combiner", g, source=src)
+
+
+def test_weighted_sssp_equals_dijkstra():
+    g = _weighted(O.gen_rmat(12, 16, seed=12, undirected=True))
+    res = _gpu_run("sssp_weighted", "spread", g, params={"source": 0})
+    np.testing.assert_array_equal(res.values, O.dijkstra(g, 0))
+
+
+def test_pagerank_30_rounds():
+    g = O.gen_rmat(12, 16, seed=1, undirected=False)
+    res = _compare("pagerank", "single_broadcast", g, rounds=30)
+    assert res.supersteps == 31
+
+
+def test_er_graphs():
+    for n in (1024, 5000, 65536):
+        g = _weighted(O.gen_er(n, 8 * n, seed=n, undirected=False))
+        _compare("cc", "spread", g)
+        _compare("sssp_weighted", "spread", g)
+
+
+def test_send_message_in_broadcast_version_is_fatal():
+    """ip_send_message under a single-broadcast version is an error, as in
+    combiner_single_broadcast_postamble.h:42-49: the engine reports it."""
+    import ipregel_b200 as ip
+    g = _weighted(O.gen_rmat(8, 8, seed=1, undirected=True))
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, wgt=g.wgt)
+    eng = ip.Engine("sssp_weighted_send", "single_broadcast")
+    eng.set_quiet()
+    eng.attach(graph)
+    with pytest.raises(ip.IPregelError, match="send_message should not be used"):
+        eng.run()
+    # the context stays usable: the same process runs another engine afterwards
+    eng.release()
+    res = ip.run_app("cc", "combiner", graph)
+    want, _, _ = O.run(g, "cc", "combiner")
+    np.testing.assert_array_equal(res.values, want)
+    graph.free()
