@@ -1,0 +1,388 @@
+#!/usr/bin/env python3
+"""Benchmark of the superstep engine on the CC + SSSP workload at scale.
+
+Workload (one step): on an undirected R-MAT graph of scale 24 (2^24 vertices,
+edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05, seed 1, self-loops and
+duplicates removed, symmetrised, u32 ids, u32 weights uniform in [1, 255]),
+  - min-label connected components with the spread version (app cc), and
+  - single-source shortest paths from vertex 0 with atomicMin delivery
+    (app sssp_weighted, spread version),
+each to quiescence.  Metric: Graph500-style GTEPS = stored edges x runs /
+time.  `value` times the runs with the graph resident in HBM; `e2e` times the
+same through the C ABI with host buffers (graph upload and result download
+inside the timed region).  Inputs are 3.8 GB, larger than the 126 MB L2, so no
+L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (torchrun), every rank runs the same workload on its own GPU
+(replicas: the path does not shard), and value is the sum over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PageRank/CC/SSSP GTEPS + HBM GB/s; served queries/s, p50/p99 vs plain GPU loop"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=int, default=24)
+    p.add_argument("--cpu-scale", type=int, default=22, help="scale of the bounded CPU sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_host_info():
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return os.cpu_count() or 1, model
+
+
+def run_reference_sample(graph_path, E, repeats):
+    """Times the reference's own OpenMP binaries (oracle/_ref) on graph files:
+    cc_spread_32 and sssp_spread_32 (the reference's SSSP counts hops; weights
+    have no reference implementation), all host threads, OMP_PROC_BIND=TRUE,
+    OMP_PLACES=cores, static schedule (submission.slurm:36-42).  Returns
+    (seconds for one CC + one SSSP run, best of `repeats` each, the reference's
+    own "Total time of supersteps")."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads, _ = cpu_host_info()
+    env = {"OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "TRUE", "OMP_PLACES": "cores"}
+    total = 0.0
+    for app in ("cc", "sssp"):
+        best = float("inf")
+        for _ in range(repeats):
+            _, out = O.run_ref(app, "spread", graph_path, threads=threads, schedule="static", chunk=0, env=env,
+                               timeout=1800)
+            best = min(best, O.parse_total_time(out))
+        total += best
+    return total, threads
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "reference binaries (oracle/_ref) were not built"}))
+        return 0
+    import ipregel_b200 as ip
+    scale = args.cpu_scale
+    g = ip.Graph.generate_rmat(scale, 16, seed=1, undirected=True)
+    E = g.E
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, f"rmat{scale}")
+        g.write(path)
+        g.free()
+        for _ in range(args.warmup):
+            run_reference_sample(path, E, 1)
+        secs = []
+        for _ in range(args.steps):
+            t, threads = run_reference_sample(path, E, 1)
+            secs.append(t)
+    cores, model = cpu_host_info()
+    value = 2.0 * E * len(secs) / sum(secs) / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"cc_spread + sssp_spread, undirected R-MAT scale {scale} (bounded CPU sample of "
+                               f"the scale-{args.scale} workload), edge factor 16, seed 1",
+                   "edges_stored": E, "teps": "Graph500: stored edges per run / superstep time"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": f"reference cc_spread_32 + sssp_spread_32 (hop-count SSSP) on R-MAT scale {scale} "
+                                   f"undirected, OMP {cores} threads, 'Total time of supersteps', CPU {model}"},
+        "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    import ipregel_b200 as ip
+
+    scale = args.scale
+    g = ip.Graph.generate_rmat(scale, 16, seed=1, undirected=True, wmax=255)
+    V, E = g.V, g.E
+    cc = ip.Engine("cc", "spread")
+    sp = ip.Engine("sssp_weighted", "spread")
+    for eng in (cc, sp):
+        eng.set_quiet(True)
+    sp.set_param("source", 0)
+    cc.attach(g)
+    sp.attach(g)
+
+    def step():
+        cc.run_only()
+        sp.run_only()
+
+    for _ in range(args.warmup):
+        step()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timed region (per-kernel events on) ----
+    for eng in (cc, sp):
+        eng.set_profile(True)
+        eng.profile_reset()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    edges_traversed = 0
+    supersteps = []
+    for _ in range(args.steps):
+        step()
+        edges_traversed += cc.stats()[1] + sp.stats()[1]
+        supersteps.append((cc.stats()[2], sp.stats()[2]))
+    t1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(t0.elapsed_time(t1))
+    launches = cc.launches() + sp.launches()
+    prof = {}
+    for tag, eng in (("cc", cc), ("sssp", sp)):
+        for k, v in eng.profile().items():
+            prof[f"{tag}:{k}"] = v
+    for eng in (cc, sp):
+        eng.set_profile(False)
+
+    runs = 2 * args.steps
+    value = world * E * runs / (ms * 1e-3) / 1e9
+    traversed_gteps = world * edges_traversed / (ms * 1e-3) / 1e9
+
+    # dominant kernel and its roofline
+    peak, peak_kind = measured_peaks()
+    top = max(prof.items(), key=lambda kv: kv[1]["ms"])
+    top_name, top_rec = top
+    avg_ms = top_rec["ms"] / max(top_rec["timed"], 1)
+    bytes_per_launch = top_rec["bytes"] / max(top_rec["timed"], 1)
+    achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    total_kernel_ms = sum(v["ms"] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "bytes_per_launch": round(bytes_per_launch), "avg_launch_ms": round(avg_ms, 4),
+                "share_of_kernel_time": round(top_rec["ms"] / total_kernel_ms, 3) if total_kernel_ms else None}
+    traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_path):
+        try:
+            tr = json.load(open(traffic_path)).get(top_name.split(":", 1)[1])
+            if tr:
+                roofline["traffic"] = round(tr["dram_bytes_per_algorithmic_byte"] * bytes_per_launch)
+                roofline["traffic_source"] = tr["source"]
+        except Exception:
+            pass
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        idx, adj, wgt = g.to_host()
+        p_idx = ip.PinnedArray(V, np.uint64)
+        p_adj = ip.PinnedArray(E, np.uint32)
+        p_wgt = ip.PinnedArray(E, np.uint32)
+        p_idx.array[:] = idx
+        p_adj.array[:] = adj
+        p_wgt.array[:] = wgt
+        out_cc = ip.PinnedArray(V, np.uint32)
+        out_sp = ip.PinnedArray(V, np.uint32)
+        del idx, adj, wgt
+
+        def e2e_step():
+            g2 = ip.Graph.from_csr(V, E, p_idx.array, p_adj.array, wgt=p_wgt.array)
+            cc.attach(g2)
+            cc.run_only()
+            cc.values(out_cc.array)
+            sp.attach(g2)
+            sp.run_only()
+            sp.values(out_sp.array)
+            g2.free()
+
+        e2e_step()
+        barrier()
+        t0.record()
+        for _ in range(args.steps):
+            e2e_step()
+        t1.record()
+        barrier()
+        ms_e2e = max_over_ranks(t0.elapsed_time(t1))
+        e2e = {"value": round(world * E * runs / (ms_e2e * 1e-3) / 1e9, 4), "unit": "GTEPS",
+               "h2d_bytes_per_step": int(V * 8 + E * 4 + E * 4), "d2h_bytes_per_step": int(2 * V * 4),
+               "ms_per_step": round(ms_e2e / args.steps, 3)}
+        # the results of the last end-to-end step are the results of the workload
+        cc_labels_components = int(len(np.unique(out_cc.array)))
+        reached = int(np.count_nonzero(out_sp.array != 0xFFFFFFFF))
+        for a in (p_idx, p_adj, p_wgt, out_cc, out_sp):
+            a.free()
+    else:
+        cc_labels_components = reached = None
+
+    # ---- CPU baseline: the reference's binaries on a bounded sample ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        cores, model = cpu_host_info()
+        if O.have_ref():
+            gs = ip.Graph.generate_rmat(args.cpu_scale, 16, seed=1, undirected=True)
+            Es = gs.E
+            with tempfile.TemporaryDirectory() as td:
+                path = os.path.join(td, f"rmat{args.cpu_scale}")
+                gs.write(path)
+                gs.free()
+                secs, threads = run_reference_sample(path, Es, 2)
+            cpu = {"value": round(2.0 * Es / secs / 1e9, 4), "unit": "GTEPS", "cores": threads, "kind": "reference",
+                   "sample": f"reference cc_spread_32 + sssp_spread_32 (hop-count SSSP; weighted SSSP has no "
+                             f"reference implementation) on undirected R-MAT scale {args.cpu_scale} "
+                             f"(E={Es}), best of 2, 'Total time of supersteps', CPU {model}"}
+        else:
+            cpu = {"value": None, "unit": "GTEPS", "cores": cores, "kind": "reference",
+                   "sample": "reference binaries not built"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"cc (spread) + weighted sssp from 0 (spread, atomicMin), undirected R-MAT "
+                                   f"scale {scale}, edge factor 16, a/b/c=0.57/0.19/0.19, seed 1, weights U[1,255]",
+                       "vertices": V, "edges_stored": E, "parallelism": f"replicas x{world}",
+                       "teps": "Graph500: stored edges x runs / time",
+                       "l2": "inputs (3.8 GB) larger than L2; no flush",
+                       "traversed_gteps": round(traversed_gteps, 4),
+                       "supersteps_cc_sssp": list(supersteps[0]) if supersteps else None,
+                       "cc_components": cc_labels_components, "sssp_reached": reached},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                            "gbs": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9, 1) if v["ms"] else None}
+                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
+        }
+        print(json.dumps(line))
+    cc.release()
+    sp.release()
+    g.free()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

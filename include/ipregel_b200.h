@@ -134,6 +134,7 @@ void ipg_graph_free(ipg_graph* g);
 typedef struct ipg_bins {
     const uint32_t* d_list[3];
     uint64_t count[3];
+    uint64_t edges[3];       /* degree sum of each class */
     uint64_t t0, t1;
 } ipg_bins;
 int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1,
@@ -147,8 +148,8 @@ int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1,
 /* Compacts the set bits of d_bitmap (NULL = all of [0, V)) into up to three
  * degree-class lists, as ipg_graph_bins does, appending at d_counts[k]
  * (u32, device, not reset here).  d_row gives degrees (NULL puts every vertex
- * in list 0).  d_edges (nullable, u64, device) accumulates the sum of degrees.
- * clear != 0 zeroes the bitmap words it read. */
+ * in list 0).  d_edges (nullable, three u64 on the device) accumulates the
+ * degree sum of each class.  clear != 0 zeroes the bitmap words it read. */
 int ipg_compact(uint32_t* d_bitmap, uint64_t V, const uint64_t* d_row,
                 uint64_t t0, uint64_t t1, uint32_t* d_list0, uint32_t* d_list1,
                 uint32_t* d_list2, uint32_t* d_counts, uint64_t* d_edges,

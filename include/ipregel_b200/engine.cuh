@@ -436,7 +436,32 @@ struct ipx_consts {
 
 __constant__ ipx_consts ipx_c;
 
-#define IPX_CTR_EDGES 4
+/* ctr layout (u64): [0..3] active-count ring, [5] error word (low half),
+ * [8..10] degree sums of the broadcaster classes, [11..13] of the target
+ * classes, both reset every superstep. */
+#define IPX_NCTR 16
+#define IPX_CTR_ERR 5
+
+/* Kernel ids for launch counting and per-kernel profiling. */
+enum {
+    IPX_K_COMPUTE,
+    IPX_K_COMPACT_B,
+    IPX_K_PUSH0,
+    IPX_K_PUSH1,
+    IPX_K_PUSH2,
+    IPX_K_COMPACT_T,
+    IPX_K_GATHER0,
+    IPX_K_GATHER1,
+    IPX_K_GATHER2,
+    IPX_K_MARK0,
+    IPX_K_MARK1,
+    IPX_K_MARK2,
+    IPX_K_COUNT,
+    IPX_K_N
+};
+static const char* const ipx_kname[IPX_K_N] = {
+    "compute", "compact_broadcasters", "push_thread", "push_warp", "push_block", "compact_targets",
+    "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active"};
 
 __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }

@@ -61,6 +61,17 @@ struct ipx_host_state {
     std::vector<struct ip_vertex_t> host_vertices;
     bool host_valid = false;
     char err[512] = {0};
+    /* profiling */
+    bool profile = false;
+    uint64_t prof_launches[IPX_K_N] = {0};
+    uint64_t prof_timed[IPX_K_N] = {0};
+    double prof_ms[IPX_K_N] = {0};
+    double prof_bytes[IPX_K_N] = {0};
+#define IPX_PEV 32
+    cudaEvent_t pev[2][IPX_PEV];
+    int pkid[IPX_PEV];
+    int npev = 0;
+    bool pev_made = false;
 };
 static ipx_host_state ipx_h;
 
@@ -156,7 +167,7 @@ static int ipx_reset_vertex_state()
     IPX_CU(cudaMemsetAsync(c.bt, 0, W * 4 + 4, st));
     IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
 #endif
-    IPX_CU(cudaMemsetAsync(c.ctr, 0, 8 * sizeof(unsigned long long), st));
+    IPX_CU(cudaMemsetAsync(c.ctr, 0, IPX_NCTR * sizeof(unsigned long long), st));
     IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
     IPX_CU(cudaStreamSynchronize(st));
     ip_superstep = 0;
@@ -193,11 +204,11 @@ static int ipx_setup_state()
     IPX_CU(cudaStreamCreateWithFlags(&ipx_h.st, cudaStreamNonBlocking));
     IPX_CU(cudaEventCreate(&ipx_h.ev0));
     IPX_CU(cudaEventCreate(&ipx_h.ev1));
-    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, 8 * sizeof(unsigned long long), cudaHostAllocDefault));
+    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, IPX_NCTR * sizeof(unsigned long long), cudaHostAllocDefault));
     IPX_CU(cudaHostAlloc((void**)&ipx_h.h_lcnt, 8 * sizeof(uint32_t), cudaHostAllocDefault));
     IPX_OK(ipx_alloc(&c.value, V));
-    IPX_OK(ipx_alloc(&c.ctr, 8));
-    c.err = (uint32_t*)(c.ctr + 5);
+    IPX_OK(ipx_alloc(&c.ctr, IPX_NCTR));
+    c.err = (uint32_t*)(c.ctr + IPX_CTR_ERR);
     IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
 #if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.active_bm, W + 1));
@@ -283,15 +294,98 @@ static int ipx_set_superstep(uint64_t s)
     return IPG_OK;
 }
 
-static int ipx_end_superstep(uint64_t s, uint64_t* count)
+static int ipx_push_class(int k, int p, uint32_t g);
+
+/* ---- per-kernel profiling (the role of IP_ENABLE_THREAD_PROFILING in the
+ * reference, e.g. combiner_spread_postamble.h:166-178, :353-401): every
+ * launch is counted; with profiling on, each is bracketed by events and its
+ * algorithmic bytes are added from the sizes read back after the superstep. */
+static void ipx_k_begin(int kid)
+{
+    ipx_h.prof_launches[kid]++;
+    if (ipx_h.profile && ipx_h.npev < IPX_PEV) {
+        cudaEventRecord(ipx_h.pev[0][ipx_h.npev], ipx_h.st);
+        ipx_h.pkid[ipx_h.npev] = kid;
+    }
+}
+
+static void ipx_k_end()
+{
+    if (ipx_h.profile && ipx_h.npev < IPX_PEV) {
+        cudaEventRecord(ipx_h.pev[1][ipx_h.npev], ipx_h.st);
+        ipx_h.npev++;
+    }
+}
+
+#define IPX_LAUNCH(kid, ...)       \
+    do {                           \
+        ipx_k_begin(kid);          \
+        __VA_ARGS__;               \
+        ipx_k_end();               \
+    } while (0)
+
+static int ipx_push_class(int k, int p, uint32_t g)
 {
     cudaStream_t st = ipx_h.st;
-    IPX_CU(cudaMemcpyAsync(ipx_h.h_ctr, ipx_h.c.ctr, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, p));
+    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, p));
+    if (k == 2) IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, p));
+    IPX_CU(cudaGetLastError());
+    return IPG_OK;
+}
+
+/* Algorithmic bytes of the superstep's kernels: the data each must move once
+ * (ids, row offsets, values, messages, mailbox read-modify-writes, bitmap
+ * bits), from the list sizes and degree sums of this superstep. */
+static void ipx_account_bytes(uint64_t s, uint64_t frontier)
+{
+    const double V = (double)ipx_h.c.V;
+    const double ib = sizeof(ipx_vid), vb = sizeof(ipx_val), mb = sizeof(ipx_msg), sb = sizeof(ipx_slot);
+    const double wb = IPX_EDGE_MSG ? (double)IPX_WEIGHT_BYTES : 0.0;
+    const unsigned long long* ctr = ipx_h.h_ctr;
+    const uint32_t* l = ipx_h.h_lcnt;
+    double* B = ipx_h.prof_bytes;
+    (void)s;
+    (void)sb;
+    (void)wb;
+    (void)ctr;
+    (void)l;
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
+    const double nb = (double)l[0] + l[1] + l[2];
+    B[IPX_K_COMPUTE] += (IPX_VERSION == IPX_COMBINER ? V * 3.0 / 8.0 : frontier * 4.0) +
+                        frontier * (2 * vb + sb) + nb * mb;
+    B[IPX_K_COMPACT_B] += V / 8.0 + nb * 20.0;
+    for (int k = 0; k < 3; k++) B[IPX_K_PUSH0 + k] += l[k] * (20.0 + mb) + ctr[8 + k] * (ib + sb + wb);
+#if IPX_VERSION == IPX_COMBINER
+    B[IPX_K_COUNT] += V / 4.0;
+#else
+    B[IPX_K_COMPACT_T] += V / 8.0 + l[4] * 4.0;
+#endif
+#elif IPX_VERSION == IPX_SINGLE_BROADCAST
+    const ipg_bins& b = ipx_h.gbins;
+    B[IPX_K_COMPUTE] += V * 1.0 / 8.0 + frontier * (2 * vb + mb + 2);
+    for (int k = 0; k < 3; k++)
+        B[IPX_K_GATHER0 + k] += b.count[k] * (4.0 + 8.0 + 2.0 + mb) + b.edges[k] * (ib + mb + 0.125);
+#else
+    const double nb = (double)l[0] + l[1] + l[2];
+    B[IPX_K_COMPUTE] += frontier * (4.0 + 2 * vb + 1 + mb) + nb * mb;
+    B[IPX_K_COMPACT_B] += V / 8.0 + nb * 20.0;
+    for (int k = 0; k < 3; k++) B[IPX_K_MARK0 + k] += l[k] * 20.0 + ctr[8 + k] * (ib + 0.125);
+    B[IPX_K_COMPACT_T] += V / 8.0 + ((double)l[4] + l[5] + l[6]) * 20.0;
+    for (int k = 0; k < 3; k++)
+        B[IPX_K_GATHER0 + k] += l[4 + k] * (4.0 + 16.0 + 1.0 + mb) + ctr[11 + k] * (ib + mb + 0.125);
+#endif
+}
+
+static int ipx_end_superstep(uint64_t s, uint64_t* count, uint64_t frontier)
+{
+    cudaStream_t st = ipx_h.st;
+    IPX_CU(cudaMemcpyAsync(ipx_h.h_ctr, ipx_h.c.ctr, IPX_NCTR * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     IPX_CU(cudaMemcpyAsync(ipx_h.h_lcnt, ipx_h.lcnt, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     IPX_CU(cudaEventRecord(ipx_h.ev1, st));
     IPX_CU(cudaEventSynchronize(ipx_h.ev1));
     IPX_CU(cudaGetLastError());
-    uint32_t err = (uint32_t)(ipx_h.h_ctr[5] & 0xffffffffu);
+    uint32_t err = (uint32_t)(ipx_h.h_ctr[IPX_CTR_ERR] & 0xffffffffu);
     if (err & IPX_ERR_SEND_IN_BROADCAST)
         return ipx_fail(IPG_EDEVICE,
                         "The function send_message should not be used in the SINGLE_BROADCAST version; only "
@@ -304,6 +398,21 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count)
 #else
     *count = (uint64_t)ipx_h.h_lcnt[4] + ipx_h.h_lcnt[5] + ipx_h.h_lcnt[6];
 #endif
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    ipx_h.edges += ipx_h.c.E;
+#else
+    for (int k = 8; k < 14; k++) ipx_h.edges += ipx_h.h_ctr[k];
+#endif
+    if (ipx_h.profile) {
+        for (int i = 0; i < ipx_h.npev; i++) {
+            float kms = 0.f;
+            IPX_CU(cudaEventElapsedTime(&kms, ipx_h.pev[0][i], ipx_h.pev[1][i]));
+            ipx_h.prof_ms[ipx_h.pkid[i]] += kms;
+            ipx_h.prof_timed[ipx_h.pkid[i]]++;
+        }
+        ipx_h.npev = 0;
+        ipx_account_bytes(s, frontier);
+    }
     float ms = 0.f;
     IPX_CU(cudaEventElapsedTime(&ms, ipx_h.ev0, ipx_h.ev1));
     double sec = ms * 1e-3;
@@ -317,17 +426,6 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count)
     return IPG_OK;
 }
 
-static int ipx_push_lists(int p)
-{
-    const uint32_t g = ipx_grid();
-    cudaStream_t st = ipx_h.st;
-    ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, p);
-    ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, p);
-    ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, p);
-    IPX_CU(cudaGetLastError());
-    return IPG_OK;
-}
-
 static int ipx_run_impl()
 {
     if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
@@ -338,68 +436,82 @@ static int ipx_run_impl()
     const uint32_t g = ipx_grid();
     const uint64_t V = c.V;
     uint64_t count = ip_active_vertices;
-    unsigned long long* edges = c.ctr + IPX_CTR_EDGES;
+    uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
+    uint64_t* edges_t = (uint64_t*)(c.ctr + 11);
     (void)V;
-    (void)edges;
+    (void)edges_b;
+    (void)edges_t;
+    /* The reference loops until quiescence; a bound (IPG_MAX_SUPERSTEPS,
+     * default 10^6) turns a program that never halts into an error. */
+    const char* lim = getenv("IPG_MAX_SUPERSTEPS");
+    const uint64_t max_supersteps = (lim && *lim) ? strtoull(lim, nullptr, 10) : 1000000ULL;
     for (uint64_t s = 0;; s++) {
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
         if (count == 0) break; /* while(ip_active_vertices != 0), combiner_postamble.h:134 */
 #else
         if (s > 0 && count == 0) break; /* while(first || count > 0), combiner_spread_postamble.h:212 */
 #endif
+        if (s >= max_supersteps) return ipx_fail(IPG_EDEVICE, "superstep limit (IPG_MAX_SUPERSTEPS) reached");
+        /* vertices the compute kernel runs: the frontier (spread versions) or
+         * the active ones of the previous superstep */
+        const uint64_t frontier = (s == 0) ? V : count;
         IPX_OK(ipx_set_superstep(s));
         IPX_CU(cudaEventRecord(ipx_h.ev0, st));
         IPX_CU(cudaMemsetAsync(c.ctr + (s & 3), 0, sizeof(unsigned long long), st));
+        IPX_CU(cudaMemsetAsync(c.ctr + 8, 0, 6 * sizeof(unsigned long long), st));
 #if IPX_VERSION == IPX_COMBINER
-        ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>(s);
+        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>(s));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
-        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
-                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
-        IPX_OK(ipx_push_lists((int)(s & 1)));
-        IPX_OK(ipg_bitmap_popc_or(c.active_bm, c.recv[s & 1], c.W, (uint64_t*)(c.ctr + (s & 3)), st));
+        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
+                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
+        for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, (int)(s & 1), g));
+        IPX_LAUNCH(IPX_K_COUNT,
+                   IPX_OK(ipg_bitmap_popc_or(c.active_bm, c.recv[s & 1], c.W, (uint64_t*)(c.ctr + (s & 3)), st)));
 #elif IPX_VERSION == IPX_SPREAD
-        ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.lcnt + 4);
+        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.lcnt + 4));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
-                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
-        IPX_OK(ipx_push_lists((int)(s & 1)));
-        IPX_OK(ipg_compact(c.recv[s & 1], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr, nullptr, ipx_h.lcnt + 4,
-                           nullptr, 1, st));
+        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
+                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
+        for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, (int)(s & 1), g));
+        IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.recv[s & 1], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr,
+                                                       nullptr, ipx_h.lcnt + 4, nullptr, 1, st)));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
         {
             const int slot = (int)(s & 3);
-            ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>(s, slot);
+            IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>(s, slot));
             const ipg_bins& b = ipx_h.gbins;
-            if (b.count[0]) ipx_k_gather<0, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr, b.count[0], slot);
-            if (b.count[1]) ipx_k_gather<1, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr, b.count[1], slot);
-            if (b.count[2]) ipx_k_gather<2, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr, b.count[2], slot);
+            if (b.count[0])
+                IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr,
+                                                                                            b.count[0], slot));
+            if (b.count[1])
+                IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr,
+                                                                                            b.count[1], slot));
+            if (b.count[2])
+                IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr,
+                                                                                            b.count[2], slot));
             IPX_CU(cudaGetLastError());
         }
 #else
-        ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.tlist[1], ipx_h.tlist[2],
-                                                      ipx_h.lcnt + 4);
+        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.tlist[1],
+                                                                                ipx_h.tlist[2], ipx_h.lcnt + 4));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0], ipx_h.blist[1], ipx_h.blist[2],
-                           ipx_h.lcnt, (uint64_t*)edges, 1, st));
-        ipx_k_mark<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0);
-        ipx_k_mark<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1);
-        ipx_k_mark<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2);
-        IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0], ipx_h.tlist[1], ipx_h.tlist[2],
-                           ipx_h.lcnt + 4, (uint64_t*)edges, 1, st));
-        ipx_k_gather<0, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0);
-        ipx_k_gather<1, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0);
-        ipx_k_gather<2, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0);
+        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
+                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
+        IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0));
+        IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1));
+        IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2));
+        IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0],
+                                                       ipx_h.tlist[1], ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1,
+                                                       st)));
+        IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0));
+        IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0));
+        IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0));
         IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
         IPX_CU(cudaGetLastError());
 #endif
-        IPX_OK(ipx_end_superstep(s, &count));
+        IPX_OK(ipx_end_superstep(s, &count, frontier));
         ip_superstep = s + 1;
     }
-#if IPX_VERSION == IPX_SINGLE_BROADCAST
-    ipx_h.edges = (uint64_t)ip_superstep * c.E;
-#else
-    IPX_CU(cudaMemcpy(&ipx_h.edges, edges, sizeof(uint64_t), cudaMemcpyDeviceToHost));
-#endif
     if (!ipx_h.quiet) printf("Total time of supersteps: %fs.\n", ipx_h.total_seconds);
     ipx_h.host_valid = false;
     return IPG_OK;
@@ -695,6 +807,51 @@ int ipg_app_set_quiet(int quiet)
 {
     ipx_h.quiet = quiet != 0;
     return IPG_OK;
+}
+
+/* Per-kernel profiling: events around every launch while on (adds a few
+ * microseconds per launch). */
+int ipg_app_set_profile(int on)
+{
+    if (on && !ipx_h.pev_made) {
+        for (int i = 0; i < IPX_PEV; i++) {
+            IPX_CU(cudaEventCreate(&ipx_h.pev[0][i]));
+            IPX_CU(cudaEventCreate(&ipx_h.pev[1][i]));
+        }
+        ipx_h.pev_made = true;
+    }
+    ipx_h.profile = on != 0;
+    ipx_h.npev = 0;
+    return IPG_OK;
+}
+
+void ipg_app_profile_reset(void)
+{
+    for (int k = 0; k < IPX_K_N; k++) {
+        ipx_h.prof_launches[k] = ipx_h.prof_timed[k] = 0;
+        ipx_h.prof_ms[k] = ipx_h.prof_bytes[k] = 0.0;
+    }
+}
+
+/* Kernel launches of this library since the last reset. */
+uint64_t ipg_app_launches(void)
+{
+    uint64_t n = 0;
+    for (int k = 0; k < IPX_K_N; k++) n += ipx_h.prof_launches[k];
+    return n;
+}
+
+/* One line per kernel: "name launches timed_launches total_ms algorithmic_bytes". */
+int ipg_app_profile(char* buf, int len)
+{
+    int off = 0;
+    for (int k = 0; k < IPX_K_N && off < len; k++) {
+        if (!ipx_h.prof_launches[k]) continue;
+        off += snprintf(buf + off, (size_t)(len - off), "%s %llu %llu %.6f %.0f\n", ipx_kname[k],
+                        (unsigned long long)ipx_h.prof_launches[k], (unsigned long long)ipx_h.prof_timed[k],
+                        ipx_h.prof_ms[k], ipx_h.prof_bytes[k]);
+    }
+    return off;
 }
 
 int ipg_app_set_param(const char* key, double value)

@@ -52,7 +52,7 @@ APP_SYMBOLS = (
     "ipg_app_abi_version", "ipg_app_describe", "ipg_app_last_error", "ipg_app_attach", "ipg_app_load_host",
     "ipg_app_run", "ipg_app_values", "ipg_app_values_device", "ipg_app_supersteps", "ipg_app_counts",
     "ipg_app_stats", "ipg_app_stream", "ipg_app_set_quiet", "ipg_app_set_param", "ipg_app_release",
-    "ipg_app_main",
+    "ipg_app_set_profile", "ipg_app_profile_reset", "ipg_app_launches", "ipg_app_profile", "ipg_app_main",
 )
 
 
@@ -297,6 +297,9 @@ class Engine:
             L.ipg_app_describe.argtypes = [ctypes.c_char_p, ctypes.c_int]
             L.ipg_app_release.restype = None
             L.ip_get_vertices_count.restype = ctypes.c_size_t
+            L.ipg_app_launches.restype = u64
+            L.ipg_app_profile.argtypes = [ctypes.c_char_p, ctypes.c_int]
+            L.ipg_app_profile_reset.restype = None
             Engine._loaded[path] = L
         self.lib = Engine._loaded[path]
         self.app, self.version, self.id_bits = app, version, id_bits
@@ -362,6 +365,26 @@ class Engine:
 
     def stream(self):
         return self.lib.ipg_app_stream()
+
+    def set_profile(self, on=True):
+        self._check(self.lib.ipg_app_set_profile(int(on)), "ipg_app_set_profile")
+
+    def profile_reset(self):
+        self.lib.ipg_app_profile_reset()
+
+    def launches(self) -> int:
+        """Kernel launches of this application library since the last reset."""
+        return int(self.lib.ipg_app_launches())
+
+    def profile(self) -> dict:
+        """{kernel: {launches, timed, ms, bytes}} accumulated while profiling."""
+        buf = ctypes.create_string_buffer(8192)
+        self.lib.ipg_app_profile(buf, 8192)
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, t, ms, b = line.split()
+            out[name] = {"launches": int(n), "timed": int(t), "ms": float(ms), "bytes": float(b)}
+        return out
 
     def run(self) -> RunResult:
         self.run_only()

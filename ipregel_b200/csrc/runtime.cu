@@ -517,7 +517,7 @@ extern "C" int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int 
 {
     if (!out) return fail(IPG_EINVAL, "ipg_graph_from_host: null output");
     *out = nullptr;
-    if (!wgt) weight_bytes = 0;
+    if (!wgt && E) weight_bytes = 0; /* an edgeless graph may still be declared weighted */
     IPG_TRY(check_widths(id_bytes, weight_bytes));
     if ((V && !idx) || (E && !adj)) return fail(IPG_EINVAL, "ipg_graph_from_host: null buffer");
     if (V >= (1ULL << 32)) return fail(IPG_EINVAL, "at most 2^32-1 vertices are supported");
@@ -543,7 +543,7 @@ extern "C" int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_r
 {
     if (!out) return fail(IPG_EINVAL, "ipg_graph_from_device: null output");
     *out = nullptr;
-    if (!d_wgt) weight_bytes = 0;
+    if (!d_wgt && E) weight_bytes = 0;
     IPG_TRY(check_widths(id_bytes, weight_bytes));
     if (!d_row || (E && !d_adj)) return fail(IPG_EINVAL, "ipg_graph_from_device: null buffer");
     ipg_graph* g = new ipg_graph();
@@ -987,12 +987,12 @@ __global__ void __launch_bounds__(CT_THREADS) k_compact(uint32_t* __restrict__ b
 {
     __shared__ uint32_t s_cnt[CT_WARPS][3];
     __shared__ uint32_t s_base[3];
-    __shared__ unsigned long long s_edges;
+    __shared__ unsigned long long s_edges[3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const uint64_t nwords = (V + 31) >> 5;
     const uint64_t tiles = (nwords + CT_THREADS - 1) / CT_THREADS;
-    if (threadIdx.x == 0) s_edges = 0;
+    if (threadIdx.x < 3) s_edges[threadIdx.x] = 0;
     __syncthreads();
     for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint64_t wbase = tile * CT_THREADS + (uint64_t)warp * 32;
@@ -1003,7 +1003,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_compact(uint32_t* __restrict__ b
             if (wi == nwords - 1 && (V & 31)) word &= (1u << (V & 31)) - 1u;
         }
         uint32_t c0 = 0, c1 = 0, c2 = 0;
-        unsigned long long esum = 0;
+        unsigned long long es[3] = {0, 0, 0};
         for (int j = 0; j < 32; j++) {
             uint32_t w = __shfl_sync(0xffffffffu, word, j);
             if (w == 0) continue;
@@ -1013,26 +1013,28 @@ __global__ void __launch_bounds__(CT_THREADS) k_compact(uint32_t* __restrict__ b
             if (set && row) {
                 uint64_t d = row[v + 1] - row[v];
                 cls = deg_class(d, t0, t1);
-                esum += d;
+                es[cls] += d;
             }
             c0 += __popc(__ballot_sync(0xffffffffu, set && cls == 0));
             c1 += __popc(__ballot_sync(0xffffffffu, set && cls == 1));
             c2 += __popc(__ballot_sync(0xffffffffu, set && cls == 2));
         }
-        for (int o = 16; o > 0; o >>= 1) esum += __shfl_down_sync(0xffffffffu, esum, o);
+        for (int k = 0; k < 3; k++)
+            for (int o = 16; o > 0; o >>= 1) es[k] += __shfl_down_sync(0xffffffffu, es[k], o);
         if (lane == 0) {
             s_cnt[warp][0] = c0;
             s_cnt[warp][1] = c1;
             s_cnt[warp][2] = c2;
-            if (esum) atomicAdd(&s_edges, esum);
+            for (int k = 0; k < 3; k++)
+                if (es[k]) atomicAdd(&s_edges[k], es[k]);
         }
         __syncthreads();
         if (threadIdx.x < 3) {
             uint32_t tot = 0;
             for (int w = 0; w < CT_WARPS; w++) tot += s_cnt[w][threadIdx.x];
             s_base[threadIdx.x] = tot ? atomicAdd(&counts[threadIdx.x], tot) : 0u;
+            if (edges && s_edges[threadIdx.x]) atomicAdd(&edges[threadIdx.x], s_edges[threadIdx.x]);
         }
-        if (threadIdx.x == 3 && edges && s_edges) atomicAdd(edges, s_edges);
         __syncthreads();
         uint32_t o0 = s_base[0], o1 = s_base[1], o2 = s_base[2];
         for (int w = 0; w < warp; w++) {
@@ -1061,7 +1063,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_compact(uint32_t* __restrict__ b
         }
         if (clear && bitmap && wi < nwords && word) bitmap[wi] = 0;
         __syncthreads();
-        if (threadIdx.x == 0) s_edges = 0;
+        if (threadIdx.x < 3) s_edges[threadIdx.x] = 0;
         __syncthreads();
     }
 }
@@ -1131,15 +1133,18 @@ extern "C" int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1
     c.bytes = (V ? V : 1) * 4 + 64;
     IPG_TRY(ipg_dev_alloc(&c.lists, c.bytes));
     DevBuf cnt, l1, l2;
-    IPG_TRY(cnt.alloc(16));
+    IPG_TRY(cnt.alloc(64));
     IPG_TRY(l1.alloc((V ? V : 1) * 4));
     IPG_TRY(l2.alloc((V ? V : 1) * 4));
-    IPG_CUDA(cudaMemset(cnt.p, 0, 16));
+    IPG_CUDA(cudaMemset(cnt.p, 0, 64));
     const uint64_t* row = use_in ? g->v.d_in_row : g->v.d_row;
+    uint64_t* d_esum = (uint64_t*)((char*)cnt.p + 32);
     IPG_TRY(ipg_compact(nullptr, V, row, t0, t1, (uint32_t*)c.lists, l1.as<uint32_t>(), l2.as<uint32_t>(),
-                        cnt.as<uint32_t>(), nullptr, 0, nullptr));
+                        cnt.as<uint32_t>(), d_esum, 0, nullptr));
     uint32_t h[3] = {0, 0, 0};
+    uint64_t esum[3] = {0, 0, 0};
     IPG_CUDA(cudaMemcpy(h, cnt.p, 12, cudaMemcpyDeviceToHost));
+    IPG_CUDA(cudaMemcpy(esum, d_esum, 24, cudaMemcpyDeviceToHost));
     // Pack the three lists back to back in one allocation.
     uint32_t* base = (uint32_t*)c.lists;
     if (h[1]) IPG_CUDA(cudaMemcpy(base + h[0], l1.p, (uint64_t)h[1] * 4, cudaMemcpyDeviceToDevice));
@@ -1164,9 +1169,10 @@ extern "C" int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1
     c.bins.d_list[0] = base;
     c.bins.d_list[1] = base + h[0];
     c.bins.d_list[2] = base + h[0] + h[1];
-    c.bins.count[0] = h[0];
-    c.bins.count[1] = h[1];
-    c.bins.count[2] = h[2];
+    for (int k = 0; k < 3; k++) {
+        c.bins.count[k] = h[k];
+        c.bins.edges[k] = esum[k];
+    }
     c.bins.t0 = t0;
     c.bins.t1 = t1;
     c.t0 = t0;

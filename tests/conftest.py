@@ -16,6 +16,9 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
 
+os.environ.setdefault("IPG_MAX_SUPERSTEPS", "20000")
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs an NVIDIA B200 (runs the CUDA engine)")
 
