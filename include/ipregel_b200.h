@@ -140,6 +140,24 @@ typedef struct ipg_bins {
 int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1,
                    ipg_bins* bins);
 
+/* The same degree classes without allocating anything -- no counterpart in
+ * the reference.  Meant for callers that must not call cudaMalloc: code
+ * running while a stream is being captured, serving loops that cannot afford
+ * the device-wide synchronisation an allocation may cause, and host programs
+ * whose memory pool already owns all of HBM.  The caller passes the row
+ * offsets (V+1 u64), d_lists (V u32: class 0, then class 1, then class 2,
+ * each sorted by id, as ipg_graph_bins packs them) and d_totals (six u64 on
+ * the device: the three class sizes, then their degree sums).  Scratch is a
+ * static device array of 384 KiB that every GPU loading the library holds
+ * until exit, so V is limited to 67,108,864 (IPG_EINVAL beyond).  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams, or concurrent host threads) race and must be
+ * serialised by the caller.  Asynchronous on `stream`. */
+int ipg_degree_classes_noalloc(uint64_t V, const uint64_t* d_row, uint64_t t0,
+                               uint64_t t1, uint32_t* d_lists, uint64_t* d_totals,
+                               void* stream);
+
 /* ------------------------------------------------------------------------
  * Frontier primitives (stream-ordered, no host synchronisation, safe to
  * capture in a CUDA graph).

@@ -39,7 +39,7 @@ RUNTIME_SYMBOLS = (
     "ipg_set_hbm_budget", "ipg_hbm_in_use", "ipg_host_alloc", "ipg_host_free", "ipg_graph_load",
     "ipg_graph_from_host", "ipg_graph_from_device", "ipg_graph_generate_rmat", "ipg_graph_generate_er",
     "ipg_graph_view_get", "ipg_graph_build_in", "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
-    "ipg_graph_bins", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
+    "ipg_graph_bins", "ipg_degree_classes_noalloc", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.

@@ -56,6 +56,12 @@ static int fail(int code, const char* fmt, ...)
     } while (0)
 
 extern "C" const char* ipg_last_error(void) { return g_err.c_str(); }
+
+// Lets other translation units of this library report through ipg_last_error.
+extern "C" __attribute__((visibility("hidden"))) int ipg_internal_fail(int code, const char* msg)
+{
+    return fail(code, "%s", msg);
+}
 extern "C" int ipg_abi_version(void) { return IPG_ABI_VERSION; }
 
 static int g_sm_count = 0;
