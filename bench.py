@@ -304,6 +304,7 @@ def main():
 
         def e2e_step():
             g2 = ip.Graph.from_csr(V, E, p_idx.array, p_adj.array, wgt=p_wgt.array)
+            g2.set_symmetric(True)  # the workload is undirected: every edge has its reverse, same weight
             cc.attach(g2)
             cc.run_only()
             cc.values(out_cc.array)

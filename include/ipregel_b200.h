@@ -84,6 +84,8 @@ typedef struct ipg_graph_view {
     uint64_t max_out_degree;
     uint64_t max_in_degree;
     uint64_t device_bytes;   /* HBM held by the graph */
+    int symmetric;           /* every edge (u,v) has its reverse (v,u) with the
+                                same weight: the rows are also the in-lists */
 } ipg_graph_view;
 
 /* Replaces ip_load_graph (src/iPregel_postamble.h:508-546): reads
@@ -119,6 +121,15 @@ int ipg_graph_generate_er(uint64_t n, uint64_t m, uint64_t seed, int undirected,
                           uint32_t wmax, int need_in, ipg_graph** out);
 
 int ipg_graph_view_get(const ipg_graph* g, ipg_graph_view* view);
+/* Declares (1) or withdraws (0) that the stored graph is symmetric, weights
+ * included.  The generators set it for undirected graphs; for other graphs
+ * it is the caller's statement.  The push versions then may deliver a dense
+ * superstep's broadcasts by pulling over the rows instead of pushing along
+ * them; a wrong declaration gives wrong results, so the default is 0.
+ * ipg_graph_check_symmetric verifies it on the device (rows must be sorted
+ * by neighbour id; *result = 1 symmetric, 0 not, -1 rows unsorted). */
+int ipg_graph_set_symmetric(ipg_graph* g, int symmetric);
+int ipg_graph_check_symmetric(const ipg_graph* g, int* result);
 /* Builds the in-CSR if it is missing (no-op for undirected graphs). */
 int ipg_graph_build_in(ipg_graph* g);
 /* Copies the CSR back to host buffers in the file layout (idx: V x u64). */

@@ -78,6 +78,11 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 
 #define IPX_FULL 0xffffffffu
 #define IPX_THREADS 256
+/* Resident CTAs per SM the edge kernels (push, mark, gather) are compiled
+ * for: 6 x 256 threads keeps their ~40 registers without spilling. */
+#ifndef IPX_EDGE_CTAS
+#define IPX_EDGE_CTAS 6
+#endif
 #define IPX_ERR_SEND_IN_BROADCAST 1u
 #define IPX_ERR_COMBINE_HINT 2u
 
@@ -91,9 +96,10 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 
 /* ------------------------------------------------------------------------ */
 /* Mailbox policies: how a push delivers a message into mailbox[w].          */
-/* deliver() returns true when this call filled an empty mailbox (so the     */
-/* caller sets the received bit once per vertex); kFirstKnown = false means  */
-/* the policy cannot tell and the caller tests the bit itself.               */
+/* deliver() returns true when the received bit of w may still be clear      */
+/* (the CAS policies know exactly: this call filled an empty mailbox; the    */
+/* hardware-atomic ones return true whenever they issued an update), and the */
+/* caller then sets the bit with a fire-and-forget atomic OR.                */
 /* ------------------------------------------------------------------------ */
 template <class T>
 struct ipx_word {
@@ -176,6 +182,25 @@ __device__ __forceinline__ void ipx_atomic_add(T* a, T v)
     else ipx_atomic_cas_op(a, v, [](T x, T y) { return x + y; });
 }
 
+/* Read of a mailbox for the precheck of a monotone combiner.  Within a
+ * superstep a min (max) mailbox only falls (rises), so a stale read can only
+ * let a redundant atomic through, never drop a message: the read may come
+ * from L1 (IPX_PRECHECK_L1 = 1, each SM keeps its own copy of hot mailboxes
+ * such as the hubs') or from L2 (0, fresher but every read of a hot mailbox
+ * lands on one L2 slice). */
+#ifndef IPX_PRECHECK_L1
+#define IPX_PRECHECK_L1 1
+#endif
+template <class T>
+__device__ __forceinline__ T ipx_peek(const T* p)
+{
+#if IPX_PRECHECK_L1
+    return *p;
+#else
+    return __ldcg(p);
+#endif
+}
+
 /* 128-bit compare-and-swap (sm_90+ atom.cas.b128) for the generic 8-byte path. */
 struct __align__(16) ipx_slot128 {
     unsigned long long flag;
@@ -208,22 +233,30 @@ struct ipx_mailbox;
 template <>
 struct ipx_mailbox<IP_COMBINE_MIN, 4> {
     typedef unsigned long long slot;
-    static constexpr bool kFirstKnown = true;
-    static constexpr bool kNeedsRMWCheck = true;
     __device__ static slot empty() { return ~0ULL; }
-    __device__ static bool deliver(slot* s, ipx_msg m)
+    /* The precheck reads through L2 (values only fall within a superstep, so
+     * a stale read can only let a redundant atomic through); the atomic's
+     * result is unused, so it issues as a fire-and-forget reduction. */
+    __device__ static unsigned long long enc(ipx_msg m)
     {
-        const unsigned long long w = (unsigned long long)ipx_to_word(m);
-        if constexpr (std::is_signed<ipx_msg>::value) {
-            // signed order: bias into unsigned order
-            const unsigned long long b = (unsigned long long)(ipx_to_word(m) ^ 0x80000000u);
-            if (b >= __ldcg(s)) return false;
-            return atomicMin(s, b) == ~0ULL;
-        } else {
-            if (w >= __ldcg(s)) return false;
-            return atomicMin(s, w) == ~0ULL;
-        }
+        unsigned int b = ipx_to_word(m);
+        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u; /* signed order as unsigned */
+        return (unsigned long long)b;
     }
+    __device__ static bool precheck(slot* s, ipx_msg m) { return enc(m) < ipx_peek(s); }
+    __device__ static bool commit(slot* s, ipx_msg m)
+    {
+        atomicMin(s, enc(m));
+        return true;
+    }
+    /* merge() is used where one thread owns the mailbox (pull delivery). */
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        const unsigned long long e = enc(m);
+        if (e < *s) *s = e;
+        return true;
+    }
+    __device__ static bool deliver(slot* s, ipx_msg m) { return precheck(s, m) && commit(s, m); }
     __device__ static ipx_msg take(slot* s)
     {
         unsigned long long w = *s;
@@ -237,16 +270,26 @@ struct ipx_mailbox<IP_COMBINE_MIN, 4> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MAX, 4> {
     typedef unsigned long long slot;
-    static constexpr bool kFirstKnown = true;
     __device__ static slot empty() { return 0ULL; }
-    __device__ static bool deliver(slot* s, ipx_msg m)
+    __device__ static unsigned long long enc(ipx_msg m)
     {
         unsigned int b = ipx_to_word(m);
         if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
-        const unsigned long long w = (1ULL << 32) | b;
-        if (w <= __ldcg(s)) return false;
-        return atomicMax(s, w) == 0ULL;
+        return (1ULL << 32) | b;
     }
+    __device__ static bool precheck(slot* s, ipx_msg m) { return enc(m) > ipx_peek(s); }
+    __device__ static bool commit(slot* s, ipx_msg m)
+    {
+        atomicMax(s, enc(m));
+        return true;
+    }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        const unsigned long long e = enc(m);
+        if (e > *s) *s = e;
+        return true;
+    }
+    __device__ static bool deliver(slot* s, ipx_msg m) { return precheck(s, m) && commit(s, m); }
     __device__ static ipx_msg take(slot* s)
     {
         unsigned long long w = *s;
@@ -260,12 +303,28 @@ struct ipx_mailbox<IP_COMBINE_MAX, 4> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MIN, 8> {
     typedef ipx_msg slot;
-    static constexpr bool kFirstKnown = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::max(); }
+    /* No room for a flag: a message equal to the empty value still sets the
+     * received bit (the caller sets it whenever this returns true). */
+    __device__ static bool precheck(slot* s, ipx_msg m)
+    {
+        const ipx_msg c = ipx_peek(s);
+        return m < c || (m == c && c == empty());
+    }
+    __device__ static bool commit(slot* s, ipx_msg m)
+    {
+        ipx_atomic_min(s, m);
+        return true;
+    }
     __device__ static bool deliver(slot* s, ipx_msg m)
     {
         if (m < __ldcg(s)) ipx_atomic_min(s, m);
-        return false;
+        return true;
+    }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        if (m < *s) *s = m;
+        return true;
     }
     __device__ static ipx_msg take(slot* s)
     {
@@ -278,12 +337,26 @@ struct ipx_mailbox<IP_COMBINE_MIN, 8> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MAX, 8> {
     typedef ipx_msg slot;
-    static constexpr bool kFirstKnown = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::lowest(); }
+    __device__ static bool precheck(slot* s, ipx_msg m)
+    {
+        const ipx_msg c = ipx_peek(s);
+        return m > c || (m == c && c == empty());
+    }
+    __device__ static bool commit(slot* s, ipx_msg m)
+    {
+        ipx_atomic_max(s, m);
+        return true;
+    }
     __device__ static bool deliver(slot* s, ipx_msg m)
     {
         if (m > __ldcg(s)) ipx_atomic_max(s, m);
-        return false;
+        return true;
+    }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        if (m > *s) *s = m;
+        return true;
     }
     __device__ static ipx_msg take(slot* s)
     {
@@ -296,12 +369,18 @@ struct ipx_mailbox<IP_COMBINE_MAX, 8> {
 template <int MSGBYTES>
 struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
     typedef ipx_msg slot;
-    static constexpr bool kFirstKnown = false;
     __device__ static slot empty() { return (ipx_msg)0; }
+    __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool deliver(slot* s, ipx_msg m)
     {
         ipx_atomic_add(s, m);
-        return false;
+        return true;
+    }
+    __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        *s = *s + m;
+        return true;
     }
     __device__ static ipx_msg take(slot* s)
     {
@@ -317,8 +396,9 @@ struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
 template <int MSGBYTES>
 struct ipx_mailbox_generic32 {
     typedef unsigned long long slot;
-    static constexpr bool kFirstKnown = true;
     __device__ static slot empty() { return 0ULL; }
+    __device__ static bool precheck(slot*, ipx_msg) { return true; }
+    __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
     __device__ static bool deliver(slot* s, ipx_msg m)
     {
         unsigned long long old = __ldcg(s);
@@ -339,6 +419,17 @@ struct ipx_mailbox_generic32 {
             old = prev;
         }
     }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        const unsigned long long old = *s;
+        ipx_msg v = m;
+        if (old >> 32) {
+            v = ipx_from_word<ipx_msg>((unsigned int)old);
+            ip_combine(&v, m);
+        }
+        *s = (1ULL << 32) | ipx_to_word(v);
+        return true;
+    }
     __device__ static ipx_msg take(slot* s)
     {
         unsigned long long w = *s;
@@ -358,8 +449,9 @@ struct ipx_mailbox<IP_COMBINE_GENERIC, 4> : ipx_mailbox_generic32<4> {};
 template <>
 struct ipx_mailbox<IP_COMBINE_GENERIC, 8> {
     typedef ipx_slot128 slot;
-    static constexpr bool kFirstKnown = true;
     __device__ static slot empty() { return slot{0ULL, 0ULL}; }
+    __device__ static bool precheck(slot*, ipx_msg) { return true; }
+    __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
     __device__ static bool deliver(slot* s, ipx_msg m)
     {
         unsigned long long of = __ldcg(&s->flag), ob = __ldcg(&s->bits);
@@ -380,6 +472,17 @@ struct ipx_mailbox<IP_COMBINE_GENERIC, 8> {
             of = pf;
             ob = pb;
         }
+    }
+    __device__ static bool merge(slot* s, ipx_msg m)
+    {
+        ipx_msg v = m;
+        if (s->flag) {
+            v = ipx_from_word<ipx_msg>(s->bits);
+            ip_combine(&v, m);
+        }
+        s->bits = ipx_to_word(v);
+        s->flag = 1ULL;
+        return true;
     }
     __device__ static ipx_msg take(slot* s)
     {
@@ -432,6 +535,8 @@ struct ipx_consts {
     /* counters: [0..3] active counts ring, [4] edges, [5] error word */
     unsigned long long* ctr;
     uint32_t* err;
+    /* direction optimisation (push versions on symmetric graphs) */
+    int pull_ok;
 };
 
 __constant__ ipx_consts ipx_c;
@@ -441,6 +546,8 @@ __constant__ ipx_consts ipx_c;
  * classes, both reset every superstep. */
 #define IPX_NCTR 16
 #define IPX_CTR_ERR 5
+/* [6]: delivery direction of the current superstep (0 push, 1 pull). */
+#define IPX_CTR_MODE 6
 
 /* Kernel ids for launch counting and per-kernel profiling. */
 enum {
@@ -457,11 +564,15 @@ enum {
     IPX_K_MARK1,
     IPX_K_MARK2,
     IPX_K_COUNT,
+    IPX_K_PULLD0,
+    IPX_K_PULLD1,
+    IPX_K_PULLD2,
     IPX_K_N
 };
 static const char* const ipx_kname[IPX_K_N] = {
     "compute", "compact_broadcasters", "push_thread", "push_warp", "push_block", "compact_targets",
-    "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active"};
+    "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active",
+    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block"};
 
 __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }
@@ -501,12 +612,206 @@ __device__ __forceinline__ void ipx_block_count(unsigned long long c, unsigned l
 /* Delivery of one message into mailbox parity p of vertex w. */
 __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 {
-    const bool first = ipx_mb::deliver(&ipx_c.mbox[p][w], m);
-    if constexpr (ipx_mb::kFirstKnown) {
-        if (first) atomicOr(&ipx_c.recv[p][w >> 5], 1u << (w & 31));
-    } else {
-        ipx_mark(ipx_c.recv[p], w);
+    if (ipx_mb::deliver(&ipx_c.mbox[p][w], m)) atomicOr(&ipx_c.recv[p][w >> 5], 1u << (w & 31));
+}
+
+/* Edges per chunk of a high-degree vertex: the block class is split into
+ * chunks that all CTAs share, so one hub does not leave a single CTA working
+ * after the others have finished. */
+#ifndef IPX_HUB_CHUNK
+#define IPX_HUB_CHUNK 2048
+#endif
+#ifndef IPX_UNROLL
+#define IPX_UNROLL 4
+#endif
+/* 1: sources of the thread and warp classes go through the warp-cooperative
+ * expansion; 0: a thread per source (degree <= IPX_T0), a warp per source. */
+#ifndef IPX_PUSH_EXPAND
+#define IPX_PUSH_EXPAND 0
+#endif
+/* First degree threshold of the broadcaster classes. */
+#define IPX_PUSH_T0 (IPX_PUSH_EXPAND ? IPX_T1 : IPX_T0)
+
+template <class T>
+__device__ __forceinline__ T ipx_shfl_idx(T x, int src)
+{
+    typedef typename ipx_word<T>::type W;
+    W w = ipx_to_word(x);
+    w = __shfl_sync(IPX_FULL, w, src);
+    return ipx_from_word<T>(w);
+}
+
+/* A visitor gets batches of U edges: edge index e[k], target w[k], the
+ * source's message m[k] (outbox value) and ok[k] (lane holds an edge). */
+
+/* Push visitor: prechecks a batch of mailboxes first, then commits. */
+struct ipx_push_visit {
+    static constexpr bool kNeedsMessage = true;
+    int p;
+    template <int U>
+    __device__ __forceinline__ void batch(const uint64_t* e, const ipx_vid* w, const ipx_msg* m, const bool* ok) const
+    {
+        ipx_msg mk[U];
+        bool go[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            go[k] = false;
+            if (ok[k]) {
+#if IPX_EDGE_MSG
+                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_c.wgt[e[k]]);
+#else
+                mk[k] = m[k];
+#endif
+                go[k] = ipx_mb::precheck(&ipx_c.mbox[p][(uint64_t)w[k]], mk[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint64_t t = (uint64_t)w[k];
+            if (go[k] && ipx_mb::commit(&ipx_c.mbox[p][t], mk[k])) atomicOr(&ipx_c.recv[p][t >> 5], 1u << (t & 31));
+        }
     }
+};
+
+/* Target-marking visitor (spread+single_broadcast). */
+struct ipx_mark_visit {
+    static constexpr bool kNeedsMessage = false;
+    template <int U>
+    __device__ __forceinline__ void batch(const uint64_t* e, const ipx_vid* w, const ipx_msg* m, const bool* ok) const
+    {
+        (void)e;
+        (void)m;
+        uint32_t cur[U];
+#pragma unroll
+        for (int k = 0; k < U; k++) cur[k] = ok[k] ? __ldcg(&ipx_c.bt[(uint64_t)w[k] >> 5]) : IPX_FULL;
+#pragma unroll
+        for (int k = 0; k < U; k++) {
+            const uint32_t bit = 1u << ((uint64_t)w[k] & 31);
+            if (!(cur[k] & bit)) atomicOr(&ipx_c.bt[(uint64_t)w[k] >> 5], bit);
+        }
+    }
+};
+
+/* Visits edges [e0, e1) of one source lane-strided, IPX_UNROLL edges a lane
+ * at a time, loading the ids of a batch before visiting any of it. */
+template <class Visit>
+__device__ __forceinline__ void ipx_edges_strided(const ipx_vid* __restrict__ adj, uint64_t e0, uint64_t e1,
+                                                  uint64_t lane, uint64_t lanes, ipx_msg m, const Visit& visit)
+{
+    for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
+        uint64_t ek[IPX_UNROLL];
+        ipx_vid w[IPX_UNROLL];
+        ipx_msg mk[IPX_UNROLL];
+        bool ok[IPX_UNROLL];
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++) {
+            ek[k] = e + k * lanes;
+            ok[k] = ek[k] < e1;
+            w[k] = ok[k] ? adj[ek[k]] : (ipx_vid)0;
+            mk[k] = m;
+        }
+        visit.template batch<IPX_UNROLL>(ek, w, mk, ok);
+    }
+}
+
+/* Warp-cooperative expansion: a warp takes 32 sources of a list at once
+ * (one coalesced read of their ids, row bounds and messages), scans their
+ * degrees, and spreads the concatenated edges over its lanes, so every lane
+ * has work whatever the degrees and the per-source load latency is paid once
+ * per 32 sources.  Each lane finds its source by a 5-step search over the
+ * warp's exclusive degree prefix (shuffles). */
+template <class Visit>
+__device__ __forceinline__ void ipx_warp_expand(const uint32_t* __restrict__ list, uint64_t n, const Visit& visit)
+{
+    const ipx_vid* __restrict__ adj = ipx_c.adj;
+    const uint64_t* __restrict__ row = ipx_c.row;
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ipx_gstride() >> 5;
+    for (uint64_t base = (ipx_gtid() >> 5) * 32; base < n; base += nwarps * 32) {
+        uint64_t r0 = 0;
+        uint32_t deg = 0;
+        ipx_msg m = ipx_msg();
+        if (base + lane < n) {
+            const uint64_t u = list[base + lane];
+            r0 = row[u];
+            deg = (uint32_t)(row[u + 1] - r0);
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+        }
+        uint32_t inc = deg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(IPX_FULL, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const uint32_t excl = inc - deg;
+        const uint32_t total = __shfl_sync(IPX_FULL, inc, 31);
+        for (uint32_t t0 = 0; t0 < total; t0 += 32 * IPX_UNROLL) {
+            uint64_t ek[IPX_UNROLL];
+            ipx_vid w[IPX_UNROLL];
+            ipx_msg mk[IPX_UNROLL];
+            bool ok[IPX_UNROLL];
+#pragma unroll
+            for (int k = 0; k < IPX_UNROLL; k++) {
+                const uint32_t pos = t0 + (uint32_t)(k * 32 + lane);
+                int j = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const uint32_t ex = __shfl_sync(IPX_FULL, excl, j + step);
+                    if (ex <= pos) j += step;
+                }
+                const uint64_t rj = __shfl_sync(IPX_FULL, r0, j);
+                const uint32_t xj = __shfl_sync(IPX_FULL, excl, j);
+                mk[k] = ipx_shfl_idx(m, j);
+                ok[k] = pos < total;
+                ek[k] = rj + (pos - xj);
+                w[k] = ok[k] ? adj[ek[k]] : (ipx_vid)0;
+            }
+            visit.template batch<IPX_UNROLL>(ek, w, mk, ok);
+        }
+    }
+}
+
+/* Chunk prefix of the high-degree class: prefix[i] = chunks of the hubs before
+ * i, prefix[n] = total (one block, a carried scan over tiles of its width). */
+__global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restrict__ list,
+                                                         const uint32_t* __restrict__ count,
+                                                         const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix)
+{
+    __shared__ uint32_t s[1024];
+    const uint64_t n = *count;
+    uint32_t carry = 0;
+    for (uint64_t base = 0; base < n; base += 1024) {
+        const uint64_t i = base + threadIdx.x;
+        uint32_t c = 0;
+        if (i < n) {
+            const uint64_t u = list[i];
+            c = (uint32_t)((row[u + 1] - row[u] + IPX_HUB_CHUNK - 1) / IPX_HUB_CHUNK);
+        }
+        s[threadIdx.x] = c;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            const uint32_t x = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += x;
+            __syncthreads();
+        }
+        if (i < n) prefix[i] = carry + s[threadIdx.x] - c;
+        carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) prefix[n] = carry;
+}
+
+/* Hub index of chunk c: the last i with prefix[i] <= c. */
+__device__ __forceinline__ uint64_t ipx_hub_of_chunk(const uint32_t* __restrict__ prefix, uint64_t n, uint32_t c)
+{
+    uint64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (prefix[mid] <= c) lo = mid;
+        else hi = mid;
+    }
+    return lo;
 }
 
 /* ---- the vertex functions that depend on the version ---- */
@@ -587,63 +892,76 @@ __device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_
 /* Push delivery over degree-class lists of broadcasters.                   */
 /* MODE 0: a thread per broadcaster; 1: a warp; 2: a block.                 */
 /* ------------------------------------------------------------------------ */
-template <int MODE>
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_push(const uint32_t* __restrict__ list,
-                                                          const uint32_t* __restrict__ count, int p)
+/* Runs a visitor over the out-edges of a degree-class list of sources:
+ * MODE 0 and 1 by warp-cooperative expansion, MODE 2 (the hubs) a CTA per
+ * IPX_HUB_CHUNK-edge chunk, chunks located through `prefix`. */
+template <int MODE, class Visit>
+__device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ list, uint64_t n,
+                                                 const uint32_t* __restrict__ prefix, const Visit& visit)
 {
-    const uint64_t n = *count;
-    const ipx_vid* __restrict__ adj = ipx_c.adj;
-    const uint64_t* __restrict__ row = ipx_c.row;
-    if constexpr (MODE == 0) {
+    if constexpr ((MODE == 0 || MODE == 1) && IPX_PUSH_EXPAND) {
+        ipx_warp_expand(list, n, visit);
+    } else if constexpr (MODE == 0) {
+        const ipx_vid* __restrict__ adj = ipx_c.adj;
+        const uint64_t* __restrict__ row = ipx_c.row;
         for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
             const uint64_t u = list[i];
-            const ipx_msg m = ipx_c.outbox[u];
-            const uint64_t e1 = row[u + 1];
-            for (uint64_t e = row[u]; e < e1; e++) {
-#if IPX_EDGE_MSG
-                ipx_deliver(p, (uint64_t)adj[e], IP_BROADCAST_EDGE_MESSAGE(m, ipx_c.wgt[e]));
-#else
-                ipx_deliver(p, (uint64_t)adj[e], m);
-#endif
-            }
+            ipx_msg m = ipx_msg();
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+            ipx_edges_strided(adj, row[u], row[u + 1], 0, 1, m, visit);
+        }
+    } else if constexpr (MODE == 1) {
+        const ipx_vid* __restrict__ adj = ipx_c.adj;
+        const uint64_t* __restrict__ row = ipx_c.row;
+        const uint64_t lane = threadIdx.x & 31;
+        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
+            const uint64_t u = list[i];
+            ipx_msg m = ipx_msg();
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+            ipx_edges_strided(adj, row[u], row[u + 1], lane, 32, m, visit);
         }
     } else {
-        const uint64_t lanes = (MODE == 1) ? 32 : IPX_THREADS;
-        const uint64_t lane = (MODE == 1) ? (threadIdx.x & 31) : threadIdx.x;
-        const uint64_t unit = (MODE == 1) ? (ipx_gtid() >> 5) : blockIdx.x;
-        const uint64_t units = (MODE == 1) ? (ipx_gstride() >> 5) : gridDim.x;
-        for (uint64_t i = unit; i < n; i += units) {
+        if (n == 0) return;
+        const ipx_vid* __restrict__ adj = ipx_c.adj;
+        const uint64_t* __restrict__ row = ipx_c.row;
+        const uint32_t chunks = prefix[n];
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint64_t i = ipx_hub_of_chunk(prefix, n, c);
             const uint64_t u = list[i];
-            const ipx_msg m = ipx_c.outbox[u];
-            const uint64_t e1 = row[u + 1];
-            for (uint64_t e = row[u] + lane; e < e1; e += lanes) {
-#if IPX_EDGE_MSG
-                ipx_deliver(p, (uint64_t)adj[e], IP_BROADCAST_EDGE_MESSAGE(m, ipx_c.wgt[e]));
-#else
-                ipx_deliver(p, (uint64_t)adj[e], m);
-#endif
-            }
+            const uint64_t e0 = row[u] + (uint64_t)(c - prefix[i]) * IPX_HUB_CHUNK;
+            const uint64_t end = row[u + 1];
+            const uint64_t e1 = (e0 + IPX_HUB_CHUNK < end) ? e0 + IPX_HUB_CHUNK : end;
+            ipx_msg m = ipx_msg();
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+            ipx_edges_strided(adj, e0, e1, threadIdx.x, IPX_THREADS, m, visit);
         }
     }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_push(const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ count,
+                                                          const uint32_t* __restrict__ prefix, int p)
+{
+    if (ipx_c.pull_ok && __ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pulls */
+    ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{p});
+}
+
+/* Direction of the superstep's delivery: pull when the broadcasters' out-edges
+ * (degree sums of the compaction) exceed `threshold`. */
+__global__ void ipx_k_decide(unsigned long long threshold)
+{
+    const unsigned long long m = ipx_c.ctr[8] + ipx_c.ctr[9] + ipx_c.ctr[10];
+    ipx_c.ctr[IPX_CTR_MODE] = (m > threshold) ? 1ULL : 0ULL;
+}
+
 /* Marks the out-neighbours of broadcasters as targets (spread+single_broadcast). */
 template <int MODE>
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_mark(const uint32_t* __restrict__ list,
-                                                          const uint32_t* __restrict__ count)
+__global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_mark(const uint32_t* __restrict__ list,
+                                                          const uint32_t* __restrict__ count,
+                                                          const uint32_t* __restrict__ prefix)
 {
-    const uint64_t n = *count;
-    const ipx_vid* __restrict__ adj = ipx_c.adj;
-    const uint64_t* __restrict__ row = ipx_c.row;
-    const uint64_t lanes = (MODE == 0) ? 1 : (MODE == 1 ? 32 : IPX_THREADS);
-    const uint64_t lane = (MODE == 0) ? 0 : (MODE == 1 ? (threadIdx.x & 31) : threadIdx.x);
-    const uint64_t unit = (MODE == 0) ? ipx_gtid() : (MODE == 1 ? (ipx_gtid() >> 5) : blockIdx.x);
-    const uint64_t units = (MODE == 0) ? ipx_gstride() : (MODE == 1 ? (ipx_gstride() >> 5) : gridDim.x);
-    for (uint64_t i = unit; i < n; i += units) {
-        const uint64_t u = list[i];
-        const uint64_t e1 = row[u + 1];
-        for (uint64_t e = row[u] + lane; e < e1; e += lanes) ipx_mark(ipx_c.bt, (uint64_t)adj[e]);
-    }
+    ipx_over_sources<MODE>(list, *count, prefix, ipx_mark_visit{});
 }
 
 /* ------------------------------------------------------------------------ */
@@ -676,7 +994,7 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
 
 /* REACT: reactivate and count (single_broadcast) or not (spread+single_broadcast). */
 template <int MODE, bool REACT>
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_gather(const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ count_dev,
                                                             uint64_t count_host, int ctr_slot)
 {
@@ -769,6 +1087,103 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_gather(const uint32_t* __re
         }
     }
     if constexpr (REACT) ipx_block_count(react, &ipx_c.ctr[ctr_slot]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Pull delivery for the push versions (direction optimisation).  On a       */
+/* symmetric graph a vertex's row lists exactly the vertices that would push */
+/* to it, so folding the messages of its broadcasting row-neighbours gives   */
+/* the message a push would have left in its mailbox (the fold order differs */
+/* only as ip_combine's contract allows).  Used in dense supersteps: it      */
+/* streams every row once and needs no atomics except for the hubs' chunks.  */
+/* MODE 0: thread per vertex, 1: warp per vertex, 2: CTA per 2048-edge chunk */
+/* of a high-degree vertex, committed with the mailbox's atomic.             */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ void ipx_pull_fold_edges(uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes, bool& has,
+                                                    ipx_msg& acc)
+{
+    const ipx_vid* __restrict__ adj = ipx_c.in_adj;
+    const uint32_t* __restrict__ bc = ipx_c.bcaster;
+    const ipx_msg* __restrict__ ob = ipx_c.outbox;
+    for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
+        uint64_t u[IPX_UNROLL];
+        uint32_t word[IPX_UNROLL];
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++) {
+            const uint64_t ek = e + k * lanes;
+            u[k] = (ek < e1) ? (uint64_t)adj[ek] : 0;
+            word[k] = (ek < e1) ? __ldg(&bc[u[k] >> 5]) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++) {
+            if ((word[k] >> (u[k] & 31)) & 1u) {
+#if IPX_EDGE_MSG
+                ipx_msg m = IP_BROADCAST_EDGE_MESSAGE(__ldg(&ob[u[k]]), ipx_c.in_wgt[e + k * lanes]);
+#else
+                ipx_msg m = __ldg(&ob[u[k]]);
+#endif
+                ipx_fold(has, acc, true, m);
+            }
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver(const uint32_t* __restrict__ list,
+                                                                                uint64_t n,
+                                                                                const uint32_t* __restrict__ prefix,
+                                                                                int p)
+{
+    if (!__ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pushes */
+    const uint64_t* __restrict__ row = ipx_c.in_row;
+    if constexpr (MODE == 0) {
+        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            ipx_pull_fold_edges(row[v], row[v + 1], 0, 1, has, acc);
+            if (has && ipx_mb::merge(&ipx_c.mbox[p][v], acc)) ipx_set_bit_agg(ipx_c.recv[p], v);
+        }
+    } else if constexpr (MODE == 1) {
+        const int lane = threadIdx.x & 31;
+        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            ipx_pull_fold_edges(row[v], row[v + 1], lane, 32, has, acc);
+            ipx_warp_fold(has, acc);
+            if (lane == 0 && has && ipx_mb::merge(&ipx_c.mbox[p][v], acc))
+                atomicOr(&ipx_c.recv[p][v >> 5], 1u << (v & 31));
+        }
+    } else {
+        __shared__ bool s_has[IPX_THREADS / 32];
+        __shared__ ipx_msg s_acc[IPX_THREADS / 32];
+        if (n == 0) return;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const uint32_t chunks = prefix[n];
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint64_t i = ipx_hub_of_chunk(prefix, n, c);
+            const uint64_t v = list[i];
+            const uint64_t e0 = row[v] + (uint64_t)(c - prefix[i]) * IPX_HUB_CHUNK;
+            const uint64_t e1 = (e0 + IPX_HUB_CHUNK < row[v + 1]) ? e0 + IPX_HUB_CHUNK : row[v + 1];
+            bool has = false;
+            ipx_msg acc;
+            ipx_pull_fold_edges(e0, e1, threadIdx.x, IPX_THREADS, has, acc);
+            ipx_warp_fold(has, acc);
+            if (lane == 0) {
+                s_has[warp] = has;
+                s_acc[warp] = acc;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                has = false;
+                for (int w = 0; w < IPX_THREADS / 32; w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+                /* chunks of one hub meet in its mailbox: the atomic delivery */
+                if (has && ipx_mb::deliver(&ipx_c.mbox[p][v], acc)) atomicOr(&ipx_c.recv[p][v >> 5], 1u << (v & 31));
+            }
+            __syncthreads();
+        }
+    }
 }
 
 /* ------------------------------------------------------------------------ */

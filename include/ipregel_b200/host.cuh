@@ -46,6 +46,9 @@ struct ipx_host_state {
     uint32_t* blist[3] = {nullptr, nullptr, nullptr};  /* broadcaster classes */
     uint32_t* tlist[3] = {nullptr, nullptr, nullptr};  /* frontier / target classes */
     uint32_t* lcnt = nullptr;                          /* [0..2] broadcaster, [4..6] targets */
+    uint32_t* hub_prefix = nullptr;                    /* chunk prefix of the broadcaster hubs */
+    uint32_t* pull_prefix = nullptr;                   /* chunk prefix of the static in-degree hubs */
+    unsigned long long pull_threshold = 0;             /* pull when broadcaster edges exceed this */
     unsigned long long* h_ctr = nullptr;               /* pinned mirror of ctr */
     uint32_t* h_lcnt = nullptr;                        /* pinned mirror of lcnt */
     cudaStream_t st = nullptr;
@@ -54,6 +57,7 @@ struct ipx_host_state {
     std::vector<uint64_t> counts;
     double total_seconds = 0.0;
     uint64_t edges = 0;
+    uint64_t pulled_supersteps = 0;
     bool quiet = false;
     bool ready = false;
     bool dirty = false;
@@ -175,6 +179,7 @@ static int ipx_reset_vertex_state()
     ipx_h.counts.clear();
     ipx_h.total_seconds = 0.0;
     ipx_h.edges = 0;
+    ipx_h.pulled_supersteps = 0;
     ipx_h.dirty = false;
     ipx_h.host_valid = false;
     return IPG_OK;
@@ -210,6 +215,7 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&c.ctr, IPX_NCTR));
     c.err = (uint32_t*)(c.ctr + IPX_CTR_ERR);
     IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
+    IPX_OK(ipx_alloc(&ipx_h.hub_prefix, gv.E / (IPX_T1 + 1) + 2));
 #if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.active_bm, W + 1));
     IPX_OK(ipx_alloc(&c.hasmsg_bm, W + 1));
@@ -226,6 +232,30 @@ static int ipx_setup_state()
 #endif
 #if IPX_VERSION == IPX_SPREAD
     IPX_OK(ipx_alloc(&ipx_h.tlist[0], V));
+#endif
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
+    /* Direction optimisation: on a symmetric graph (weights included) the
+     * rows are the in-lists, and a dense superstep may pull.  IPG_PULL_DIV
+     * sets the switch point: pull when the broadcasters' out-edges exceed
+     * E / IPG_PULL_DIV.  Default 0, never pull: on R-MAT scale 24 every
+     * threshold measured slower than pushing with the cached precheck. */
+    {
+        const char* d = getenv("IPG_PULL_DIV");
+        const unsigned long long div = (d && *d) ? strtoull(d, nullptr, 10) : 0ULL;
+        c.pull_ok = (gv.symmetric && div > 0 && V > 0) ? 1 : 0;
+        ipx_h.pull_threshold = div ? gv.E / div : ~0ULL;
+    }
+    if (c.pull_ok) {
+        IPX_OK(ipg_graph_bins(ipx_h.g, 0, IPX_T0, IPX_T1, &ipx_h.gbins));
+        IPX_OK(ipx_alloc(&ipx_h.pull_prefix, ipx_h.gbins.count[2] + 2));
+        uint32_t* dcount = nullptr;
+        IPX_OK(ipx_alloc(&dcount, 1));
+        const uint32_t n2 = (uint32_t)ipx_h.gbins.count[2];
+        IPX_CU(cudaMemcpy(dcount, &n2, 4, cudaMemcpyHostToDevice));
+        ipx_k_hub_prefix<<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, gv.d_row, ipx_h.pull_prefix);
+        IPX_CU(cudaGetLastError());
+        IPX_CU(cudaDeviceSynchronize());
+    }
 #endif
 #if IPX_PULL
     IPX_OK(ipx_alloc(&c.hasmsg_b, V + 1));
@@ -295,6 +325,7 @@ static int ipx_set_superstep(uint64_t s)
 }
 
 static int ipx_push_class(int k, int p, uint32_t g);
+static int ipx_deliver_superstep(int p, uint32_t ge);
 
 /* ---- per-kernel profiling (the role of IP_ENABLE_THREAD_PROFILING in the
  * reference, e.g. combiner_spread_postamble.h:166-178, :353-401): every
@@ -327,10 +358,47 @@ static void ipx_k_end()
 static int ipx_push_class(int k, int p, uint32_t g)
 {
     cudaStream_t st = ipx_h.st;
-    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, p));
-    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, p));
-    if (k == 2) IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, p));
+    uint32_t* pre = ipx_h.hub_prefix;
+    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre, p));
+    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre, p));
+    if (k == 2)
+        IPX_LAUNCH(IPX_K_PUSH2, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre);
+                   ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre, p));
     IPX_CU(cudaGetLastError());
+    return IPG_OK;
+}
+
+/* Delivery of the superstep's broadcasts (push versions): compact the
+ * broadcasters into degree classes, then push along their rows, or, on a
+ * symmetric graph when their out-edges pass the threshold, pull over every
+ * row.  The direction is chosen on the device (ipx_k_decide); the kernels of
+ * the other direction return at once. */
+static int ipx_deliver_superstep(int p, uint32_t ge)
+{
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
+    const ipx_consts& c = ipx_h.c;
+    cudaStream_t st = ipx_h.st;
+    uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
+    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, c.V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
+                                                   ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b,
+                                                   c.pull_ok ? 0 : 1, st)));
+    if (c.pull_ok) ipx_k_decide<<<1, 1, 0, st>>>(ipx_h.pull_threshold);
+    for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, p, ge));
+    if (c.pull_ok) {
+        const ipg_bins& b = ipx_h.gbins;
+        IPX_LAUNCH(IPX_K_PULLD0, ipx_k_pull_deliver<0><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], b.count[0],
+                                                                                   ipx_h.pull_prefix, p));
+        IPX_LAUNCH(IPX_K_PULLD1, ipx_k_pull_deliver<1><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], b.count[1],
+                                                                                   ipx_h.pull_prefix, p));
+        IPX_LAUNCH(IPX_K_PULLD2, ipx_k_pull_deliver<2><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], b.count[2],
+                                                                                   ipx_h.pull_prefix, p));
+        IPX_CU(cudaMemsetAsync(c.bcaster, 0, c.W * 4 + 4, st));
+    }
+    IPX_CU(cudaGetLastError());
+#else
+    (void)p;
+    (void)ge;
+#endif
     return IPG_OK;
 }
 
@@ -355,7 +423,17 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
     B[IPX_K_COMPUTE] += (IPX_VERSION == IPX_COMBINER ? V * 3.0 / 8.0 : frontier * 4.0) +
                         frontier * (2 * vb + sb) + nb * mb;
     B[IPX_K_COMPACT_B] += V / 8.0 + nb * 20.0;
-    for (int k = 0; k < 3; k++) B[IPX_K_PUSH0 + k] += l[k] * (20.0 + mb) + ctr[8 + k] * (ib + sb + wb);
+    if (ipx_h.c.pull_ok && ctr[IPX_CTR_MODE]) {
+        /* pulled: every row once, messages of the broadcasting neighbours */
+        const ipg_bins& b = ipx_h.gbins;
+        const double bedges = (double)ctr[8] + ctr[9] + ctr[10];
+        const double E = ipx_h.c.E ? (double)ipx_h.c.E : 1.0;
+        for (int k = 0; k < 3; k++)
+            B[IPX_K_PULLD0 + k] +=
+                b.count[k] * (4.0 + 16.0 + sb) + b.edges[k] * (ib + 0.125) + bedges * (mb + wb) * (b.edges[k] / E);
+    } else {
+        for (int k = 0; k < 3; k++) B[IPX_K_PUSH0 + k] += l[k] * (20.0 + mb) + ctr[8 + k] * (ib + sb + wb);
+    }
 #if IPX_VERSION == IPX_COMBINER
     B[IPX_K_COUNT] += V / 4.0;
 #else
@@ -401,7 +479,13 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count, uint64_t frontier)
 #if IPX_VERSION == IPX_SINGLE_BROADCAST
     ipx_h.edges += ipx_h.c.E;
 #else
-    for (int k = 8; k < 14; k++) ipx_h.edges += ipx_h.h_ctr[k];
+    if (ipx_h.c.pull_ok && ipx_h.h_ctr[IPX_CTR_MODE]) {
+        ipx_h.edges += ipx_h.c.E; /* a pulled superstep reads every row */
+        ipx_h.pulled_supersteps++;
+    } else {
+        for (int k = 8; k < 11; k++) ipx_h.edges += ipx_h.h_ctr[k];
+    }
+    for (int k = 11; k < 14; k++) ipx_h.edges += ipx_h.h_ctr[k];
 #endif
     if (ipx_h.profile) {
         for (int i = 0; i < ipx_h.npev; i++) {
@@ -434,6 +518,7 @@ static int ipx_run_impl()
     const ipx_consts& c = ipx_h.c;
     cudaStream_t st = ipx_h.st;
     const uint32_t g = ipx_grid();
+    const uint32_t ge = ipx_grid(IPX_EDGE_CTAS);
     const uint64_t V = c.V;
     uint64_t count = ip_active_vertices;
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
@@ -462,17 +547,13 @@ static int ipx_run_impl()
 #if IPX_VERSION == IPX_COMBINER
         IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>(s));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
-        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
-                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
-        for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, (int)(s & 1), g));
+        IPX_OK(ipx_deliver_superstep((int)(s & 1), ge));
         IPX_LAUNCH(IPX_K_COUNT,
                    IPX_OK(ipg_bitmap_popc_or(c.active_bm, c.recv[s & 1], c.W, (uint64_t*)(c.ctr + (s & 3)), st)));
 #elif IPX_VERSION == IPX_SPREAD
         IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.lcnt + 4));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
-                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
-        for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, (int)(s & 1), g));
+        IPX_OK(ipx_deliver_superstep((int)(s & 1), ge));
         IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.recv[s & 1], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr,
                                                        nullptr, ipx_h.lcnt + 4, nullptr, 1, st)));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
@@ -481,13 +562,13 @@ static int ipx_run_impl()
             IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>(s, slot));
             const ipg_bins& b = ipx_h.gbins;
             if (b.count[0])
-                IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr,
+                IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr,
                                                                                             b.count[0], slot));
             if (b.count[1])
-                IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr,
+                IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr,
                                                                                             b.count[1], slot));
             if (b.count[2])
-                IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<g, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr,
+                IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr,
                                                                                             b.count[2], slot));
             IPX_CU(cudaGetLastError());
         }
@@ -495,17 +576,21 @@ static int ipx_run_impl()
         IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.tlist[1],
                                                                                 ipx_h.tlist[2], ipx_h.lcnt + 4));
         IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_T0, IPX_T1, ipx_h.blist[0],
+        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
                                                        ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
-        IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0));
-        IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1));
-        IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2));
+        IPX_LAUNCH(IPX_K_MARK0,
+                   ipx_k_mark<0><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
+        IPX_LAUNCH(IPX_K_MARK1,
+                   ipx_k_mark<1><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
+        IPX_LAUNCH(IPX_K_MARK2, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row,
+                                                                    ipx_h.hub_prefix);
+                   ipx_k_mark<2><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
         IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0],
                                                        ipx_h.tlist[1], ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1,
                                                        st)));
-        IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0));
-        IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0));
-        IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0));
+        IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0));
+        IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0));
+        IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0));
         IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
         IPX_CU(cudaGetLastError());
 #endif

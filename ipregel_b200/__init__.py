@@ -26,7 +26,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_DIR = os.path.join(HERE, "lib")
+# IPG_LIB_DIR selects another build of the libraries (e.g. a tuning variant).
+LIB_DIR = os.environ.get("IPG_LIB_DIR") or os.path.join(HERE, "lib")
 BIN_DIR = os.path.join(HERE, "bin")
 RUNTIME_PATH = os.path.join(LIB_DIR, "libipregel_b200.so")
 
@@ -38,7 +39,8 @@ RUNTIME_SYMBOLS = (
     "ipg_last_error", "ipg_abi_version", "ipg_device_info", "ipg_dev_alloc", "ipg_dev_free",
     "ipg_set_hbm_budget", "ipg_hbm_in_use", "ipg_host_alloc", "ipg_host_free", "ipg_graph_load",
     "ipg_graph_from_host", "ipg_graph_from_device", "ipg_graph_generate_rmat", "ipg_graph_generate_er",
-    "ipg_graph_view_get", "ipg_graph_build_in", "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
+    "ipg_graph_view_get", "ipg_graph_set_symmetric", "ipg_graph_check_symmetric", "ipg_graph_build_in",
+    "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
     "ipg_graph_bins", "ipg_degree_classes_noalloc", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
@@ -66,7 +68,7 @@ class _View(ctypes.Structure):
                 ("d_row", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("d_wgt", ctypes.c_void_p),
                 ("d_in_row", ctypes.c_void_p), ("d_in_adj", ctypes.c_void_p), ("d_in_wgt", ctypes.c_void_p),
                 ("max_out_degree", ctypes.c_uint64), ("max_in_degree", ctypes.c_uint64),
-                ("device_bytes", ctypes.c_uint64)]
+                ("device_bytes", ctypes.c_uint64), ("symmetric", ctypes.c_int)]
 
 
 def build():
@@ -95,6 +97,8 @@ def runtime():
         L.ipg_graph_generate_er.argtypes = [u64, u64, u64, i32, ctypes.c_uint32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_view_get.argtypes = [vp, ctypes.POINTER(_View)]
         L.ipg_graph_build_in.argtypes = [vp]
+        L.ipg_graph_set_symmetric.argtypes = [vp, i32]
+        L.ipg_graph_check_symmetric.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.ipg_graph_to_host.argtypes = [vp, vp, vp, vp]
         L.ipg_graph_write.argtypes = [vp, ctypes.c_char_p]
         L.ipg_graph_free.argtypes = [vp]
@@ -224,6 +228,23 @@ class Graph:
         _check(runtime().ipg_graph_load(path.encode(), id_bytes, idx_bytes, int(directed), int(weighted),
                                         weight_bytes, int(need_in), ctypes.byref(h)), where="ipg_graph_load")
         return cls(h.value)
+
+    @property
+    def symmetric(self) -> bool:
+        return bool(self.view.symmetric)
+
+    def set_symmetric(self, symmetric=True):
+        """Declares the stored graph symmetric (weights included), which lets
+        the push versions pull in dense supersteps.  A wrong declaration gives
+        wrong results; check_symmetric() verifies it on the device."""
+        _check(runtime().ipg_graph_set_symmetric(self._h, int(symmetric)), where="ipg_graph_set_symmetric")
+        self.refresh()
+
+    def check_symmetric(self) -> int:
+        """1 symmetric, 0 not, -1 rows not sorted (cannot tell)."""
+        r = ctypes.c_int()
+        _check(runtime().ipg_graph_check_symmetric(self._h, ctypes.byref(r)), where="ipg_graph_check_symmetric")
+        return r.value
 
     def build_in(self):
         _check(runtime().ipg_graph_build_in(self._h), where="ipg_graph_build_in")

@@ -792,6 +792,7 @@ static int build_from_keys(uint64_t V, int vbits, DevBuf& keys, uint64_t n, int 
     }
     ipg_graph* g = new ipg_graph();
     g->v.directed = !undirected;
+    g->v.symmetric = undirected ? 1 : 0; /* every reverse edge was added, weights are symmetric */
     int r = alloc_out(g, V, E, 4, wmax ? 4 : 0);
     if (r == IPG_OK) {
         k_fill_u64<<<grid_for(V + 1, 256), 256, 0, st>>>((uint64_t*)g->row, V + 1, E);
@@ -970,6 +971,58 @@ extern "C" int ipg_graph_write(const ipg_graph* g, const char* path)
 }
 
 extern "C" void ipg_graph_free(ipg_graph* g) { delete g; }
+
+extern "C" int ipg_graph_set_symmetric(ipg_graph* g, int symmetric)
+{
+    if (!g) return fail(IPG_EINVAL, "ipg_graph_set_symmetric: null graph");
+    g->v.symmetric = symmetric ? 1 : 0;
+    return IPG_OK;
+}
+
+// err bit 1: a row is not sorted; bit 2: an edge has no reverse (or the
+// reverse has another weight).
+template <class T>
+__global__ void k_check_symmetric(const uint64_t* __restrict__ row, const T* __restrict__ adj,
+                                  const uint32_t* __restrict__ wgt, uint64_t V, uint64_t E, uint32_t* err)
+{
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t lo = 0, hi = V;  // source u: row[u] <= e < row[u+1]
+        while (hi - lo > 1) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (row[mid] <= e) lo = mid; else hi = mid;
+        }
+        const uint64_t u = lo, v = (uint64_t)adj[e];
+        if (e + 1 < row[u + 1] && (uint64_t)adj[e + 1] <= v) atomicOr(err, 1u);
+        uint64_t a = row[v], b = row[v + 1];  // find u in row(v)
+        while (a < b) {
+            uint64_t mid = (a + b) >> 1;
+            if ((uint64_t)adj[mid] < u) a = mid + 1; else b = mid;
+        }
+        if (a >= row[v + 1] || (uint64_t)adj[a] != u || (wgt && wgt[a] != wgt[e])) atomicOr(err, 2u);
+    }
+}
+
+extern "C" int ipg_graph_check_symmetric(const ipg_graph* g, int* result)
+{
+    if (!g || !result) return fail(IPG_EINVAL, "ipg_graph_check_symmetric: null argument");
+    *result = 1;
+    if (g->v.E == 0) return IPG_OK;
+    if (g->v.d_wgt && g->v.weight_bytes != 4) return fail(IPG_EINVAL, "symmetry check supports u32 weights only");
+    DevBuf err;
+    IPG_TRY(err.alloc(4));
+    IPG_CUDA(cudaMemset(err.p, 0, 4));
+    if (g->v.id_bytes == 4)
+        k_check_symmetric<<<grid_for(g->v.E, 256), 256>>>(g->v.d_row, (const uint32_t*)g->v.d_adj,
+                                                          (const uint32_t*)g->v.d_wgt, g->v.V, g->v.E, err.as<uint32_t>());
+    else
+        k_check_symmetric<<<grid_for(g->v.E, 256), 256>>>(g->v.d_row, (const uint64_t*)g->v.d_adj,
+                                                          (const uint32_t*)g->v.d_wgt, g->v.V, g->v.E, err.as<uint32_t>());
+    IPG_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    IPG_CUDA(cudaMemcpy(&h, err.p, 4, cudaMemcpyDeviceToHost));
+    *result = (h & 1) ? -1 : ((h & 2) ? 0 : 1);
+    return IPG_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Frontier compaction: bitmap -> up to three degree-class lists.

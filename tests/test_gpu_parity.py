@@ -151,3 +151,47 @@ def test_send_message_in_broadcast_version_is_fatal():
     want, _, _ = O.run(g, "cc", "combiner")
     np.testing.assert_array_equal(res.values, want)
     graph.free()
+
+
+PULL_CASES = [("cc", "combiner"), ("cc", "spread"), ("sssp", "combiner"), ("sssp", "spread"),
+              ("sssp_weighted", "combiner"), ("sssp_weighted", "spread"), ("sssp_weighted_send", "spread"),
+              ("pagerank", "combiner"), ("pagerank", "spread"), ("ppr", "combiner")]
+
+
+@pytest.mark.parametrize("app,version", PULL_CASES)
+@pytest.mark.parametrize("div", ["1000000000", "3"])
+def test_pull_delivery_on_symmetric_graphs(app, version, div, monkeypatch):
+    """Push versions on a graph declared symmetric deliver dense supersteps by
+    pulling over the rows (always, with a huge IPG_PULL_DIV, or past E/3):
+    same results as the oracle's push."""
+    import ipregel_b200 as ip
+    monkeypatch.setenv("IPG_PULL_DIV", div)
+    g = _weighted(O.gen_rmat(12, 16, seed=13, undirected=True))
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, wgt=g.wgt)
+    assert graph.check_symmetric() == 1
+    graph.set_symmetric(True)
+    params = {"source": 0} if app in ("sssp", "sssp_weighted", "sssp_weighted_send", "ppr") else {}
+    try:
+        res = ip.run_app(app, version, graph, params=params)
+    finally:
+        graph.free()
+    kw = {"rounds": 20} if app == "ppr" else {}
+    want, counts, _ = O.run(g, ORACLE_APP[app], version, **kw)
+    if app in ("pagerank", "ppr"):
+        assert np.max(np.abs(res.values - want)) <= PR_TOL
+    else:
+        np.testing.assert_array_equal(res.values, want)
+    assert res.counts == [int(c) for c in counts]
+
+
+def test_symmetry_check_and_generator_flag():
+    import ipregel_b200 as ip
+    und = ip.Graph.generate_rmat(10, 8, seed=2, undirected=True, wmax=9)
+    assert und.symmetric and und.check_symmetric() == 1
+    d = ip.Graph.generate_rmat(10, 8, seed=2, undirected=False)
+    assert not d.symmetric and d.check_symmetric() == 0
+    g = O.from_edges(3, [(0, 2), (0, 1), (1, 0), (2, 0)])  # row 0 not sorted
+    u = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+    assert u.check_symmetric() == -1
+    for x in (und, d, u):
+        x.free()
