@@ -281,7 +281,7 @@ def main():
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_path):
         try:
-            tr = json.load(open(traffic_path)).get(top_name.split(":", 1)[1])
+            tr = json.load(open(traffic_path)).get(top_name)
             if tr:
                 roofline["traffic"] = round(tr["dram_bytes_per_algorithmic_byte"] * bytes_per_launch)
                 roofline["traffic_source"] = tr["source"]

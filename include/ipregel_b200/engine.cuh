@@ -233,6 +233,9 @@ struct ipx_mailbox;
 template <>
 struct ipx_mailbox<IP_COMBINE_MIN, 4> {
     typedef unsigned long long slot;
+    /* A delivered message always differs from the empty slot, so whether a
+     * vertex received mail can be read off its mailbox after delivery. */
+    static constexpr bool kFlagInSlot = true;
     __device__ static slot empty() { return ~0ULL; }
     /* The precheck reads through L2 (values only fall within a superstep, so
      * a stale read can only let a redundant atomic through); the atomic's
@@ -270,6 +273,7 @@ struct ipx_mailbox<IP_COMBINE_MIN, 4> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MAX, 4> {
     typedef unsigned long long slot;
+    static constexpr bool kFlagInSlot = true;
     __device__ static slot empty() { return 0ULL; }
     __device__ static unsigned long long enc(ipx_msg m)
     {
@@ -303,6 +307,7 @@ struct ipx_mailbox<IP_COMBINE_MAX, 4> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MIN, 8> {
     typedef ipx_msg slot;
+    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::max(); }
     /* No room for a flag: a message equal to the empty value still sets the
      * received bit (the caller sets it whenever this returns true). */
@@ -337,6 +342,7 @@ struct ipx_mailbox<IP_COMBINE_MIN, 8> {
 template <>
 struct ipx_mailbox<IP_COMBINE_MAX, 8> {
     typedef ipx_msg slot;
+    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::lowest(); }
     __device__ static bool precheck(slot* s, ipx_msg m)
     {
@@ -369,6 +375,7 @@ struct ipx_mailbox<IP_COMBINE_MAX, 8> {
 template <int MSGBYTES>
 struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
     typedef ipx_msg slot;
+    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return (ipx_msg)0; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool deliver(slot* s, ipx_msg m)
@@ -396,6 +403,7 @@ struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
 template <int MSGBYTES>
 struct ipx_mailbox_generic32 {
     typedef unsigned long long slot;
+    static constexpr bool kFlagInSlot = false; /* CAS: the first deliverer knows */
     __device__ static slot empty() { return 0ULL; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
@@ -449,6 +457,7 @@ struct ipx_mailbox<IP_COMBINE_GENERIC, 4> : ipx_mailbox_generic32<4> {};
 template <>
 struct ipx_mailbox<IP_COMBINE_GENERIC, 8> {
     typedef ipx_slot128 slot;
+    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return slot{0ULL, 0ULL}; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
@@ -567,12 +576,13 @@ enum {
     IPX_K_PULLD0,
     IPX_K_PULLD1,
     IPX_K_PULLD2,
+    IPX_K_RECV,
     IPX_K_N
 };
 static const char* const ipx_kname[IPX_K_N] = {
     "compute", "compact_broadcasters", "push_thread", "push_warp", "push_block", "compact_targets",
     "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active",
-    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block"};
+    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block", "received_from_mailbox"};
 
 __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }
@@ -644,6 +654,14 @@ __device__ __forceinline__ T ipx_shfl_idx(T x, int src)
 /* A visitor gets batches of U edges: edge index e[k], target w[k], the
  * source's message m[k] (outbox value) and ok[k] (lane holds an edge). */
 
+/* Blind push (IPX_PUSH_BLIND = 1, packed min/max mailboxes only): every
+ * message is a fire-and-forget atomic with no precheck read, and the
+ * received bitmap is rebuilt from the mailboxes after delivery. */
+#ifndef IPX_PUSH_BLIND
+#define IPX_PUSH_BLIND 0
+#endif
+constexpr bool ipx_blind = IPX_PUSH_BLIND && ipx_mb::kFlagInSlot;
+
 /* Push visitor: prechecks a batch of mailboxes first, then commits. */
 struct ipx_push_visit {
     static constexpr bool kNeedsMessage = true;
@@ -651,6 +669,18 @@ struct ipx_push_visit {
     template <int U>
     __device__ __forceinline__ void batch(const uint64_t* e, const ipx_vid* w, const ipx_msg* m, const bool* ok) const
     {
+        if constexpr (ipx_blind) {
+#pragma unroll
+            for (int k = 0; k < U; k++) {
+                if (!ok[k]) continue;
+#if IPX_EDGE_MSG
+                ipx_mb::commit(&ipx_c.mbox[p][(uint64_t)w[k]], IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_c.wgt[e[k]]));
+#else
+                ipx_mb::commit(&ipx_c.mbox[p][(uint64_t)w[k]], m[k]);
+#endif
+            }
+            return;
+        }
         ipx_msg mk[U];
         bool go[U];
 #pragma unroll
@@ -945,6 +975,26 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_push(const u
 {
     if (ipx_c.pull_ok && __ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pulls */
     ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{p});
+}
+
+template <class S>
+__device__ __forceinline__ bool ipx_filled(const S& s, const S& empty)
+{
+    return !(s == empty);
+}
+__device__ __forceinline__ bool ipx_filled(const ipx_slot128& s, const ipx_slot128&) { return s.flag != 0ULL; }
+
+/* Blind push: received bits of parity p from the mailboxes' flags (one warp
+ * per bitmap word; bits set by direct sends are kept). */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_recv_from_mailbox(int p)
+{
+    const uint64_t V = ipx_c.V;
+    const uint64_t Vp = (V + 31) & ~31ULL;
+    for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
+        const bool r = ipx_mb::kFlagInSlot && v < V && ipx_filled(ipx_c.mbox[p][v], ipx_mb::empty());
+        const uint32_t bits = __ballot_sync(IPX_FULL, r);
+        if ((threadIdx.x & 31) == 0 && bits) ipx_c.recv[p][v >> 5] |= bits;
+    }
 }
 
 /* Direction of the superstep's delivery: pull when the broadcasters' out-edges

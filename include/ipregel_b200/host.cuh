@@ -394,6 +394,7 @@ static int ipx_deliver_superstep(int p, uint32_t ge)
                                                                                    ipx_h.pull_prefix, p));
         IPX_CU(cudaMemsetAsync(c.bcaster, 0, c.W * 4 + 4, st));
     }
+    if constexpr (ipx_blind) IPX_LAUNCH(IPX_K_RECV, ipx_k_recv_from_mailbox<<<ipx_grid(), IPX_THREADS, 0, st>>>(p));
     IPX_CU(cudaGetLastError());
 #else
     (void)p;
