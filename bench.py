@@ -54,6 +54,45 @@ def dist_setup(n_gpus):
     return rank, world, local
 
 
+def reduce_max(x, world, device):
+    """Max of a float over the ranks of the default process group (the timing
+    rule: a multi-GPU time is the slowest rank's)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_gteps(world, edges_per_rank_run, runs, ms_max):
+    """Whole-job Graph500 GTEPS of `world` replicas, each processing the same
+    graph `runs` times, over the slowest rank's time."""
+    return world * edges_per_rank_run * runs / (ms_max * 1e-3) / 1e9
+
+
+def parse_clock_csv(path):
+    """Median SM clock, max clock and throttle reasons seen in an nvidia-smi
+    --query-gpu CSV (ClockSampler.FIELDS, noheader, nounits)."""
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for n, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -94,23 +133,9 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
+        out = parse_clock_csv(self.path)
         os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return out
 
 
 def cpu_host_info():
@@ -227,11 +252,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, world, "cuda")
 
     # ---- device-resident timed region (per-kernel events on) ----
     for eng in (cc, sp):
@@ -262,7 +283,7 @@ def main():
         eng.set_profile(False)
 
     runs = 2 * args.steps
-    value = world * E * runs / (ms * 1e-3) / 1e9
+    value = replica_gteps(world, E, runs, ms)
     traversed_gteps = world * edges_traversed / (ms * 1e-3) / 1e9
 
     # dominant kernel and its roofline
@@ -321,7 +342,7 @@ def main():
         t1.record()
         barrier()
         ms_e2e = max_over_ranks(t0.elapsed_time(t1))
-        e2e = {"value": round(world * E * runs / (ms_e2e * 1e-3) / 1e9, 4), "unit": "GTEPS",
+        e2e = {"value": round(replica_gteps(world, E, runs, ms_e2e), 4), "unit": "GTEPS",
                "h2d_bytes_per_step": int(V * 8 + E * 4 + E * 4), "d2h_bytes_per_step": int(2 * V * 4),
                "ms_per_step": round(ms_e2e / args.steps, 3)}
         # the results of the last end-to-end step are the results of the workload
