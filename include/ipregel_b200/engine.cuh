@@ -85,6 +85,8 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 #endif
 #define IPX_ERR_SEND_IN_BROADCAST 1u
 #define IPX_ERR_COMBINE_HINT 2u
+#define IPX_ERR_SUPERSTEP_LIMIT 4u
+#define IPX_HIST 65536
 
 /* Degree-class thresholds for the thread / warp / block kernels. */
 #ifndef IPX_T0
@@ -546,9 +548,20 @@ struct ipx_consts {
     uint32_t* err;
     /* direction optimisation (push versions on symmetric graphs) */
     int pull_ok;
+    /* list sizes ([0..2] broadcaster classes, [4..6] targets) and the
+     * per-superstep history of a captured loop: hist[s % IPX_HIST][0..3] =
+     * active count, edges traversed, direction, unused */
+    uint32_t* lcnt;
+    unsigned long long* hist;
 };
 
 __constant__ ipx_consts ipx_c;
+
+/* The current superstep, from device memory: the host writes it before each
+ * superstep (host loop), or the previous superstep's last kernel advances it
+ * (captured loop), so every kernel of a superstep reads the same value. */
+__device__ __forceinline__ uint64_t ipx_step() { return (uint64_t)__ldg((const unsigned long long*)&ipd_superstep); }
+__device__ __forceinline__ int ipx_parity() { return (int)(ipx_step() & 1); }
 
 /* ctr layout (u64): [0..3] active-count ring, [5] error word (low half),
  * [8..10] degree sums of the broadcaster classes, [11..13] of the target
@@ -577,12 +590,14 @@ enum {
     IPX_K_PULLD1,
     IPX_K_PULLD2,
     IPX_K_RECV,
+    IPX_K_CTRL,
     IPX_K_N
 };
 static const char* const ipx_kname[IPX_K_N] = {
     "compute", "compact_broadcasters", "push_thread", "push_warp", "push_block", "compact_targets",
     "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active",
-    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block", "received_from_mailbox"};
+    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block", "received_from_mailbox",
+    "superstep_control"};
 
 __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }
@@ -971,10 +986,10 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
 template <int MODE>
 __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_push(const uint32_t* __restrict__ list,
                                                           const uint32_t* __restrict__ count,
-                                                          const uint32_t* __restrict__ prefix, int p)
+                                                          const uint32_t* __restrict__ prefix)
 {
     if (ipx_c.pull_ok && __ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pulls */
-    ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{p});
+    ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{ipx_parity()});
 }
 
 template <class S>
@@ -986,8 +1001,9 @@ __device__ __forceinline__ bool ipx_filled(const ipx_slot128& s, const ipx_slot1
 
 /* Blind push: received bits of parity p from the mailboxes' flags (one warp
  * per bitmap word; bits set by direct sends are kept). */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_recv_from_mailbox(int p)
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_recv_from_mailbox()
 {
+    const int p = ipx_parity();
     const uint64_t V = ipx_c.V;
     const uint64_t Vp = (V + 31) & ~31ULL;
     for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
@@ -1046,8 +1062,9 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
 template <int MODE, bool REACT>
 __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ count_dev,
-                                                            uint64_t count_host, int ctr_slot)
+                                                            uint64_t count_host)
 {
+    const int ctr_slot = (int)(ipx_step() & 3);
     const uint64_t n = count_dev ? (uint64_t)*count_dev : count_host;
     const ipx_vid* __restrict__ adj = ipx_c.in_adj;
     const uint64_t* __restrict__ row = ipx_c.in_row;
@@ -1181,10 +1198,10 @@ __device__ __forceinline__ void ipx_pull_fold_edges(uint64_t e0, uint64_t e1, ui
 template <int MODE>
 __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver(const uint32_t* __restrict__ list,
                                                                                 uint64_t n,
-                                                                                const uint32_t* __restrict__ prefix,
-                                                                                int p)
+                                                                                const uint32_t* __restrict__ prefix)
 {
     if (!__ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pushes */
+    const int p = ipx_parity();
     const uint64_t* __restrict__ row = ipx_c.in_row;
     if constexpr (MODE == 0) {
         for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
@@ -1244,8 +1261,9 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver
  * warp-aligned so that each warp owns whole bitmap words.  The mailbox swap
  * of the previous superstep (:168-183) happens here, for the vertex about to
  * run: a received message becomes the vertex's message and reactivates it. */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner(uint64_t s)
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner()
 {
+    const uint64_t s = ipx_step();
     const uint64_t V = ipx_c.V;
     const uint64_t Vp = (V + 31) & ~31ULL;
     const int pprev = (int)((s + 1) & 1);  /* parity of superstep s-1 */
@@ -1297,9 +1315,10 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner(uint64_t s
 /* Spread (frontier push): src/combiner_spread_postamble.h:235-272 and the
  * mailbox update :331-342.  Superstep 0 runs every vertex, later supersteps
  * the vertices that received mail; a frontier vertex always has a message. */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(uint64_t s, const uint32_t* __restrict__ frontier,
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32_t* __restrict__ frontier,
                                                                     const uint32_t* __restrict__ fcount)
 {
+    const uint64_t s = ipx_step();
     const uint64_t n = s ? (uint64_t)*fcount : ipx_c.V;
     const int pprev = (int)((s + 1) & 1);
     for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
@@ -1324,9 +1343,9 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(uint64_t s, 
 /* Single broadcast (pull) compute phase: combiner_single_broadcast_postamble.h:
  * 185-201.  Each warp rewrites whole has_broadcast words, which also clears
  * last superstep's flags. */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb(uint64_t s, int ctr_slot)
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb()
 {
-    (void)s;
+    const int ctr_slot = (int)(ipx_step() & 3);
     const uint64_t V = ipx_c.V;
     const uint64_t Vp = (V + 31) & ~31ULL;
     const int lane = threadIdx.x & 31;
@@ -1364,11 +1383,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb(uint64_t s, int 
 
 /* Spread + single broadcast compute phase: combiner_spread_single_broadcast_
  * postamble.h:228-237, over the targets (all vertices at superstep 0). */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(uint64_t s, const uint32_t* __restrict__ l0,
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(const uint32_t* __restrict__ l0,
                                                                  const uint32_t* __restrict__ l1,
                                                                  const uint32_t* __restrict__ l2,
                                                                  const uint32_t* __restrict__ cnt)
 {
+    const uint64_t s = ipx_step();
     const uint64_t c0 = s ? cnt[0] : ipx_c.V, c1 = s ? cnt[1] : 0, c2 = s ? cnt[2] : 0;
     const uint64_t n = c0 + c1 + c2;
     for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
@@ -1415,6 +1435,75 @@ __global__ void ipx_k_fill_bits(uint32_t* bm, uint64_t V, uint64_t W)
         if (w == W - 1 && (V & 31)) x = (1u << (V & 31)) - 1u;
         bm[w] = x;
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Superstep control on the device.                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Zeroes the counters a superstep accumulates into. */
+__global__ void ipx_k_begin_superstep()
+{
+    const uint64_t s = ipx_step();
+    ipx_c.ctr[s & 3] = 0ULL;
+    for (int k = 8; k < 14; k++) ipx_c.ctr[k] = 0ULL;
+}
+
+/* Combiner: active count of the superstep = |active or received|
+ * (combiner_postamble.h:151-183), parity read on the device. */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_count_combiner()
+{
+    const uint64_t s = ipx_step();
+    const uint32_t* __restrict__ a = ipx_c.active_bm;
+    const uint32_t* __restrict__ r = ipx_c.recv[s & 1];
+    unsigned long long c = 0;
+    for (uint64_t i = ipx_gtid(); i < ipx_c.W; i += ipx_gstride()) c += __popc(a[i] | r[i]);
+    ipx_block_count(c, &ipx_c.ctr[s & 3]);
+}
+
+/* Active count the reference prints for the superstep just run and tests in
+ * its loop condition (each version's ip_run). */
+__device__ __forceinline__ unsigned long long ipx_superstep_count(uint64_t s)
+{
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    return ipx_c.ctr[s & 3];
+#elif IPX_VERSION == IPX_SPREAD
+    (void)s;
+    return ipx_c.lcnt[4];
+#else
+    (void)s;
+    return (unsigned long long)ipx_c.lcnt[4] + ipx_c.lcnt[5] + ipx_c.lcnt[6];
+#endif
+}
+
+/* Last kernel of a captured superstep: records the superstep in the history,
+ * advances the superstep and sets the loop's condition: continue while the
+ * count is nonzero (combiner_postamble.h:134; spread versions test it after
+ * superstep 0, combiner_spread_postamble.h:212), no kernel reported an error
+ * and the superstep bound is not reached. */
+__global__ void ipx_k_advance(cudaGraphConditionalHandle loop, unsigned long long max_supersteps)
+{
+    const uint64_t s = ipx_step();
+    const unsigned long long count = ipx_superstep_count(s);
+    unsigned long long edges = 0;
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    edges = ipx_c.E;
+#else
+    const bool pulled = ipx_c.pull_ok && ipx_c.ctr[IPX_CTR_MODE];
+    edges = pulled ? ipx_c.E : ipx_c.ctr[8] + ipx_c.ctr[9] + ipx_c.ctr[10];
+    edges += ipx_c.ctr[11] + ipx_c.ctr[12] + ipx_c.ctr[13];
+#endif
+    unsigned long long* h = ipx_c.hist + (s % IPX_HIST) * 4;
+    h[0] = count;
+    h[1] = edges;
+    h[2] = ipx_c.pull_ok ? ipx_c.ctr[IPX_CTR_MODE] : 0ULL;
+    bool go = count != 0 && *ipx_c.err == 0;
+    if (go && s + 1 >= max_supersteps) {
+        atomicOr(ipx_c.err, IPX_ERR_SUPERSTEP_LIMIT);
+        go = false;
+    }
+    ipd_superstep = s + 1;
+    cudaGraphSetConditional(loop, go ? 1u : 0u);
 }
 
 /* Checks an IP_COMBINE_KIND hint against the user's ip_combine on sample

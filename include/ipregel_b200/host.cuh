@@ -29,6 +29,12 @@ extern "C" int ipg_app_main(int argc, char* argv[]);
 extern "C" int ip_app_set_param(const char* key, double value);
 #endif
 
+static bool ipx_env_flag(const char* name)
+{
+    const char* v = getenv(name);
+    return v && *v && atoi(v) != 0;
+}
+
 static double ipx_wtime()
 {
     struct timeval tv;
@@ -76,6 +82,11 @@ struct ipx_host_state {
     int pkid[IPX_PEV];
     int npev = 0;
     bool pev_made = false;
+    /* captured superstep loop */
+    bool graph_loop = ipx_env_flag("IPG_GRAPH_LOOP"); /* read once, at load */
+    cudaGraphExec_t gexec = nullptr;
+    uint64_t body_launches[IPX_K_N] = {0};
+    uint64_t graph_launches = 0;
 };
 static ipx_host_state ipx_h;
 
@@ -122,6 +133,8 @@ static void ipx_release_state()
 {
     for (auto& a : ipx_h.allocs) ipg_dev_free(a.first, a.second);
     ipx_h.allocs.clear();
+    if (ipx_h.gexec) cudaGraphExecDestroy(ipx_h.gexec);
+    ipx_h.gexec = nullptr;
     if (ipx_h.h_ctr) cudaFreeHost(ipx_h.h_ctr);
     if (ipx_h.h_lcnt) cudaFreeHost(ipx_h.h_lcnt);
     ipx_h.h_ctr = nullptr;
@@ -215,6 +228,8 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&c.ctr, IPX_NCTR));
     c.err = (uint32_t*)(c.ctr + IPX_CTR_ERR);
     IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
+    c.lcnt = ipx_h.lcnt;
+    IPX_OK(ipx_alloc(&c.hist, (uint64_t)IPX_HIST * 4));
     IPX_OK(ipx_alloc(&ipx_h.hub_prefix, gv.E / (IPX_T1 + 1) + 2));
 #if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.active_bm, W + 1));
@@ -225,7 +240,11 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&c.mbox[0], V));
     IPX_OK(ipx_alloc(&c.mbox[1], V));
     IPX_OK(ipx_alloc(&c.recv[0], W + 1));
+#if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.recv[1], W + 1));
+#else
+    c.recv[1] = c.recv[0]; /* compacted (and cleared) every superstep */
+#endif
     IPX_OK(ipx_alloc(&c.outbox, V));
     IPX_OK(ipx_alloc(&c.bcaster, W + 1));
     for (int k = 0; k < 3; k++) IPX_OK(ipx_alloc(&ipx_h.blist[k], V));
@@ -324,8 +343,8 @@ static int ipx_set_superstep(uint64_t s)
     return IPG_OK;
 }
 
-static int ipx_push_class(int k, int p, uint32_t g);
-static int ipx_deliver_superstep(int p, uint32_t ge);
+static int ipx_push_class(int k, uint32_t g);
+static int ipx_deliver_superstep(uint32_t ge);
 
 /* ---- per-kernel profiling (the role of IP_ENABLE_THREAD_PROFILING in the
  * reference, e.g. combiner_spread_postamble.h:166-178, :353-401): every
@@ -355,15 +374,16 @@ static void ipx_k_end()
         ipx_k_end();               \
     } while (0)
 
-static int ipx_push_class(int k, int p, uint32_t g)
+static int ipx_push_class(int k, uint32_t g)
 {
     cudaStream_t st = ipx_h.st;
     uint32_t* pre = ipx_h.hub_prefix;
-    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre, p));
-    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre, p));
-    if (k == 2)
-        IPX_LAUNCH(IPX_K_PUSH2, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre);
-                   ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre, p));
+    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre));
+    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre));
+    if (k == 2) {
+        IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre));
+        IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre));
+    }
     IPX_CU(cudaGetLastError());
     return IPG_OK;
 }
@@ -373,7 +393,7 @@ static int ipx_push_class(int k, int p, uint32_t g)
  * symmetric graph when their out-edges pass the threshold, pull over every
  * row.  The direction is chosen on the device (ipx_k_decide); the kernels of
  * the other direction return at once. */
-static int ipx_deliver_superstep(int p, uint32_t ge)
+static int ipx_deliver_superstep(uint32_t ge)
 {
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
     const ipx_consts& c = ipx_h.c;
@@ -382,22 +402,21 @@ static int ipx_deliver_superstep(int p, uint32_t ge)
     IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, c.V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
                                                    ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b,
                                                    c.pull_ok ? 0 : 1, st)));
-    if (c.pull_ok) ipx_k_decide<<<1, 1, 0, st>>>(ipx_h.pull_threshold);
-    for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, p, ge));
+    if (c.pull_ok) IPX_LAUNCH(IPX_K_CTRL, ipx_k_decide<<<1, 1, 0, st>>>(ipx_h.pull_threshold));
+    for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, ge));
     if (c.pull_ok) {
         const ipg_bins& b = ipx_h.gbins;
         IPX_LAUNCH(IPX_K_PULLD0, ipx_k_pull_deliver<0><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], b.count[0],
-                                                                                   ipx_h.pull_prefix, p));
+                                                                                   ipx_h.pull_prefix));
         IPX_LAUNCH(IPX_K_PULLD1, ipx_k_pull_deliver<1><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], b.count[1],
-                                                                                   ipx_h.pull_prefix, p));
+                                                                                   ipx_h.pull_prefix));
         IPX_LAUNCH(IPX_K_PULLD2, ipx_k_pull_deliver<2><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], b.count[2],
-                                                                                   ipx_h.pull_prefix, p));
+                                                                                   ipx_h.pull_prefix));
         IPX_CU(cudaMemsetAsync(c.bcaster, 0, c.W * 4 + 4, st));
     }
-    if constexpr (ipx_blind) IPX_LAUNCH(IPX_K_RECV, ipx_k_recv_from_mailbox<<<ipx_grid(), IPX_THREADS, 0, st>>>(p));
+    if constexpr (ipx_blind) IPX_LAUNCH(IPX_K_RECV, ipx_k_recv_from_mailbox<<<ipx_grid(), IPX_THREADS, 0, st>>>());
     IPX_CU(cudaGetLastError());
 #else
-    (void)p;
     (void)ge;
 #endif
     return IPG_OK;
@@ -411,14 +430,12 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
     const double V = (double)ipx_h.c.V;
     const double ib = sizeof(ipx_vid), vb = sizeof(ipx_val), mb = sizeof(ipx_msg), sb = sizeof(ipx_slot);
     const double wb = IPX_EDGE_MSG ? (double)IPX_WEIGHT_BYTES : 0.0;
-    const unsigned long long* ctr = ipx_h.h_ctr;
-    const uint32_t* l = ipx_h.h_lcnt;
+    [[maybe_unused]] const unsigned long long* ctr = ipx_h.h_ctr;
+    [[maybe_unused]] const uint32_t* l = ipx_h.h_lcnt;
     double* B = ipx_h.prof_bytes;
     (void)s;
     (void)sb;
     (void)wb;
-    (void)ctr;
-    (void)l;
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
     const double nb = (double)l[0] + l[1] + l[2];
     B[IPX_K_COMPUTE] += (IPX_VERSION == IPX_COMBINER ? V * 3.0 / 8.0 : frontier * 4.0) +
@@ -511,26 +528,82 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count, uint64_t frontier)
     return IPG_OK;
 }
 
-static int ipx_run_impl()
+/* Enqueues one superstep's kernels on the engine stream.  Nothing here
+ * depends on host-side values of the superstep: kernels read it (and the
+ * mailbox parity) from device memory, so the same sequence serves the host
+ * loop and the captured loop. */
+static int ipx_enqueue_superstep()
 {
-    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
-    if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
-    ipx_h.dirty = true;
     const ipx_consts& c = ipx_h.c;
     cudaStream_t st = ipx_h.st;
     const uint32_t g = ipx_grid();
     const uint32_t ge = ipx_grid(IPX_EDGE_CTAS);
     const uint64_t V = c.V;
-    uint64_t count = ip_active_vertices;
+    (void)V;
+    (void)ge;
+    IPX_LAUNCH(IPX_K_CTRL, ipx_k_begin_superstep<<<1, 1, 0, st>>>());
+#if IPX_VERSION == IPX_COMBINER
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>());
+    IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
+    IPX_OK(ipx_deliver_superstep(ge));
+    IPX_LAUNCH(IPX_K_COUNT, ipx_k_count_combiner<<<ipx_grid(4), IPX_THREADS, 0, st>>>());
+#elif IPX_VERSION == IPX_SPREAD
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4));
+    IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
+    IPX_OK(ipx_deliver_superstep(ge));
+    /* spread keeps one received bitmap (recv[0] == recv[1]): its compaction
+     * clears it before the next superstep's sends */
+    IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.recv[0], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr, nullptr,
+                                                   ipx_h.lcnt + 4, nullptr, 1, st)));
+#elif IPX_VERSION == IPX_SINGLE_BROADCAST
+    {
+        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>());
+        const ipg_bins& b = ipx_h.gbins;
+        if (b.count[0])
+            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr, b.count[0]));
+        if (b.count[1])
+            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr, b.count[1]));
+        if (b.count[2])
+            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr, b.count[2]));
+    }
+#else
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
     uint64_t* edges_t = (uint64_t*)(c.ctr + 11);
-    (void)V;
-    (void)edges_b;
-    (void)edges_t;
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.tlist[1],
+                                                                            ipx_h.tlist[2], ipx_h.lcnt + 4));
+    IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
+    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
+                                                   ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
+    IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0], ipx_h.tlist[1],
+                                                   ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1, st)));
+    IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0));
+    IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0));
+    IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0));
+    IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
+#endif
+    IPX_CU(cudaGetLastError());
+    return IPG_OK;
+}
+
+static uint64_t ipx_max_supersteps()
+{
     /* The reference loops until quiescence; a bound (IPG_MAX_SUPERSTEPS,
      * default 10^6) turns a program that never halts into an error. */
     const char* lim = getenv("IPG_MAX_SUPERSTEPS");
-    const uint64_t max_supersteps = (lim && *lim) ? strtoull(lim, nullptr, 10) : 1000000ULL;
+    return (lim && *lim) ? strtoull(lim, nullptr, 10) : 1000000ULL;
+}
+
+/* Host-driven loop: one synchronisation per superstep, which gives the
+ * reference's per-superstep log lines with their durations. */
+static int ipx_run_host_loop()
+{
+    const uint64_t V = ipx_h.c.V;
+    uint64_t count = ip_active_vertices;
+    const uint64_t max_supersteps = ipx_max_supersteps();
     for (uint64_t s = 0;; s++) {
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
         if (count == 0) break; /* while(ip_active_vertices != 0), combiner_postamble.h:134 */
@@ -542,62 +615,118 @@ static int ipx_run_impl()
          * the active ones of the previous superstep */
         const uint64_t frontier = (s == 0) ? V : count;
         IPX_OK(ipx_set_superstep(s));
-        IPX_CU(cudaEventRecord(ipx_h.ev0, st));
-        IPX_CU(cudaMemsetAsync(c.ctr + (s & 3), 0, sizeof(unsigned long long), st));
-        IPX_CU(cudaMemsetAsync(c.ctr + 8, 0, 6 * sizeof(unsigned long long), st));
-#if IPX_VERSION == IPX_COMBINER
-        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>(s));
-        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
-        IPX_OK(ipx_deliver_superstep((int)(s & 1), ge));
-        IPX_LAUNCH(IPX_K_COUNT,
-                   IPX_OK(ipg_bitmap_popc_or(c.active_bm, c.recv[s & 1], c.W, (uint64_t*)(c.ctr + (s & 3)), st)));
-#elif IPX_VERSION == IPX_SPREAD
-        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.lcnt + 4));
-        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_OK(ipx_deliver_superstep((int)(s & 1), ge));
-        IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.recv[s & 1], V, nullptr, 0, 0, ipx_h.tlist[0], nullptr,
-                                                       nullptr, ipx_h.lcnt + 4, nullptr, 1, st)));
-#elif IPX_VERSION == IPX_SINGLE_BROADCAST
-        {
-            const int slot = (int)(s & 3);
-            IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>(s, slot));
-            const ipg_bins& b = ipx_h.gbins;
-            if (b.count[0])
-                IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr,
-                                                                                            b.count[0], slot));
-            if (b.count[1])
-                IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr,
-                                                                                            b.count[1], slot));
-            if (b.count[2])
-                IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr,
-                                                                                            b.count[2], slot));
-            IPX_CU(cudaGetLastError());
-        }
-#else
-        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(s, ipx_h.tlist[0], ipx_h.tlist[1],
-                                                                                ipx_h.tlist[2], ipx_h.lcnt + 4));
-        IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-        IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
-                                                       ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
-        IPX_LAUNCH(IPX_K_MARK0,
-                   ipx_k_mark<0><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
-        IPX_LAUNCH(IPX_K_MARK1,
-                   ipx_k_mark<1><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
-        IPX_LAUNCH(IPX_K_MARK2, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row,
-                                                                    ipx_h.hub_prefix);
-                   ipx_k_mark<2><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
-        IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0],
-                                                       ipx_h.tlist[1], ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1,
-                                                       st)));
-        IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0, 0));
-        IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0, 0));
-        IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0, 0));
-        IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
-        IPX_CU(cudaGetLastError());
-#endif
+        IPX_CU(cudaEventRecord(ipx_h.ev0, ipx_h.st));
+        IPX_OK(ipx_enqueue_superstep());
         IPX_OK(ipx_end_superstep(s, &count, frontier));
         ip_superstep = s + 1;
     }
+    return IPG_OK;
+}
+
+/* Captured loop: the superstep's kernels, then ipx_k_advance, as the body of
+ * a CUDA-graph while node; one launch runs the program to quiescence with no
+ * host synchronisation between supersteps.  The graph is built once per
+ * attached graph and reused by later runs. */
+static int ipx_build_graph_loop()
+{
+    if (ipx_h.gexec) return IPG_OK;
+    cudaGraph_t graph = nullptr, body = nullptr;
+    IPX_CU(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle;
+    IPX_CU(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    IPX_CU(cudaGraphAddNode(&node, graph, nullptr, 0, &params));
+    body = params.conditional.phGraph_out[0];
+    const bool prof = ipx_h.profile;
+    ipx_h.profile = false; /* no event nodes inside the body */
+    uint64_t before[IPX_K_N];
+    memcpy(before, ipx_h.prof_launches, sizeof before);
+    IPX_CU(cudaStreamBeginCaptureToGraph(ipx_h.st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int r = ipx_enqueue_superstep();
+    IPX_LAUNCH(IPX_K_CTRL, ipx_k_advance<<<1, 1, 0, ipx_h.st>>>(handle, (unsigned long long)ipx_max_supersteps()));
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ipx_h.st, &captured);
+    ipx_h.profile = prof;
+    for (int k = 0; k < IPX_K_N; k++) {
+        ipx_h.body_launches[k] = ipx_h.prof_launches[k] - before[k];
+        ipx_h.prof_launches[k] = before[k];
+    }
+    if (r != IPG_OK) {
+        cudaGraphDestroy(graph);
+        return r;
+    }
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
+    }
+    e = cudaGraphInstantiate(&ipx_h.gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        ipx_h.gexec = nullptr;
+        return ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
+    }
+    return IPG_OK;
+}
+
+static int ipx_run_graph_loop()
+{
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    if (ip_active_vertices == 0) return IPG_OK;
+#endif
+    IPX_OK(ipx_build_graph_loop());
+    cudaStream_t st = ipx_h.st;
+    IPX_OK(ipx_set_superstep(0));
+    IPX_CU(cudaEventRecord(ipx_h.ev0, st));
+    IPX_CU(cudaGraphLaunch(ipx_h.gexec, st));
+    IPX_CU(cudaEventRecord(ipx_h.ev1, st));
+    IPX_CU(cudaEventSynchronize(ipx_h.ev1));
+    IPX_CU(cudaGetLastError());
+    size_t S = 0;
+    IPX_CU(cudaMemcpyFromSymbol(&S, ipd_superstep, sizeof S));
+    uint32_t err = 0;
+    IPX_CU(cudaMemcpy(&err, ipx_h.c.err, 4, cudaMemcpyDeviceToHost));
+    float ms = 0.f;
+    IPX_CU(cudaEventElapsedTime(&ms, ipx_h.ev0, ipx_h.ev1));
+    ipx_h.total_seconds = ms * 1e-3;
+    const uint64_t kept = S < IPX_HIST ? S : IPX_HIST;
+    std::vector<unsigned long long> hist(kept * 4);
+    if (kept) IPX_CU(cudaMemcpy(hist.data(), ipx_h.c.hist, kept * 4 * 8, cudaMemcpyDeviceToHost));
+    for (uint64_t s = 0; s < S; s++) {
+        const unsigned long long* h = S <= IPX_HIST ? &hist[s * 4] : nullptr;
+        const uint64_t count = h ? h[0] : 0;
+        if (h) ipx_h.edges += h[1];
+        if (h && h[2]) ipx_h.pulled_supersteps++;
+        ipx_h.counts.push_back(count);
+        if (!ipx_h.quiet) {
+            /* one launch for all supersteps: durations are the loop's average */
+            printf("Superstep%zuDuration:%f\n", (size_t)s, ipx_h.total_seconds / (double)S);
+            printf("Superstep%zuActiveVertexCount:%zu\n", (size_t)s, (size_t)count);
+        }
+    }
+    for (int k = 0; k < IPX_K_N; k++) ipx_h.prof_launches[k] += ipx_h.body_launches[k] * S;
+    ipx_h.graph_launches++;
+    ip_superstep = S;
+    ip_active_vertices = ipx_h.counts.empty() ? 0 : ipx_h.counts.back();
+    if (err & IPX_ERR_SEND_IN_BROADCAST)
+        return ipx_fail(IPG_EDEVICE,
+                        "The function send_message should not be used in the SINGLE_BROADCAST version; only "
+                        "broadcast() should be called, and once per superstep maximum.");
+    if (err & IPX_ERR_SUPERSTEP_LIMIT) return ipx_fail(IPG_EDEVICE, "superstep limit (IPG_MAX_SUPERSTEPS) reached");
+    if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
+    return IPG_OK;
+}
+
+static int ipx_run_impl()
+{
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
+    if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
+    ipx_h.dirty = true;
+    IPX_OK(ipx_h.graph_loop ? ipx_run_graph_loop() : ipx_run_host_loop());
     if (!ipx_h.quiet) printf("Total time of supersteps: %fs.\n", ipx_h.total_seconds);
     ipx_h.host_valid = false;
     return IPG_OK;
@@ -910,6 +1039,18 @@ int ipg_app_set_profile(int on)
     ipx_h.npev = 0;
     return IPG_OK;
 }
+
+/* Superstep loop mode: 0 drives supersteps from the host (one
+ * synchronisation each, the reference's per-superstep log), 1 runs them as a
+ * captured CUDA graph with a device-evaluated while condition (one launch per
+ * ip_run).  Default from IPG_GRAPH_LOOP, else 0. */
+int ipg_app_set_graph_loop(int on)
+{
+    ipx_h.graph_loop = on != 0;
+    return IPG_OK;
+}
+
+int ipg_app_graph_loop(void) { return ipx_h.graph_loop ? 1 : 0; }
 
 void ipg_app_profile_reset(void)
 {

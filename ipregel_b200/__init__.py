@@ -55,6 +55,7 @@ APP_SYMBOLS = (
     "ipg_app_run", "ipg_app_values", "ipg_app_values_device", "ipg_app_supersteps", "ipg_app_counts",
     "ipg_app_stats", "ipg_app_stream", "ipg_app_set_quiet", "ipg_app_set_param", "ipg_app_release",
     "ipg_app_set_profile", "ipg_app_profile_reset", "ipg_app_launches", "ipg_app_profile", "ipg_app_main",
+    "ipg_app_set_graph_loop", "ipg_app_graph_loop",
 )
 
 
@@ -393,6 +394,14 @@ class Engine:
     def profile_reset(self):
         self.lib.ipg_app_profile_reset()
 
+    def set_graph_loop(self, on=True):
+        """Run supersteps as one captured CUDA graph whose while condition is
+        evaluated on the device (no host synchronisation per superstep)."""
+        self._check(self.lib.ipg_app_set_graph_loop(int(on)), "ipg_app_set_graph_loop")
+
+    def graph_loop(self) -> bool:
+        return bool(self.lib.ipg_app_graph_loop())
+
     def launches(self) -> int:
         """Kernel launches of this application library since the last reset."""
         return int(self.lib.ipg_app_launches())
@@ -434,10 +443,15 @@ def _ptr(a):
     return a.ctypes.data
 
 
-def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, quiet=True) -> RunResult:
-    """Attach + set params + run, returning values and per-superstep counts."""
+def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, quiet=True,
+            graph_loop=None) -> RunResult:
+    """Attach + set params + run, returning values and per-superstep counts.
+    graph_loop: None keeps the library's mode (IPG_GRAPH_LOOP), True/False
+    selects the captured or the host-driven superstep loop."""
     eng = Engine(app, version, id_bits, generic)
     eng.set_quiet(quiet)
+    if graph_loop is not None:
+        eng.set_graph_loop(graph_loop)
     for k, v in (params or {}).items():
         eng.set_param(k, v)
     eng.attach(graph)
