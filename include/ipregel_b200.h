@@ -56,6 +56,8 @@ uint64_t ipg_hbm_in_use(void);
 /* Page-locked host buffers, for host<->device copies at full link speed. */
 int ipg_host_alloc(void** ptr, uint64_t bytes);
 int ipg_host_free(void* ptr);
+/* Synchronous copy between any two of host and device memory. */
+int ipg_memcpy(void* dst, const void* src, uint64_t bytes);
 
 /* ------------------------------------------------------------------------
  * Graphs.  A graph is the reference loader's CSR (src/iPregel_postamble.h:
@@ -130,6 +132,11 @@ int ipg_graph_view_get(const ipg_graph* g, ipg_graph_view* view);
  * by neighbour id; *result = 1 symmetric, 0 not, -1 rows unsorted). */
 int ipg_graph_set_symmetric(ipg_graph* g, int symmetric);
 int ipg_graph_check_symmetric(const ipg_graph* g, int* result);
+/* The `directed` argument of ip_init (iPregel_preamble.h:298) for a graph
+ * already resident: 0 makes the in-lists alias the rows (what the reference's
+ * benchmarks load, pagerank.c:91), 1 makes them the transpose, built on the
+ * next ipg_graph_build_in.  In-lists built for the other meaning are freed. */
+int ipg_graph_set_directed(ipg_graph* g, int directed);
 /* Builds the in-CSR if it is missing (no-op for undirected graphs). */
 int ipg_graph_build_in(ipg_graph* g);
 /* Copies the CSR back to host buffers in the file layout (idx: V x u64). */
@@ -190,6 +197,42 @@ int ipg_bitmap_popc_or(const uint32_t* d_a, const uint32_t* d_b, uint64_t nwords
 
 /* SM count of the current device (cached). */
 int ipg_sm_count(void);
+
+/* ------------------------------------------------------------------------
+ * PageRank precision split -- no counterpart in the reference, whose
+ * PageRank (benchmarks/pagerank.c:36-66,98-99, run by the single-broadcast
+ * version, combiner_single_broadcast_postamble.h:57-89) is FP64 throughout.
+ * Same formula and superstep structure: x = 1/V at superstep 0, then
+ * x_v = (1-d)/V + d * sum over u in row(v) with deg u > 0 of x_u / deg u for
+ * supersteps 1..rounds (the stored rows are the gather lists, as with the
+ * reference's directed = false).  Values and broadcast quotients are FP32;
+ * every gather sum is compensated (TwoSum-carried error, Neumaier's variant
+ * of Kahan summation) when `compensated` != 0; diagnostics are FP64.
+ * ------------------------------------------------------------------------ */
+typedef struct ipg_pr_plan ipg_pr_plan;
+
+/* Degree classes and scratch for runs on graph g (32-bit ids); holds
+ * 12 bytes per vertex plus 8 bytes per 4096 hub edges of HBM until freed
+ * (and builds the graph's in-lists if it is directed). */
+int ipg_pr_plan_create(ipg_graph* g, ipg_pr_plan** plan);
+void ipg_pr_plan_free(ipg_pr_plan* plan);
+/* Vertices and edge sums of the thread / warp / hub classes, hub chunks. */
+int ipg_pr_plan_info(const ipg_pr_plan* plan, uint64_t* class_counts, uint64_t* class_edges,
+                     uint64_t* hub_chunks);
+
+/* Runs rounds + 1 supersteps, leaving the values in d_values (V floats,
+ * device).  d_diag (device, (rounds + 1) x 3 doubles) receives per superstep
+ * {sum of x, sum of x over vertices without out-edges, sum |x - x_prev|}
+ * (the last is 0 at superstep 0).  Asynchronous on `stream`; allocates and
+ * synchronises nothing, so it can be captured into a CUDA graph. */
+int ipg_pr_run_f32(ipg_pr_plan* plan, uint32_t rounds, double damping, int compensated,
+                   float* d_values, double* d_diag, void* stream);
+
+/* Per-vertex error of d_a (FP32) against d_ref (FP64), n entries on the
+ * device: max abs, max rel (abs where ref is 0), mean abs, and the smallest
+ * index with the max abs error.  Synchronous. */
+int ipg_error_f32_f64(const float* d_a, const double* d_ref, uint64_t n, double* max_abs,
+                      double* max_rel, double* mean_abs, uint64_t* argmax_abs, void* stream);
 
 #ifdef __cplusplus
 }

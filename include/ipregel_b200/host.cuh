@@ -67,7 +67,7 @@ struct ipx_host_state {
     bool quiet = false;
     bool ready = false;
     bool dirty = false;
-    int grid = 0;
+    uint32_t grid_compute = 0; /* resident CTAs of the compute kernel */
     std::vector<struct ip_vertex_t> host_vertices;
     bool host_valid = false;
     char err[512] = {0};
@@ -153,6 +153,17 @@ static void ipx_release_state()
 }
 
 static uint32_t ipx_grid(int per_sm = 8) { return (uint32_t)(ipg_sm_count() * per_sm); }
+
+/* Grid of a grid-stride kernel: the CTAs resident at once (at most per_sm
+ * per SM); a larger grid would run a second wave after the first CTAs
+ * finished their static shares. */
+template <class K>
+static uint32_t ipx_resident_grid(K kernel, int per_sm = 8)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, IPX_THREADS, 0) != cudaSuccess || n <= 0) n = 1;
+    return ipx_grid(n < per_sm ? n : per_sm);
+}
 
 /* ip_init_vertex_range (combiner_postamble.h:89-117 and the other versions):
  * every per-vertex flag back to its initial value. */
@@ -304,6 +315,15 @@ static int ipx_setup_state()
     IPX_CU(cudaMemcpy(&herr, c.err, 4, cudaMemcpyDeviceToHost));
     if (herr & IPX_ERR_COMBINE_HINT)
         return ipx_fail(IPG_EINVAL, "IP_COMBINE_KIND disagrees with ip_combine on sample messages");
+#endif
+#if IPX_VERSION == IPX_COMBINER
+    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_combiner);
+#elif IPX_VERSION == IPX_SPREAD
+    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_spread);
+#elif IPX_VERSION == IPX_SINGLE_BROADCAST
+    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb);
+#else
+    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb);
 #endif
     ipx_h.ready = true;
     return ipx_reset_vertex_state();
@@ -536,7 +556,7 @@ static int ipx_enqueue_superstep()
 {
     const ipx_consts& c = ipx_h.c;
     cudaStream_t st = ipx_h.st;
-    const uint32_t g = ipx_grid();
+    const uint32_t g = ipx_h.grid_compute;
     const uint32_t ge = ipx_grid(IPX_EDGE_CTAS);
     const uint64_t V = c.V;
     (void)V;

@@ -42,6 +42,8 @@ RUNTIME_SYMBOLS = (
     "ipg_graph_view_get", "ipg_graph_set_symmetric", "ipg_graph_check_symmetric", "ipg_graph_build_in",
     "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
     "ipg_graph_bins", "ipg_degree_classes_noalloc", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
+    "ipg_graph_set_directed", "ipg_memcpy", "ipg_pr_plan_create", "ipg_pr_plan_free", "ipg_pr_plan_info", "ipg_pr_run_f32",
+    "ipg_error_f32_f64",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -99,6 +101,7 @@ def runtime():
         L.ipg_graph_view_get.argtypes = [vp, ctypes.POINTER(_View)]
         L.ipg_graph_build_in.argtypes = [vp]
         L.ipg_graph_set_symmetric.argtypes = [vp, i32]
+        L.ipg_graph_set_directed.argtypes = [vp, i32]
         L.ipg_graph_check_symmetric.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
         L.ipg_graph_to_host.argtypes = [vp, vp, vp, vp]
         L.ipg_graph_write.argtypes = [vp, ctypes.c_char_p]
@@ -111,6 +114,14 @@ def runtime():
         L.ipg_set_hbm_budget.argtypes = [u64]
         L.ipg_device_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(u64),
                                       ctypes.POINTER(ctypes.c_int)]
+        L.ipg_memcpy.argtypes = [vp, vp, u64]
+        L.ipg_pr_plan_create.argtypes = [vp, ctypes.POINTER(vp)]
+        L.ipg_pr_plan_free.argtypes = [vp]
+        L.ipg_pr_plan_free.restype = None
+        L.ipg_pr_plan_info.argtypes = [vp, vp, vp, vp]
+        L.ipg_pr_run_f32.argtypes = [vp, ctypes.c_uint32, dbl, i32, vp, vp, vp]
+        L.ipg_error_f32_f64.argtypes = [vp, vp, u64, ctypes.POINTER(dbl), ctypes.POINTER(dbl),
+                                        ctypes.POINTER(dbl), ctypes.POINTER(u64), vp]
         _rt = L
     return _rt
 
@@ -161,6 +172,46 @@ class PinnedArray:
             runtime().ipg_host_free(self._p)
         self._p = None
         self.array = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class DeviceArray:
+    """n elements of dtype in HBM, allocated through the runtime's budgeted
+    allocator (ipg_dev_alloc)."""
+
+    def __init__(self, n, dtype):
+        self.dtype = np.dtype(dtype)
+        self.n = int(n)
+        self.nbytes = max(self.n * self.dtype.itemsize, 16)
+        p = ctypes.c_void_p()
+        _check(runtime().ipg_dev_alloc(ctypes.byref(p), self.nbytes), where="ipg_dev_alloc")
+        self._p = p
+
+    @property
+    def ptr(self):
+        return self._p.value
+
+    def to_host(self):
+        out = np.empty(self.n, dtype=self.dtype)
+        if self.n:
+            _check(runtime().ipg_memcpy(out.ctypes.data, self._p, self.n * self.dtype.itemsize), where="ipg_memcpy")
+        return out
+
+    def from_host(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        assert a.size == self.n
+        if self.n:
+            _check(runtime().ipg_memcpy(self._p, a.ctypes.data, self.n * self.dtype.itemsize), where="ipg_memcpy")
+
+    def free(self):
+        if self._p is not None and self._p.value:
+            runtime().ipg_dev_free(self._p, ctypes.c_uint64(self.nbytes))
+        self._p = None
 
     def __del__(self):
         try:
@@ -239,6 +290,12 @@ class Graph:
         the push versions pull in dense supersteps.  A wrong declaration gives
         wrong results; check_symmetric() verifies it on the device."""
         _check(runtime().ipg_graph_set_symmetric(self._h, int(symmetric)), where="ipg_graph_set_symmetric")
+        self.refresh()
+
+    def set_directed(self, directed=True):
+        """ip_init's `directed` for a resident graph: False makes the in-lists
+        alias the rows (the reference's benchmarks), True the transpose."""
+        _check(runtime().ipg_graph_set_directed(self._h, int(directed)), where="ipg_graph_set_directed")
         self.refresh()
 
     def check_symmetric(self) -> int:
@@ -456,3 +513,68 @@ def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, 
         eng.set_param(k, v)
     eng.attach(graph)
     return eng.run()
+
+
+class PageRankF32:
+    """PageRank with FP32 values and compensated gather sums, FP64
+    diagnostics (ipg_pr_*, include/ipregel_b200.h).  Same formula and
+    superstep structure as benchmarks/pagerank.c:36-66 under the
+    single-broadcast version; rounds + 1 supersteps."""
+
+    def __init__(self, graph: Graph):
+        self.graph = graph
+        p = ctypes.c_void_p()
+        _check(runtime().ipg_pr_plan_create(graph.handle, ctypes.byref(p)), where="ipg_pr_plan_create")
+        self._p = p
+
+    def info(self) -> dict:
+        cnt = np.zeros(3, np.uint64)
+        edg = np.zeros(3, np.uint64)
+        ch = np.zeros(1, np.uint64)
+        _check(runtime().ipg_pr_plan_info(self._p, cnt.ctypes.data, edg.ctypes.data, ch.ctypes.data),
+               where="ipg_pr_plan_info")
+        return {"class_counts": [int(x) for x in cnt], "class_edges": [int(x) for x in edg],
+                "hub_chunks": int(ch[0])}
+
+    def run_device(self, values: DeviceArray, diag: DeviceArray, rounds=10, damping=0.85, compensated=True,
+                   stream=None):
+        """Enqueues a run on `stream` (a cudaStream_t as int, None = legacy
+        default stream); values: V float32, diag: (rounds + 1) * 3 float64."""
+        assert values.dtype == np.float32 and values.n >= self.graph.V
+        assert diag.dtype == np.float64 and diag.n >= (rounds + 1) * 3
+        _check(runtime().ipg_pr_run_f32(self._p, int(rounds), float(damping), int(bool(compensated)), values.ptr,
+                                        diag.ptr, stream), where="ipg_pr_run_f32")
+
+    def run(self, rounds=10, damping=0.85, compensated=True):
+        """(values float32[V], diag float64[rounds + 1, 3]) with columns
+        mass, dangling mass, L1 residual."""
+        V = self.graph.V
+        x = DeviceArray(V, np.float32)
+        d = DeviceArray((rounds + 1) * 3, np.float64)
+        try:
+            self.run_device(x, d, rounds, damping, compensated)
+            return x.to_host(), d.to_host().reshape(rounds + 1, 3)
+        finally:
+            x.free()
+            d.free()
+
+    def free(self):
+        if self._p is not None and self._p.value:
+            runtime().ipg_pr_plan_free(self._p)
+        self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def error_f32_f64(a: DeviceArray, ref: DeviceArray, stream=None) -> dict:
+    """Per-vertex error of an FP32 vector against an FP64 one, on the device."""
+    n = min(a.n, ref.n)
+    mx, mr, mean = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    arg = ctypes.c_uint64()
+    _check(runtime().ipg_error_f32_f64(a.ptr, ref.ptr, n, ctypes.byref(mx), ctypes.byref(mr), ctypes.byref(mean),
+                                       ctypes.byref(arg), stream), where="ipg_error_f32_f64")
+    return {"max_abs": mx.value, "max_rel": mr.value, "mean_abs": mean.value, "argmax_abs": int(arg.value)}

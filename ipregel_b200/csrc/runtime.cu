@@ -171,6 +171,14 @@ extern "C" int ipg_host_free(void* ptr)
     return IPG_OK;
 }
 
+extern "C" int ipg_memcpy(void* dst, const void* src, uint64_t bytes)
+{
+    if (!bytes) return IPG_OK;
+    if (!dst || !src) return fail(IPG_EINVAL, "ipg_memcpy: null pointer");
+    IPG_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDefault));
+    return IPG_OK;
+}
+
 // RAII device buffer for temporaries.
 struct DevBuf {
     void* p = nullptr;
@@ -976,6 +984,29 @@ extern "C" int ipg_graph_set_symmetric(ipg_graph* g, int symmetric)
 {
     if (!g) return fail(IPG_EINVAL, "ipg_graph_set_symmetric: null graph");
     g->v.symmetric = symmetric ? 1 : 0;
+    return IPG_OK;
+}
+
+extern "C" int ipg_graph_set_directed(ipg_graph* g, int directed)
+{
+    if (!g) return fail(IPG_EINVAL, "ipg_graph_set_directed: null graph");
+    directed = directed ? 1 : 0;
+    if (g->v.directed == directed) return IPG_OK;
+    // in-lists and the degree classes over them belong to the old meaning
+    g->v.device_bytes -= g->in_row_bytes + g->in_adj_bytes + g->in_wgt_bytes;
+    ipg_dev_free(g->in_row, g->in_row_bytes);
+    ipg_dev_free(g->in_adj, g->in_adj_bytes);
+    ipg_dev_free(g->in_wgt, g->in_wgt_bytes);
+    g->in_row = g->in_adj = g->in_wgt = nullptr;
+    g->in_row_bytes = g->in_adj_bytes = g->in_wgt_bytes = 0;
+    ipg_dev_free(g->bins[1].lists, g->bins[1].bytes);
+    g->bins[1] = ipg_graph::BinCache();
+    g->v.has_in = 0;
+    g->v.d_in_row = nullptr;
+    g->v.d_in_adj = nullptr;
+    g->v.d_in_wgt = nullptr;
+    g->v.max_in_degree = directed ? 0 : g->v.max_out_degree;  // 0: unknown until ipg_graph_build_in
+    g->v.directed = directed;
     return IPG_OK;
 }
 

@@ -40,6 +40,9 @@ def _compare(app, version, g, directed=False, id_bits=32, generic=False, source=
         params["source"] = source
     if rounds is not None:
         params["rounds"] = rounds
+    elif app in ("pagerank", "ppr"):
+        # parameters are globals of the library: state the default explicitly
+        params["rounds"] = 20 if app == "ppr" else 10
     res = _gpu_run(app, version, g, directed, id_bits, generic, params)
     kw = dict(source=source, directed=directed, id_bytes=id_bits // 8)
     if rounds is not None:
