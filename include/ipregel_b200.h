@@ -110,6 +110,26 @@ int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_row,
                           int weight_bytes, int directed, int need_in,
                           ipg_graph** out);
 
+/* Disjoint union of `count` graphs (no counterpart in the reference, which
+ * loads one graph per program): a new graph whose vertices are those of
+ * parts[0], then parts[1], ... with ids shifted by the vertex offsets voff
+ * (count + 1 entries, host, nullable) and edges concatenated at the edge
+ * offsets eoff (same).  A vertex-centric program run on the union gives each
+ * part the result it gives alone, with ids shifted by the part's offset.
+ * All parts share the id width and, if weighted, the weight width. */
+int ipg_graph_concat(ipg_graph* const* parts, uint32_t count, int directed,
+                     int need_in, ipg_graph** out, uint64_t* voff, uint64_t* eoff);
+
+/* Several applications' captured superstep loops in one CUDA graph launch
+ * (each application library adds its loop with ipg_app_loop_add).  The graph
+ * is instantiated at the first launch; loops added later are not seen.
+ * ipg_fused_launch is synchronous and returns the launch's device time. */
+typedef struct ipg_fused ipg_fused;
+int ipg_fused_create(ipg_fused** out);
+void* ipg_fused_graph(ipg_fused* f);
+int ipg_fused_launch(ipg_fused* f, void* stream, double* seconds);
+void ipg_fused_free(ipg_fused* f);
+
 /* Seeded generators on the device (counter-based SplitMix64, self-loops and
  * duplicates removed, vertex ids not permuted).  R-MAT: 2^scale vertices,
  * edge_factor * 2^scale sampled edges with quadrant probabilities a, b, c,

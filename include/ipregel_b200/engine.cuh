@@ -77,6 +77,8 @@ typedef unsigned int ipx_wgt;
 static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at most 8 bytes");
 
 #define IPX_FULL 0xffffffffu
+/* Largest CTA the kernels are compiled for; the launch size is a runtime
+ * tuning parameter (a multiple of 32 up to this). */
 #define IPX_THREADS 256
 /* Resident CTAs per SM the edge kernels (push, mark, gather) are compiled
  * for: 6 x 256 threads keeps their ~40 registers without spilling. */
@@ -88,7 +90,8 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 #define IPX_ERR_SUPERSTEP_LIMIT 4u
 #define IPX_HIST 65536
 
-/* Degree-class thresholds for the thread / warp / block kernels. */
+/* Default degree-class thresholds for the thread / warp / block kernels
+ * (runtime tuning parameters). */
 #ifndef IPX_T0
 #define IPX_T0 16
 #endif
@@ -629,7 +632,7 @@ __device__ __forceinline__ void ipx_block_count(unsigned long long c, unsigned l
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
-        for (int w = 0; w < IPX_THREADS / 32; w++) t += s_part[w];
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_part[w];
         if (t) atomicAdd(dst, t);
     }
 }
@@ -654,8 +657,6 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_PUSH_EXPAND
 #define IPX_PUSH_EXPAND 0
 #endif
-/* First degree threshold of the broadcaster classes. */
-#define IPX_PUSH_T0 (IPX_PUSH_EXPAND ? IPX_T1 : IPX_T0)
 
 template <class T>
 __device__ __forceinline__ T ipx_shfl_idx(T x, int src)
@@ -978,7 +979,7 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
             const uint64_t e1 = (e0 + IPX_HUB_CHUNK < end) ? e0 + IPX_HUB_CHUNK : end;
             ipx_msg m = ipx_msg();
             if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
-            ipx_edges_strided(adj, e0, e1, threadIdx.x, IPX_THREADS, m, visit);
+            ipx_edges_strided(adj, e0, e1, threadIdx.x, blockDim.x, m, visit);
         }
     }
 }
@@ -1126,7 +1127,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             bool has = false;
             ipx_msg acc;
             const uint64_t e1 = row[v + 1];
-            for (uint64_t e = row[v] + threadIdx.x; e < e1; e += IPX_THREADS) {
+            for (uint64_t e = row[v] + threadIdx.x; e < e1; e += blockDim.x) {
                 const uint64_t u = adj[e];
                 if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
             }
@@ -1138,7 +1139,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             __syncthreads();
             if (threadIdx.x == 0) {
                 has = false;
-                for (int w = 0; w < IPX_THREADS / 32; w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
                 ipx_c.hasmsg_b[v] = has;
                 if (has) {
                     ipx_c.msg[v] = acc;
@@ -1235,7 +1236,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver
             const uint64_t e1 = (e0 + IPX_HUB_CHUNK < row[v + 1]) ? e0 + IPX_HUB_CHUNK : row[v + 1];
             bool has = false;
             ipx_msg acc;
-            ipx_pull_fold_edges(e0, e1, threadIdx.x, IPX_THREADS, has, acc);
+            ipx_pull_fold_edges(e0, e1, threadIdx.x, blockDim.x, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 s_has[warp] = has;
@@ -1244,7 +1245,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver
             __syncthreads();
             if (threadIdx.x == 0) {
                 has = false;
-                for (int w = 0; w < IPX_THREADS / 32; w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
                 /* chunks of one hub meet in its mailbox: the atomic delivery */
                 if (has && ipx_mb::deliver(&ipx_c.mbox[p][v], acc)) atomicOr(&ipx_c.recv[p][v >> 5], 1u << (v & 31));
             }

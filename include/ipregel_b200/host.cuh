@@ -28,11 +28,21 @@ extern "C" int ipg_app_main(int argc, char* argv[]);
 /* Optional application hook: set a named parameter before ip_run. */
 extern "C" int ip_app_set_param(const char* key, double value);
 #endif
+#ifdef IP_APP_PARAM_PTRS
+/* Optional application hook: a named device array of n entries. */
+extern "C" int ip_app_set_param_ptr(const char* key, const void* ptr, uint64_t n);
+#endif
 
 static bool ipx_env_flag(const char* name)
 {
     const char* v = getenv(name);
     return v && *v && atoi(v) != 0;
+}
+
+static uint64_t ipx_env_u64(const char* name, uint64_t dflt)
+{
+    const char* v = getenv(name);
+    return (v && *v) ? strtoull(v, nullptr, 10) : dflt;
 }
 
 static double ipx_wtime()
@@ -67,7 +77,18 @@ struct ipx_host_state {
     bool quiet = false;
     bool ready = false;
     bool dirty = false;
+    /* Runtime tuning, applied at the next attach: CTA size of the superstep
+     * kernels, degree-class thresholds (thread up to t0 edges, warp up to
+     * t1, CTAs beyond) and the pull switch of the push versions (pull when
+     * the broadcasters' edges exceed E / pull_div; 0 never). */
+    struct {
+        int block = IPX_THREADS;
+        uint64_t t0 = IPX_T0, t1 = IPX_T1;
+        uint64_t pull_div = ipx_env_u64("IPG_PULL_DIV", 0);
+    } tune;
+    int tb = IPX_THREADS;      /* CTA size in use */
     uint32_t grid_compute = 0; /* resident CTAs of the compute kernel */
+    uint32_t grid_edge = 0;    /* resident CTAs of the edge kernels */
     std::vector<struct ip_vertex_t> host_vertices;
     bool host_valid = false;
     char err[512] = {0};
@@ -158,12 +179,15 @@ static uint32_t ipx_grid(int per_sm = 8) { return (uint32_t)(ipg_sm_count() * pe
  * per SM); a larger grid would run a second wave after the first CTAs
  * finished their static shares. */
 template <class K>
-static uint32_t ipx_resident_grid(K kernel, int per_sm = 8)
+static uint32_t ipx_resident_grid(K kernel, int block, int per_sm)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, IPX_THREADS, 0) != cudaSuccess || n <= 0) n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess || n <= 0) n = 1;
     return ipx_grid(n < per_sm ? n : per_sm);
 }
+
+/* First degree threshold of the broadcaster classes. */
+static uint64_t ipx_push_t0() { return IPX_PUSH_EXPAND ? ipx_h.tune.t1 : ipx_h.tune.t0; }
 
 /* ip_init_vertex_range (combiner_postamble.h:89-117 and the other versions):
  * every per-vertex flag back to its initial value. */
@@ -214,6 +238,7 @@ static int ipx_setup_state()
 {
     ipx_consts& c = ipx_h.c;
     memset(&c, 0, sizeof c);
+    ipx_h.tb = ipx_h.tune.block;
     const ipg_graph_view& gv = ipx_h.gv;
     if (gv.id_bytes != (int)sizeof(ipx_vid)) return ipx_fail(IPG_EINVAL, "graph id width differs from IP_VERTEX_ID_TYPE");
     const uint64_t V = gv.V, W = (V + 31) / 32;
@@ -241,7 +266,7 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
     c.lcnt = ipx_h.lcnt;
     IPX_OK(ipx_alloc(&c.hist, (uint64_t)IPX_HIST * 4));
-    IPX_OK(ipx_alloc(&ipx_h.hub_prefix, gv.E / (IPX_T1 + 1) + 2));
+    IPX_OK(ipx_alloc(&ipx_h.hub_prefix, gv.E / (ipx_h.tune.t1 + 1) + 2));
 #if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.active_bm, W + 1));
     IPX_OK(ipx_alloc(&c.hasmsg_bm, W + 1));
@@ -264,25 +289,28 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&ipx_h.tlist[0], V));
 #endif
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
-    /* Direction optimisation: on a symmetric graph (weights included) the
-     * rows are the in-lists, and a dense superstep may pull.  IPG_PULL_DIV
-     * sets the switch point: pull when the broadcasters' out-edges exceed
-     * E / IPG_PULL_DIV.  Default 0, never pull: on R-MAT scale 24 every
-     * threshold measured slower than pushing with the cached precheck. */
+    /* Direction optimisation: a dense superstep may deliver by pulling over
+     * the in-lists, when they list exactly the vertices that would push:
+     * on a symmetric graph (weights included), whose rows are the in-lists,
+     * or on a directed graph with its transpose built.  tune.pull_div (the
+     * IPG_PULL_DIV environment variable by default) sets the switch point:
+     * pull when the broadcasters' out-edges exceed E / pull_div.  Default 0,
+     * never pull: on R-MAT scale 24 every threshold measured slower than
+     * pushing with the cached precheck. */
     {
-        const char* d = getenv("IPG_PULL_DIV");
-        const unsigned long long div = (d && *d) ? strtoull(d, nullptr, 10) : 0ULL;
-        c.pull_ok = (gv.symmetric && div > 0 && V > 0) ? 1 : 0;
+        const unsigned long long div = ipx_h.tune.pull_div;
+        const bool in_exact = gv.symmetric || (gv.directed && gv.has_in);
+        c.pull_ok = (in_exact && div > 0 && V > 0) ? 1 : 0;
         ipx_h.pull_threshold = div ? gv.E / div : ~0ULL;
     }
     if (c.pull_ok) {
-        IPX_OK(ipg_graph_bins(ipx_h.g, 0, IPX_T0, IPX_T1, &ipx_h.gbins));
+        IPX_OK(ipg_graph_bins(ipx_h.g, gv.directed ? 1 : 0, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
         IPX_OK(ipx_alloc(&ipx_h.pull_prefix, ipx_h.gbins.count[2] + 2));
         uint32_t* dcount = nullptr;
         IPX_OK(ipx_alloc(&dcount, 1));
         const uint32_t n2 = (uint32_t)ipx_h.gbins.count[2];
         IPX_CU(cudaMemcpy(dcount, &n2, 4, cudaMemcpyHostToDevice));
-        ipx_k_hub_prefix<<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, gv.d_row, ipx_h.pull_prefix);
+        ipx_k_hub_prefix<<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
         IPX_CU(cudaGetLastError());
         IPX_CU(cudaDeviceSynchronize());
     }
@@ -295,7 +323,7 @@ static int ipx_setup_state()
 #endif
 #if IPX_VERSION == IPX_SINGLE_BROADCAST
     IPX_OK(ipx_alloc(&c.active_b, V + 1));
-    IPX_OK(ipg_graph_bins(ipx_h.g, 1, IPX_T0, IPX_T1, &ipx_h.gbins));
+    IPX_OK(ipg_graph_bins(ipx_h.g, 1, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
 #endif
 #if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
     IPX_OK(ipx_alloc(&c.bt, W + 1));
@@ -316,15 +344,23 @@ static int ipx_setup_state()
     if (herr & IPX_ERR_COMBINE_HINT)
         return ipx_fail(IPG_EINVAL, "IP_COMBINE_KIND disagrees with ip_combine on sample messages");
 #endif
+    {
+        const int tb = ipx_h.tb;
+        const int per_sm = 2048 / tb;
 #if IPX_VERSION == IPX_COMBINER
-    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_combiner);
+        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_combiner, tb, per_sm);
+        ipx_h.grid_edge = ipx_resident_grid(ipx_k_push<1>, tb, per_sm);
 #elif IPX_VERSION == IPX_SPREAD
-    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_spread);
+        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_spread, tb, per_sm);
+        ipx_h.grid_edge = ipx_resident_grid(ipx_k_push<1>, tb, per_sm);
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
-    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb);
+        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb, tb, per_sm);
+        ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, true>, tb, per_sm);
 #else
-    ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb);
+        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb, tb, per_sm);
+        ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, false>, tb, per_sm);
 #endif
+    }
     ipx_h.ready = true;
     return ipx_reset_vertex_state();
 }
@@ -341,6 +377,8 @@ static int ipx_attach(ipg_graph* g, bool own)
                    || true
 #endif
         ;
+    /* the push versions pull over the transpose of a directed graph */
+    if (!IPX_PULL && ipx_h.tune.pull_div > 0 && ipx_h.gv.directed) need_in = true;
     if (need_in && !ipx_h.gv.has_in) {
         IPX_OK(ipg_graph_build_in(g));
         IPX_OK(ipg_graph_view_get(g, &ipx_h.gv));
@@ -398,11 +436,11 @@ static int ipx_push_class(int k, uint32_t g)
 {
     cudaStream_t st = ipx_h.st;
     uint32_t* pre = ipx_h.hub_prefix;
-    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre));
-    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre));
+    if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre));
+    if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre));
     if (k == 2) {
         IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre));
-        IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre));
+        IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre));
     }
     IPX_CU(cudaGetLastError());
     return IPG_OK;
@@ -419,18 +457,18 @@ static int ipx_deliver_superstep(uint32_t ge)
     const ipx_consts& c = ipx_h.c;
     cudaStream_t st = ipx_h.st;
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
-    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, c.V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
+    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, c.V, c.row, ipx_push_t0(), ipx_h.tune.t1, ipx_h.blist[0],
                                                    ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b,
                                                    c.pull_ok ? 0 : 1, st)));
     if (c.pull_ok) IPX_LAUNCH(IPX_K_CTRL, ipx_k_decide<<<1, 1, 0, st>>>(ipx_h.pull_threshold));
     for (int k = 0; k < 3; k++) IPX_OK(ipx_push_class(k, ge));
     if (c.pull_ok) {
         const ipg_bins& b = ipx_h.gbins;
-        IPX_LAUNCH(IPX_K_PULLD0, ipx_k_pull_deliver<0><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], b.count[0],
+        IPX_LAUNCH(IPX_K_PULLD0, ipx_k_pull_deliver<0><<<ge, ipx_h.tb, 0, st>>>(b.d_list[0], b.count[0],
                                                                                    ipx_h.pull_prefix));
-        IPX_LAUNCH(IPX_K_PULLD1, ipx_k_pull_deliver<1><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], b.count[1],
+        IPX_LAUNCH(IPX_K_PULLD1, ipx_k_pull_deliver<1><<<ge, ipx_h.tb, 0, st>>>(b.d_list[1], b.count[1],
                                                                                    ipx_h.pull_prefix));
-        IPX_LAUNCH(IPX_K_PULLD2, ipx_k_pull_deliver<2><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], b.count[2],
+        IPX_LAUNCH(IPX_K_PULLD2, ipx_k_pull_deliver<2><<<ge, ipx_h.tb, 0, st>>>(b.d_list[2], b.count[2],
                                                                                    ipx_h.pull_prefix));
         IPX_CU(cudaMemsetAsync(c.bcaster, 0, c.W * 4 + 4, st));
     }
@@ -557,18 +595,18 @@ static int ipx_enqueue_superstep()
     const ipx_consts& c = ipx_h.c;
     cudaStream_t st = ipx_h.st;
     const uint32_t g = ipx_h.grid_compute;
-    const uint32_t ge = ipx_grid(IPX_EDGE_CTAS);
+    const uint32_t ge = ipx_h.grid_edge;
     const uint64_t V = c.V;
     (void)V;
     (void)ge;
     IPX_LAUNCH(IPX_K_CTRL, ipx_k_begin_superstep<<<1, 1, 0, st>>>());
 #if IPX_VERSION == IPX_COMBINER
-    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, IPX_THREADS, 0, st>>>());
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, ipx_h.tb, 0, st>>>());
     IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 4 * sizeof(uint32_t), st));
     IPX_OK(ipx_deliver_superstep(ge));
-    IPX_LAUNCH(IPX_K_COUNT, ipx_k_count_combiner<<<ipx_grid(4), IPX_THREADS, 0, st>>>());
+    IPX_LAUNCH(IPX_K_COUNT, ipx_k_count_combiner<<<ipx_grid(4), 256, 0, st>>>());
 #elif IPX_VERSION == IPX_SPREAD
-    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4));
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_spread<<<g, ipx_h.tb, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4));
     IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
     IPX_OK(ipx_deliver_superstep(ge));
     /* spread keeps one received bitmap (recv[0] == recv[1]): its compaction
@@ -577,32 +615,32 @@ static int ipx_enqueue_superstep()
                                                    ipx_h.lcnt + 4, nullptr, 1, st)));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
     {
-        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, IPX_THREADS, 0, st>>>());
+        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, ipx_h.tb, 0, st>>>());
         const ipg_bins& b = ipx_h.gbins;
         if (b.count[0])
-            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[0], nullptr, b.count[0]));
+            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[0], nullptr, b.count[0]));
         if (b.count[1])
-            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[1], nullptr, b.count[1]));
+            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[1], nullptr, b.count[1]));
         if (b.count[2])
-            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, IPX_THREADS, 0, st>>>(b.d_list[2], nullptr, b.count[2]));
+            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[2], nullptr, b.count[2]));
     }
 #else
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
     uint64_t* edges_t = (uint64_t*)(c.ctr + 11);
-    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.tlist[1],
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_ssb<<<g, ipx_h.tb, 0, st>>>(ipx_h.tlist[0], ipx_h.tlist[1],
                                                                             ipx_h.tlist[2], ipx_h.lcnt + 4));
     IPX_CU(cudaMemsetAsync(ipx_h.lcnt, 0, 8 * sizeof(uint32_t), st));
-    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, IPX_PUSH_T0, IPX_T1, ipx_h.blist[0],
+    IPX_LAUNCH(IPX_K_COMPACT_B, IPX_OK(ipg_compact(c.bcaster, V, c.row, ipx_push_t0(), ipx_h.tune.t1, ipx_h.blist[0],
                                                    ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
-    IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
-    IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix));
-    IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<ge, IPX_THREADS, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
-    IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, IPX_T0, IPX_T1, ipx_h.tlist[0], ipx_h.tlist[1],
+    IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, ipx_h.tune.t0, ipx_h.tune.t1, ipx_h.tlist[0], ipx_h.tlist[1],
                                                    ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1, st)));
-    IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0));
-    IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0));
-    IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, IPX_THREADS, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0));
+    IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0));
+    IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0));
+    IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0));
     IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
 #endif
     IPX_CU(cudaGetLastError());
@@ -647,11 +685,11 @@ static int ipx_run_host_loop()
  * a CUDA-graph while node; one launch runs the program to quiescence with no
  * host synchronisation between supersteps.  The graph is built once per
  * attached graph and reused by later runs. */
-static int ipx_build_graph_loop()
+/* Adds the superstep loop as a root node of `graph`: a while node whose
+ * body is one superstep's kernels followed by ipx_k_advance, which records
+ * the superstep and sets the condition on the device. */
+static int ipx_add_loop_node(cudaGraph_t graph)
 {
-    if (ipx_h.gexec) return IPG_OK;
-    cudaGraph_t graph = nullptr, body = nullptr;
-    IPX_CU(cudaGraphCreate(&graph, 0));
     cudaGraphConditionalHandle handle;
     IPX_CU(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
     cudaGraphNodeParams params = {};
@@ -661,7 +699,7 @@ static int ipx_build_graph_loop()
     params.conditional.size = 1;
     cudaGraphNode_t node;
     IPX_CU(cudaGraphAddNode(&node, graph, nullptr, 0, &params));
-    body = params.conditional.phGraph_out[0];
+    cudaGraph_t body = params.conditional.phGraph_out[0];
     const bool prof = ipx_h.profile;
     ipx_h.profile = false; /* no event nodes inside the body */
     uint64_t before[IPX_K_N];
@@ -676,15 +714,23 @@ static int ipx_build_graph_loop()
         ipx_h.body_launches[k] = ipx_h.prof_launches[k] - before[k];
         ipx_h.prof_launches[k] = before[k];
     }
+    if (r != IPG_OK) return r;
+    if (e != cudaSuccess) return ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
+    return IPG_OK;
+}
+
+/* The library's own captured loop: built once per attached graph. */
+static int ipx_build_graph_loop()
+{
+    if (ipx_h.gexec) return IPG_OK;
+    cudaGraph_t graph = nullptr;
+    IPX_CU(cudaGraphCreate(&graph, 0));
+    int r = ipx_add_loop_node(graph);
     if (r != IPG_OK) {
         cudaGraphDestroy(graph);
         return r;
     }
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
-    }
-    e = cudaGraphInstantiate(&ipx_h.gexec, graph, 0);
+    cudaError_t e = cudaGraphInstantiate(&ipx_h.gexec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
         ipx_h.gexec = nullptr;
@@ -693,26 +739,30 @@ static int ipx_build_graph_loop()
     return IPG_OK;
 }
 
-static int ipx_run_graph_loop()
+/* Before a launch of a captured loop: superstep 0 on the device. */
+static int ipx_loop_prepare()
 {
-#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
-    if (ip_active_vertices == 0) return IPG_OK;
-#endif
-    IPX_OK(ipx_build_graph_loop());
-    cudaStream_t st = ipx_h.st;
-    IPX_OK(ipx_set_superstep(0));
-    IPX_CU(cudaEventRecord(ipx_h.ev0, st));
-    IPX_CU(cudaGraphLaunch(ipx_h.gexec, st));
-    IPX_CU(cudaEventRecord(ipx_h.ev1, st));
-    IPX_CU(cudaEventSynchronize(ipx_h.ev1));
-    IPX_CU(cudaGetLastError());
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
+    if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
+    ipx_h.dirty = true;
+    size_t zero = 0;
+    IPX_CU(cudaMemcpyToSymbol(ipd_superstep, &zero, sizeof zero));
+    return IPG_OK;
+}
+
+/* After a captured loop ran: the supersteps, their counts and the error word
+ * from the device; `seconds` is the loop's device time. */
+static int ipx_loop_collect(double seconds)
+{
     size_t S = 0;
     IPX_CU(cudaMemcpyFromSymbol(&S, ipd_superstep, sizeof S));
     uint32_t err = 0;
     IPX_CU(cudaMemcpy(&err, ipx_h.c.err, 4, cudaMemcpyDeviceToHost));
-    float ms = 0.f;
-    IPX_CU(cudaEventElapsedTime(&ms, ipx_h.ev0, ipx_h.ev1));
-    ipx_h.total_seconds = ms * 1e-3;
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    /* while(ip_active_vertices != 0): no superstep at all without vertices */
+    if (ipx_h.c.V == 0) S = 0;
+#endif
+    ipx_h.total_seconds = seconds;
     const uint64_t kept = S < IPX_HIST ? S : IPX_HIST;
     std::vector<unsigned long long> hist(kept * 4);
     if (kept) IPX_CU(cudaMemcpy(hist.data(), ipx_h.c.hist, kept * 4 * 8, cudaMemcpyDeviceToHost));
@@ -732,6 +782,7 @@ static int ipx_run_graph_loop()
     ipx_h.graph_launches++;
     ip_superstep = S;
     ip_active_vertices = ipx_h.counts.empty() ? 0 : ipx_h.counts.back();
+    ipx_h.host_valid = false;
     if (err & IPX_ERR_SEND_IN_BROADCAST)
         return ipx_fail(IPG_EDEVICE,
                         "The function send_message should not be used in the SINGLE_BROADCAST version; only "
@@ -739,6 +790,24 @@ static int ipx_run_graph_loop()
     if (err & IPX_ERR_SUPERSTEP_LIMIT) return ipx_fail(IPG_EDEVICE, "superstep limit (IPG_MAX_SUPERSTEPS) reached");
     if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
     return IPG_OK;
+}
+
+static int ipx_run_graph_loop()
+{
+#if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
+    if (ip_active_vertices == 0) return IPG_OK;
+#endif
+    IPX_OK(ipx_build_graph_loop());
+    cudaStream_t st = ipx_h.st;
+    IPX_OK(ipx_set_superstep(0));
+    IPX_CU(cudaEventRecord(ipx_h.ev0, st));
+    IPX_CU(cudaGraphLaunch(ipx_h.gexec, st));
+    IPX_CU(cudaEventRecord(ipx_h.ev1, st));
+    IPX_CU(cudaEventSynchronize(ipx_h.ev1));
+    IPX_CU(cudaGetLastError());
+    float ms = 0.f;
+    IPX_CU(cudaEventElapsedTime(&ms, ipx_h.ev0, ipx_h.ev1));
+    return ipx_loop_collect(ms * 1e-3);
 }
 
 static int ipx_run_impl()
@@ -1072,6 +1141,52 @@ int ipg_app_set_graph_loop(int on)
 
 int ipg_app_graph_loop(void) { return ipx_h.graph_loop ? 1 : 0; }
 
+/* Tuning of the superstep kernels, applied at the next attach: CTA size
+ * (a multiple of 32, at most 256), degree-class thresholds t0 <= t1 (thread
+ * per vertex up to t0 edges, warp up to t1, CTAs beyond) and the push
+ * versions' pull switch (pull when the broadcasters' edges exceed
+ * E / pull_div; 0 never; needs a symmetric graph or a directed one). */
+int ipg_app_set_tuning(int block, uint64_t t0, uint64_t t1, uint64_t pull_div)
+{
+    if (block < 32 || block > IPX_THREADS || (block & 31))
+        return ipx_fail(IPG_EINVAL, "ipg_app_set_tuning: block must be a multiple of 32 in [32, 256]");
+    if (t0 < 1 || t1 < t0) return ipx_fail(IPG_EINVAL, "ipg_app_set_tuning: need 1 <= t0 <= t1");
+    ipx_h.tune.block = block;
+    ipx_h.tune.t0 = t0;
+    ipx_h.tune.t1 = t1;
+    ipx_h.tune.pull_div = pull_div;
+    return IPG_OK;
+}
+
+/* Several applications' loops in one CUDA graph launch.  ipg_app_loop_add
+ * adds this library's superstep loop (a while node over one superstep's
+ * kernels, its condition evaluated on the device) as a root node of the
+ * caller's cudaGraph_t; nodes of different libraries share no dependency
+ * and may run concurrently.  Before every launch of the caller's graph call
+ * ipg_app_loop_prepare (resets the vertex state, superstep 0); after it
+ * completed, ipg_app_loop_collect with the launch's device time (reads the
+ * superstep history and the error word, as ip_run would report them).  The
+ * node belongs to the attached graph: attach again, add again. */
+int ipg_app_loop_add(void* cuda_graph)
+{
+    if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ipg_app_loop_add: no graph attached");
+    if (!cuda_graph) return ipx_fail(IPG_EINVAL, "ipg_app_loop_add: null graph");
+    return ipx_add_loop_node((cudaGraph_t)cuda_graph);
+}
+
+int ipg_app_loop_prepare(void) { return ipx_loop_prepare(); }
+
+int ipg_app_loop_collect(double seconds) { return ipx_loop_collect(seconds); }
+
+int ipg_app_get_tuning(int* block, uint64_t* t0, uint64_t* t1, uint64_t* pull_div)
+{
+    if (block) *block = ipx_h.tune.block;
+    if (t0) *t0 = ipx_h.tune.t0;
+    if (t1) *t1 = ipx_h.tune.t1;
+    if (pull_div) *pull_div = ipx_h.tune.pull_div;
+    return IPG_OK;
+}
+
 void ipg_app_profile_reset(void)
 {
     for (int k = 0; k < IPX_K_N; k++) {
@@ -1109,6 +1224,21 @@ int ipg_app_set_param(const char* key, double value)
     (void)key;
     (void)value;
     return ipx_fail(IPG_EINVAL, "this application takes no parameters");
+#endif
+}
+
+/* A named device array for the application (e.g. batch offsets); the
+ * caller keeps it alive while runs use it. */
+int ipg_app_set_param_ptr(const char* key, const void* ptr, uint64_t n)
+{
+#ifdef IP_APP_PARAM_PTRS
+    if (ip_app_set_param_ptr(key, ptr, n) != 0) return ipx_fail(IPG_EINVAL, "unknown array parameter");
+    return IPG_OK;
+#else
+    (void)key;
+    (void)ptr;
+    (void)n;
+    return ipx_fail(IPG_EINVAL, "this application takes no array parameters");
 #endif
 }
 

@@ -43,7 +43,8 @@ RUNTIME_SYMBOLS = (
     "ipg_graph_to_host", "ipg_graph_write", "ipg_graph_free",
     "ipg_graph_bins", "ipg_degree_classes_noalloc", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
     "ipg_graph_set_directed", "ipg_memcpy", "ipg_pr_plan_create", "ipg_pr_plan_free", "ipg_pr_plan_info", "ipg_pr_run_f32",
-    "ipg_error_f32_f64",
+    "ipg_error_f32_f64", "ipg_graph_concat", "ipg_fused_create", "ipg_fused_graph", "ipg_fused_launch",
+    "ipg_fused_free",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -57,7 +58,8 @@ APP_SYMBOLS = (
     "ipg_app_run", "ipg_app_values", "ipg_app_values_device", "ipg_app_supersteps", "ipg_app_counts",
     "ipg_app_stats", "ipg_app_stream", "ipg_app_set_quiet", "ipg_app_set_param", "ipg_app_release",
     "ipg_app_set_profile", "ipg_app_profile_reset", "ipg_app_launches", "ipg_app_profile", "ipg_app_main",
-    "ipg_app_set_graph_loop", "ipg_app_graph_loop",
+    "ipg_app_set_graph_loop", "ipg_app_graph_loop", "ipg_app_set_tuning", "ipg_app_get_tuning",
+    "ipg_app_loop_add", "ipg_app_loop_prepare", "ipg_app_loop_collect", "ipg_app_set_param_ptr",
 )
 
 
@@ -115,6 +117,13 @@ def runtime():
         L.ipg_device_info.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(u64),
                                       ctypes.POINTER(ctypes.c_int)]
         L.ipg_memcpy.argtypes = [vp, vp, u64]
+        L.ipg_graph_concat.argtypes = [vp, ctypes.c_uint32, i32, i32, ctypes.POINTER(vp), vp, vp]
+        L.ipg_fused_create.argtypes = [ctypes.POINTER(vp)]
+        L.ipg_fused_graph.argtypes = [vp]
+        L.ipg_fused_graph.restype = vp
+        L.ipg_fused_launch.argtypes = [vp, vp, ctypes.POINTER(dbl)]
+        L.ipg_fused_free.argtypes = [vp]
+        L.ipg_fused_free.restype = None
         L.ipg_pr_plan_create.argtypes = [vp, ctypes.POINTER(vp)]
         L.ipg_pr_plan_free.argtypes = [vp]
         L.ipg_pr_plan_free.restype = None
@@ -268,6 +277,19 @@ class Graph:
         return cls(h.value)
 
     @classmethod
+    def concat(cls, parts, directed=False, need_in=False):
+        """Disjoint union (ipg_graph_concat): (graph, vertex offsets, edge
+        offsets), the offsets with len(parts) + 1 entries."""
+        n = len(parts)
+        arr = (ctypes.c_void_p * n)(*[p.handle for p in parts])
+        voff = np.zeros(n + 1, dtype=np.uint64)
+        eoff = np.zeros(n + 1, dtype=np.uint64)
+        h = ctypes.c_void_p()
+        _check(runtime().ipg_graph_concat(arr, n, int(directed), int(need_in), ctypes.byref(h), voff.ctypes.data,
+                                          eoff.ctypes.data), where="ipg_graph_concat")
+        return cls(h.value), voff, eoff
+
+    @classmethod
     def generate_er(cls, n, m, seed=1, undirected=False, wmax=0, need_in=False):
         h = ctypes.c_void_p()
         _check(runtime().ipg_graph_generate_er(n, m, seed, int(undirected), wmax, int(need_in), ctypes.byref(h)),
@@ -352,6 +374,9 @@ class Engine:
     life cycle of the reference, on in-memory graphs."""
 
     _loaded = {}
+    # attach generation of every library: a fused launch captured under one
+    # attach must not run after another (its kernels hold the old state)
+    _generation = {}
 
     def __init__(self, app: str, version: str = "combiner", id_bits: int = 32, generic: bool = False):
         if version not in VERSIONS:
@@ -379,8 +404,14 @@ class Engine:
             L.ipg_app_launches.restype = u64
             L.ipg_app_profile.argtypes = [ctypes.c_char_p, ctypes.c_int]
             L.ipg_app_profile_reset.restype = None
+            L.ipg_app_set_tuning.argtypes = [ctypes.c_int, u64, u64, u64]
+            L.ipg_app_get_tuning.argtypes = [vp, vp, vp, vp]
+            L.ipg_app_loop_add.argtypes = [vp]
+            L.ipg_app_loop_collect.argtypes = [ctypes.c_double]
+            L.ipg_app_set_param_ptr.argtypes = [ctypes.c_char_p, vp, u64]
             Engine._loaded[path] = L
         self.lib = Engine._loaded[path]
+        self.path = path
         self.app, self.version, self.id_bits = app, version, id_bits
         self.info = self.describe()
         self.graph = None
@@ -405,13 +436,22 @@ class Engine:
     def set_param(self, key, value):
         self._check(self.lib.ipg_app_set_param(key.encode(), float(value)), f"set_param({key})")
 
+    def _bump(self):
+        Engine._generation[self.path] = Engine._generation.get(self.path, 0) + 1
+
+    @property
+    def generation(self) -> int:
+        return Engine._generation.get(self.path, 0)
+
     def attach(self, graph: Graph):
         self.graph = graph
+        self._bump()
         self._check(self.lib.ipg_app_attach(graph.handle), "ipg_app_attach")
 
     def load_host(self, V, E, idx, adj, wgt=None, directed=False):
         """ip_init from host buffers (idx = V row starts, u64; adj = ids)."""
         self.graph = None
+        self._bump()
         self._check(self.lib.ipg_app_load_host(int(V), int(E), _ptr(idx), _ptr(adj), _ptr(wgt), int(directed)),
                     "ipg_app_load_host")
 
@@ -459,6 +499,31 @@ class Engine:
     def graph_loop(self) -> bool:
         return bool(self.lib.ipg_app_graph_loop())
 
+    def set_tuning(self, block=256, t0=16, t1=4096, pull_div=0):
+        """CTA size, degree-class thresholds and pull switch of the superstep
+        kernels; applied at the next attach."""
+        self._check(self.lib.ipg_app_set_tuning(int(block), int(t0), int(t1), int(pull_div)), "ipg_app_set_tuning")
+
+    def tuning(self) -> dict:
+        b = ctypes.c_int()
+        t0, t1, pd = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.lib.ipg_app_get_tuning(ctypes.byref(b), ctypes.byref(t0), ctypes.byref(t1), ctypes.byref(pd))
+        return {"block": b.value, "t0": t0.value, "t1": t1.value, "pull_div": pd.value}
+
+    def set_param_ptr(self, key, ptr, n):
+        """A named device array (e.g. "batch_offsets" of weighted SSSP)."""
+        self._check(self.lib.ipg_app_set_param_ptr(key.encode(), ptr, int(n)), f"set_param_ptr({key})")
+
+    def loop_add(self, fused: "Fused"):
+        """Adds this engine's captured superstep loop to a fused launch."""
+        self._check(self.lib.ipg_app_loop_add(fused.cuda_graph), "ipg_app_loop_add")
+
+    def loop_prepare(self):
+        self._check(self.lib.ipg_app_loop_prepare(), "ipg_app_loop_prepare")
+
+    def loop_collect(self, seconds: float):
+        self._check(self.lib.ipg_app_loop_collect(float(seconds)), "ipg_app_loop_collect")
+
     def launches(self) -> int:
         """Kernel launches of this application library since the last reset."""
         return int(self.lib.ipg_app_launches())
@@ -480,6 +545,7 @@ class Engine:
         return RunResult(vals, self.counts(), sec, edges, n)
 
     def release(self):
+        self._bump()
         self.lib.ipg_app_release()
         self.graph = None
 
@@ -513,6 +579,49 @@ def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, 
         eng.set_param(k, v)
     eng.attach(graph)
     return eng.run()
+
+
+class Fused:
+    """One CUDA graph holding several engines' captured superstep loops
+    (ipg_fused_*): loop_add each engine, then run()."""
+
+    def __init__(self):
+        p = ctypes.c_void_p()
+        _check(runtime().ipg_fused_create(ctypes.byref(p)), where="ipg_fused_create")
+        self._p = p
+        self.engines = []
+
+    @property
+    def cuda_graph(self):
+        return runtime().ipg_fused_graph(self._p)
+
+    def add(self, engine: "Engine"):
+        engine.loop_add(self)
+        self.engines.append((engine, engine.generation))
+
+    def run(self, stream=None) -> float:
+        """prepare, one launch, collect; returns the launch's device seconds."""
+        for e, gen in self.engines:
+            if e.generation != gen:
+                raise IPregelError(f"{e.app}/{e.version} was attached again after it joined this fused launch")
+        for e, _ in self.engines:
+            e.loop_prepare()
+        sec = ctypes.c_double()
+        _check(runtime().ipg_fused_launch(self._p, stream, ctypes.byref(sec)), where="ipg_fused_launch")
+        for e, _ in self.engines:
+            e.loop_collect(sec.value)
+        return sec.value
+
+    def free(self):
+        if self._p is not None and self._p.value:
+            runtime().ipg_fused_free(self._p)
+        self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class PageRankF32:

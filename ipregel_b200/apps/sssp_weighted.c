@@ -5,6 +5,11 @@
  * broadcast extension (IP_BROADCAST_EDGE_MESSAGE) adds each out-edge's weight
  * on delivery, so each neighbour w hears dist + weight(v, w).  Min combines,
  * and (a + w) distributes over min, as the extension requires.
+ *
+ * Batch mode: with the parameter "batch_offsets" (the vertex offsets of a
+ * disjoint union of graphs, ipg_graph_concat, on the device) every part's
+ * vertex `source` (a local id) is a source, so one run computes every part's
+ * shortest paths.
  */
 #include <limits.h>
 #include <stdint.h>
@@ -18,16 +23,31 @@ typedef uint32_t IP_EDGE_WEIGHT_TYPE;
 #define IP_NEEDS_OUT_NEIGHBOUR_WEIGHTS
 #define IP_BROADCAST_EDGE_MESSAGE(m, w) ((IP_MESSAGE_TYPE)((m) + (w)))
 #define IP_APP_PARAMS
+#define IP_APP_PARAM_PTRS
 #include "iPregel.h"
 
 IP_GLOBAL IP_VERTEX_ID_TYPE sssp_source = 0;
+IP_GLOBAL const uint64_t* sssp_batch = NULL; /* parts + 1 vertex offsets, or NULL */
+IP_GLOBAL uint64_t sssp_batch_parts = 0;
+
+IP_DEVICE static bool sssp_is_source(uint64_t id)
+{
+    if (!sssp_batch) return id == (uint64_t)sssp_source;
+    uint64_t lo = 0, hi = sssp_batch_parts; /* sssp_batch[lo] <= id < sssp_batch[hi] */
+    while (hi - lo > 1) {
+        uint64_t mid = (lo + hi) / 2;
+        if (sssp_batch[mid] <= id) lo = mid;
+        else hi = mid;
+    }
+    return id == sssp_batch[lo] + (uint64_t)sssp_source && id < sssp_batch[lo + 1];
+}
 
 IP_DEVICE void ip_compute(struct ip_vertex_t* v)
 {
     IP_MESSAGE_TYPE best = UINT_MAX;
     if (ip_is_first_superstep()) {
         v->value = UINT_MAX;
-        if (v->id == sssp_source) best = 0;
+        if (sssp_is_source(v->id)) best = 0;
     } else {
         IP_MESSAGE_TYPE m;
         while (ip_get_next_message(v, &m))
@@ -54,6 +74,15 @@ int ip_app_set_param(const char* key, double value)
 {
     if (strcmp(key, "source") != 0) return -1;
     sssp_source = (IP_VERTEX_ID_TYPE)value;
+    return 0;
+}
+
+int ip_app_set_param_ptr(const char* key, const void* ptr, uint64_t n)
+{
+    if (strcmp(key, "batch_offsets") != 0) return -1;
+    sssp_batch = (const uint64_t*)ptr;
+    sssp_batch_parts = (ptr && n > 1) ? n - 1 : 0;
+    if (!sssp_batch_parts) sssp_batch = NULL;
     return 0;
 }
 

@@ -573,6 +573,132 @@ extern "C" int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_r
     return finalize(g, need_in, out);
 }
 
+// ---------------------------------------------------------------------------
+// Disjoint union of graphs: concatenated CSR with offset tables.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_offset_copy(const T* __restrict__ src, T* __restrict__ dst, uint64_t n, T add)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i] + add;
+}
+
+extern "C" int ipg_graph_concat(ipg_graph* const* parts, uint32_t count, int directed, int need_in, ipg_graph** out,
+                                uint64_t* voff, uint64_t* eoff)
+{
+    if (!out || (count && !parts)) return fail(IPG_EINVAL, "ipg_graph_concat: null argument");
+    *out = nullptr;
+    if (count == 0) return fail(IPG_EINVAL, "ipg_graph_concat: no graphs");
+    const int id_bytes = parts[0] ? parts[0]->v.id_bytes : 0;
+    const int wb = parts[0] ? parts[0]->v.weight_bytes : 0;
+    uint64_t V = 0, E = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        const ipg_graph* p = parts[i];
+        if (!p) return fail(IPG_EINVAL, "ipg_graph_concat: graph %u is null", i);
+        if (p->v.id_bytes != id_bytes) return fail(IPG_EINVAL, "ipg_graph_concat: graph %u has another id width", i);
+        if (p->v.weight_bytes != wb && p->v.E)
+            return fail(IPG_EINVAL, "ipg_graph_concat: graph %u has another weight width", i);
+        if (voff) voff[i] = V;
+        if (eoff) eoff[i] = E;
+        V += p->v.V;
+        E += p->v.E;
+    }
+    if (voff) voff[count] = V;
+    if (eoff) eoff[count] = E;
+    if (id_bytes == 4 && V >= (1ULL << 32)) return fail(IPG_EINVAL, "ipg_graph_concat: more than 2^32-1 vertices");
+    ipg_graph* g = new ipg_graph();
+    g->v.directed = directed;
+    int r = alloc_out(g, V, E, id_bytes, wb);
+    uint64_t v0 = 0, e0 = 0;
+    for (uint32_t i = 0; i < count && r == IPG_OK; i++) {
+        const ipg_graph* p = parts[i];
+        const uint64_t n = p->v.V, m = p->v.E;
+        if (n)
+            k_offset_copy<uint64_t><<<grid_for(n, 256), 256>>>(p->v.d_row, (uint64_t*)g->row + v0, n, e0);
+        if (m) {
+            if (id_bytes == 4)
+                k_offset_copy<uint32_t><<<grid_for(m, 256), 256>>>((const uint32_t*)p->v.d_adj,
+                                                                   (uint32_t*)g->adj + e0, m, (uint32_t)v0);
+            else
+                k_offset_copy<uint64_t><<<grid_for(m, 256), 256>>>((const uint64_t*)p->v.d_adj,
+                                                                   (uint64_t*)g->adj + e0, m, v0);
+            if (wb) {
+                cudaError_t e = cudaMemcpyAsync((char*)g->wgt + e0 * wb, p->v.d_wgt, m * (uint64_t)wb,
+                                                cudaMemcpyDeviceToDevice, 0);
+                if (e != cudaSuccess) r = fail(IPG_ECUDA, "ipg_graph_concat: %s", cudaGetErrorString(e));
+            }
+        }
+        if (cudaGetLastError() != cudaSuccess) r = fail(IPG_ECUDA, "ipg_graph_concat: copy kernel failed");
+        v0 += n;
+        e0 += m;
+    }
+    if (r == IPG_OK) {
+        k_fill_u64<<<1, 32>>>((uint64_t*)g->row + V, 1, E);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) r = fail(IPG_ECUDA, "ipg_graph_concat: %s", cudaGetErrorString(e));
+    }
+    if (r != IPG_OK) {
+        delete g;
+        return r;
+    }
+    // symmetric parts give a symmetric union
+    bool sym = true;
+    for (uint32_t i = 0; i < count; i++) sym = sym && parts[i]->v.symmetric;
+    g->v.symmetric = sym ? 1 : 0;
+    return finalize(g, need_in, out);
+}
+
+// ---------------------------------------------------------------------------
+// One CUDA graph holding several applications' superstep loops.
+// ---------------------------------------------------------------------------
+struct ipg_fused {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+extern "C" void ipg_fused_free(ipg_fused* f)
+{
+    if (!f) return;
+    if (f->exec) cudaGraphExecDestroy(f->exec);
+    if (f->graph) cudaGraphDestroy(f->graph);
+    for (auto e : f->ev)
+        if (e) cudaEventDestroy(e);
+    delete f;
+}
+
+extern "C" int ipg_fused_create(ipg_fused** out)
+{
+    if (!out) return fail(IPG_EINVAL, "ipg_fused_create: null output");
+    ipg_fused* f = new ipg_fused();
+    cudaError_t e = cudaGraphCreate(&f->graph, 0);
+    if (e == cudaSuccess) e = cudaEventCreate(&f->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&f->ev[1]);
+    if (e != cudaSuccess) {
+        ipg_fused_free(f);
+        return fail(IPG_ECUDA, "ipg_fused_create: %s", cudaGetErrorString(e));
+    }
+    *out = f;
+    return IPG_OK;
+}
+
+extern "C" void* ipg_fused_graph(ipg_fused* f) { return f ? (void*)f->graph : nullptr; }
+
+extern "C" int ipg_fused_launch(ipg_fused* f, void* stream, double* seconds)
+{
+    if (!f) return fail(IPG_EINVAL, "ipg_fused_launch: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!f->exec) IPG_CUDA(cudaGraphInstantiate(&f->exec, f->graph, 0));
+    IPG_CUDA(cudaEventRecord(f->ev[0], st));
+    IPG_CUDA(cudaGraphLaunch(f->exec, st));
+    IPG_CUDA(cudaEventRecord(f->ev[1], st));
+    IPG_CUDA(cudaEventSynchronize(f->ev[1]));
+    float ms = 0.f;
+    IPG_CUDA(cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]));
+    if (seconds) *seconds = ms * 1e-3;
+    return IPG_OK;
+}
+
 // Parallel pread of [off, off+bytes) into dst.
 static int read_range(int fd, uint64_t off, uint64_t bytes, void* dst)
 {
