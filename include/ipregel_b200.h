@@ -254,6 +254,57 @@ int ipg_pr_run_f32(ipg_pr_plan* plan, uint32_t rounds, double damping, int compe
 int ipg_error_f32_f64(const float* d_a, const double* d_ref, uint64_t n, double* max_abs,
                       double* max_rel, double* mean_abs, uint64_t* argmax_abs, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Request server -- no counterpart in the reference (one program, one graph
+ * per process).  Resident graphs (32-bit ids, u32 weights for SSSP) answer
+ * single-source shortest-path, connected-component and personalised-PageRank
+ * queries.  Concurrent queries on one graph run as lanes of one fused
+ * superstep kernel (64 min-plus lanes for SSSP and CC, 16 FP32 lanes for
+ * PPR); queries join free lanes whenever their group finishes a superstep
+ * (continuous batching), and lane groups plus result buffers are admitted
+ * under an HBM budget.  Results: u32 per vertex (SSSP distance, UINT32_MAX
+ * unreached; CC label = least vertex id reaching it, as benchmarks/cc.c), or
+ * f32 per vertex (PPR after `ppr_rounds` gathers, as the ppr application).
+ * ------------------------------------------------------------------------ */
+typedef struct ipg_server ipg_server;
+enum ipg_query_kind { IPG_QUERY_SSSP = 0, IPG_QUERY_PPR = 1, IPG_QUERY_CC = 2 };
+enum ipg_query_state { IPG_QUERY_PENDING = 0, IPG_QUERY_RUNNING = 1, IPG_QUERY_FINISHING = 2, IPG_QUERY_DONE = 3 };
+typedef struct ipg_server_stats {
+    uint64_t submitted;
+    uint64_t lanes_admitted;     /* CC queries admitted together share a lane */
+    uint64_t supersteps;         /* fused supersteps launched, all groups */
+    uint64_t kernel_launches;    /* superstep kernels launched */
+    uint64_t groups_created;
+    uint64_t groups_freed;
+    uint64_t bytes_in_use;       /* lane groups and result buffers */
+    uint64_t peak_bytes;
+} ipg_server_stats;
+
+/* hbm_budget: bytes for lane groups and results (0 = unbounded). */
+int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_server** out);
+void ipg_server_free(ipg_server* srv);
+/* The graph stays owned by the caller and must outlive the server. */
+int ipg_server_add_graph(ipg_server* srv, ipg_graph* g, int* gid);
+int ipg_server_submit(ipg_server* srv, int gid, int kind, uint64_t source, uint64_t* qid);
+/* One scheduling pass: completed supersteps retire lanes, pending queries
+ * take free lanes, next supersteps are launched.  Non-blocking.
+ * *outstanding = queries not yet done. */
+int ipg_server_poll(ipg_server* srv, uint64_t* outstanding);
+/* State; latency (submit to result on the device) and queueing time, s. */
+int ipg_server_query(ipg_server* srv, uint64_t qid, int* state, double* latency, double* queued);
+int ipg_server_result(ipg_server* srv, uint64_t qid, void* host_out, uint64_t cap_bytes);
+int ipg_server_result_device(ipg_server* srv, uint64_t qid, const void** d_ptr, uint64_t* bytes);
+/* Forgets a done query; its result buffer returns to the server's pool. */
+int ipg_server_release(ipg_server* srv, uint64_t qid);
+int ipg_server_get_stats(ipg_server* srv, ipg_server_stats* out);
+/* Replays an arrival trace in real time (arrival[i] seconds from the start,
+ * ascending): submits each query at its time, polls until all are done.
+ * latency[i] counts from the scheduled arrival; keep_results = 0 releases
+ * each result on completion. */
+int ipg_server_run_trace(ipg_server* srv, uint64_t n, const double* arrival, const int* gid,
+                         const int* kind, const uint64_t* source, int keep_results,
+                         uint64_t* qids, double* latency, double* makespan);
+
 #ifdef __cplusplus
 }
 #endif

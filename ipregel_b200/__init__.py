@@ -44,7 +44,9 @@ RUNTIME_SYMBOLS = (
     "ipg_graph_bins", "ipg_degree_classes_noalloc", "ipg_compact", "ipg_bitmap_popc_or", "ipg_sm_count",
     "ipg_graph_set_directed", "ipg_memcpy", "ipg_pr_plan_create", "ipg_pr_plan_free", "ipg_pr_plan_info", "ipg_pr_run_f32",
     "ipg_error_f32_f64", "ipg_graph_concat", "ipg_fused_create", "ipg_fused_graph", "ipg_fused_launch",
-    "ipg_fused_free",
+    "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
+    "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
+    "ipg_server_get_stats", "ipg_server_run_trace",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.

@@ -1,0 +1,1047 @@
+// serve.cu -- a request server over resident graphs (no counterpart in the
+// reference, which runs one program on one graph per process).
+//
+// Queries: single-source shortest paths (integer weights), connected
+// components (min-label propagation, as benchmarks/cc.c), and personalised
+// PageRank (x' = 0.15 [v == seed] + 0.85 * sum of x_u / deg u over the row,
+// as the ppr application, in FP32 with compensated sums).  Graphs and
+// per-query vertex state stay in HBM.  Concurrent queries on one graph share
+// a lane group and advance together, one fused superstep kernel for all
+// their lanes:
+//
+//   min-plus group (SSSP, CC): 64 lanes; dist[v][lane] (u32, 256 bytes per
+//     vertex, so the lanes of one vertex are one coalesced line), a bit-packed
+//     frontier mask per vertex (u64, a bit per lane) double-buffered, and the
+//     frontier as degree-class lists.  A warp relaxes one edge for 32 lanes
+//     at a time: nd = dist[v][k] + w (w = 0 for a CC lane), atomicMin into
+//     dist[u][k], improved lanes OR-ed into u's next mask.  A lane whose
+//     frontier empties is finished.
+//   PPR group: 16 lanes; the broadcast quotients b[v][lane] = x/deg (FP32,
+//     64 bytes per vertex) double-buffered; a pull gather over every row,
+//     each half-warp summing 16 lanes of one in-neighbour.  A lane runs
+//     exactly `rounds` gathers after admission and writes its last values
+//     into the query's result buffer.
+//
+// Continuous batching: each group advances on its own stream; whenever its
+// superstep has completed, finished lanes retire and pending queries take the
+// free lanes before the next superstep is launched, so queries join and leave
+// while others are in flight, and groups of different graphs overlap on the
+// device.  A lane's arithmetic depends on nothing but its own query (min-plus
+// is order independent; the PPR sums run in a fixed per-vertex order), so a
+// query's result is the same alone and in any mix.
+//
+// Admission is bounded by an HBM budget over the server's lane groups and
+// result buffers; groups without busy lanes are freed, least recently used
+// first, when a new group needs room.
+#include "ipregel_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <vector>
+
+extern "C" int ipg_internal_fail(int code, const char* msg);
+
+namespace {
+
+constexpr int MP_K = 64;
+constexpr int PP_K = 16;
+constexpr int SRV_THREADS = 256;
+constexpr uint64_t MP_T0 = 64, MP_T1 = 4096;
+constexpr uint32_t HUB_CHUNK = 1024;
+constexpr uint32_t SRV_INF = 0xffffffffu;
+constexpr unsigned FULL = 0xffffffffu;
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------------------
+// Shared helpers
+// ---------------------------------------------------------------------------
+
+// prefix[i] = sum over j < i of ceil(deg(list[j]) / HUB_CHUNK); prefix[n] = total.
+__global__ void __launch_bounds__(1024) k_chunk_prefix(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                                       const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix)
+{
+    __shared__ uint32_t s[1024];
+    __shared__ uint32_t carry;
+    const uint32_t n = *count;
+    const int t = threadIdx.x;
+    if (t == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < n; base += 1024) {
+        const uint32_t i = base + t;
+        uint32_t c = 0;
+        if (i < n) {
+            const uint64_t v = list[i];
+            c = (uint32_t)((row[v + 1] - row[v] + HUB_CHUNK - 1) / HUB_CHUNK);
+        }
+        s[t] = c;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const uint32_t x = t >= off ? s[t - off] : 0;
+            __syncthreads();
+            s[t] += x;
+            __syncthreads();
+        }
+        if (i < n) prefix[i] = carry + s[t] - c;
+        __syncthreads();
+        if (t == 1023) carry += s[1023];
+        __syncthreads();
+    }
+    if (t == 0) prefix[n] = carry;
+}
+
+__device__ __forceinline__ uint32_t hub_of_chunk(const uint32_t* __restrict__ prefix, uint32_t n, uint32_t c)
+{
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (prefix[mid] <= c) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Min-plus lanes (SSSP, CC)
+// ---------------------------------------------------------------------------
+struct MpArgs {
+    const uint64_t* __restrict__ row;
+    const uint32_t* __restrict__ adj;
+    const uint32_t* __restrict__ wgt;  // null for an unweighted graph (CC only)
+    uint32_t* __restrict__ dist;
+    const uint64_t* __restrict__ front;
+    uint64_t* __restrict__ next;
+    uint32_t* __restrict__ fbm;        // bit per vertex: next mask became nonzero
+    unsigned long long* __restrict__ any;
+    uint64_t wmask;                    // lanes whose edges carry their weight (SSSP)
+};
+
+// One warp relaxes the edges [e0, e1) of v for all of v's frontier lanes.
+__device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e0, uint64_t e1,
+                                         unsigned long long& any_acc)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t M = a.front[v];
+    if (!M) return;
+    const uint32_t Mlo = (uint32_t)M, Mhi = (uint32_t)(M >> 32);
+    const bool act0 = (Mlo >> lane) & 1u, act1 = (Mhi >> lane) & 1u;
+    const bool w0 = ((uint32_t)a.wmask >> lane) & 1u, w1 = ((uint32_t)(a.wmask >> 32) >> lane) & 1u;
+    const uint32_t d0 = act0 ? a.dist[v * MP_K + lane] : SRV_INF;
+    const uint32_t d1 = act1 ? a.dist[v * MP_K + 32 + lane] : SRV_INF;
+    for (uint64_t e = e0; e < e1; e += 32) {
+        const uint64_t ee = e + lane;
+        const uint32_t wj = ee < e1 ? a.adj[ee] : 0u;
+        const uint32_t tj = (ee < e1 && a.wgt) ? a.wgt[ee] : 0u;
+        const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
+        for (int j0 = 0; j0 < nj; j0 += 4) {
+            uint32_t u[4], t[4], c0[4], c1[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                u[q] = __shfl_sync(FULL, wj, (j0 + q) & 31);
+                t[q] = __shfl_sync(FULL, tj, (j0 + q) & 31);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const bool ok = j0 + q < nj;
+                c0[q] = (ok && act0) ? a.dist[(uint64_t)u[q] * MP_K + lane] : 0u;
+                c1[q] = (ok && act1) ? a.dist[(uint64_t)u[q] * MP_K + 32 + lane] : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (j0 + q >= nj) break;
+                bool i0 = false, i1 = false;
+                if (act0) {
+                    const uint32_t nd = d0 + (w0 ? t[q] : 0u);
+                    if (nd < c0[q]) i0 = nd < atomicMin(&a.dist[(uint64_t)u[q] * MP_K + lane], nd);
+                }
+                if (act1) {
+                    const uint32_t nd = d1 + (w1 ? t[q] : 0u);
+                    if (nd < c1[q]) i1 = nd < atomicMin(&a.dist[(uint64_t)u[q] * MP_K + 32 + lane], nd);
+                }
+                const uint32_t b0 = Mlo ? __ballot_sync(FULL, i0) : 0u;
+                const uint32_t b1 = Mhi ? __ballot_sync(FULL, i1) : 0u;
+                if ((b0 | b1) && lane == 0) {
+                    const unsigned long long bits = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+                    const unsigned long long old = atomicOr((unsigned long long*)&a.next[u[q]], bits);
+                    if (!old) atomicOr(&a.fbm[u[q] >> 5], 1u << (u[q] & 31));
+                    any_acc |= bits;
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void mp_block_any(unsigned long long x, unsigned long long* any)
+{
+    for (int o = 16; o > 0; o >>= 1) x |= __shfl_down_sync(FULL, x, o);
+    __shared__ unsigned long long s[SRV_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t |= s[w];
+        if (t) atomicOr(any, t);
+    }
+}
+
+// A warp per frontier vertex (classes 0 and 1).
+__global__ void __launch_bounds__(SRV_THREADS) k_mp_vertices(MpArgs a, const uint32_t* __restrict__ list,
+                                                             const uint32_t* __restrict__ count)
+{
+    const uint32_t n = *count;
+    unsigned long long acc = 0;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint64_t v = list[i];
+        mp_relax(a, v, a.row[v], a.row[v + 1], acc);
+    }
+    mp_block_any(acc, a.any);
+}
+
+// A warp per HUB_CHUNK edges of a frontier hub (class 2).
+__global__ void __launch_bounds__(SRV_THREADS) k_mp_hubs(MpArgs a, const uint32_t* __restrict__ list,
+                                                         const uint32_t* __restrict__ count,
+                                                         const uint32_t* __restrict__ prefix)
+{
+    const uint32_t n = *count;
+    unsigned long long acc = 0;
+    if (n) {
+        const uint32_t chunks = prefix[n];
+        const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+        for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
+            const uint32_t i = hub_of_chunk(prefix, n, (uint32_t)c);
+            const uint64_t v = list[i];
+            const uint64_t e0 = a.row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
+            const uint64_t end = a.row[v + 1];
+            mp_relax(a, v, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, acc);
+        }
+    }
+    mp_block_any(acc, a.any);
+}
+
+// After a superstep: the consumed frontier masks back to zero.
+__global__ void k_mp_clear(uint64_t* __restrict__ front, const uint32_t* __restrict__ l0, const uint32_t* __restrict__ l1,
+                           const uint32_t* __restrict__ l2, const uint32_t* __restrict__ cnt)
+{
+    const uint64_t n0 = cnt[0], n1 = cnt[1], n2 = cnt[2];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n0 + n1 + n2;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = i < n0 ? l0[i] : (i < n0 + n1 ? l1[i - n0] : l2[i - n0 - n1]);
+        front[v] = 0ULL;
+    }
+}
+
+// Lane k of every vertex to `init` (INF for SSSP, the vertex id for CC, which
+// also joins every vertex to the frontier of lane k).
+__global__ void k_mp_init_lane(uint32_t* __restrict__ dist, uint64_t* __restrict__ front, uint64_t V, int k, int cc)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        dist[v * MP_K + k] = cc ? (uint32_t)v : SRV_INF;
+        if (cc) front[v] |= 1ULL << k;
+    }
+}
+
+// SSSP source s of lane k: distance 0 and into the current frontier lists.
+__global__ void k_mp_admit_source(uint32_t* __restrict__ dist, uint64_t* __restrict__ front,
+                                  const uint64_t* __restrict__ row, uint64_t s, int k, uint32_t* __restrict__ l0,
+                                  uint32_t* __restrict__ l1, uint32_t* __restrict__ l2, uint32_t* __restrict__ cnt)
+{
+    dist[s * MP_K + k] = 0u;
+    const unsigned long long old = front[s];
+    front[s] = old | (1ULL << k);
+    if (!old) {
+        const uint64_t d = row[s + 1] - row[s];
+        const int cls = d <= MP_T0 ? 0 : (d <= MP_T1 ? 1 : 2);
+        const uint32_t at = cnt[cls]++;
+        (cls == 0 ? l0 : cls == 1 ? l1 : l2)[at] = (uint32_t)s;
+    }
+}
+
+// Every vertex with a nonzero frontier mask into the frontier bitmap.
+__global__ void k_mp_mark_all(const uint64_t* __restrict__ front, uint64_t V, uint32_t* __restrict__ fbm)
+{
+    const uint64_t W = (V + 31) >> 5;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < W; w += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        for (int j = 0; j < 32; j++) {
+            const uint64_t v = w * 32 + j;
+            if (v < V && front[v]) bits |= 1u << j;
+        }
+        fbm[w] |= bits;
+    }
+}
+
+__global__ void k_mp_extract(const uint32_t* __restrict__ dist, uint64_t V, int k, uint32_t* __restrict__ out)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        out[v] = dist[v * MP_K + k];
+}
+
+// ---------------------------------------------------------------------------
+// PPR lanes
+// ---------------------------------------------------------------------------
+struct PpLanes {
+    float* out[PP_K];       // result buffer of a lane in its last gather, else null
+    uint32_t seed[PP_K];
+    uint32_t active;        // lanes gathering this superstep
+};
+
+struct PpArgs {
+    const uint64_t* __restrict__ row;
+    const uint32_t* __restrict__ adj;
+    const float* __restrict__ b_cur;
+    float* __restrict__ b_next;
+    float2* __restrict__ partial;  // (sum, compensation) per hub chunk and lane
+};
+
+__device__ __forceinline__ void pp_add(float& s, float& c, float x)
+{
+    const float t = __fadd_rn(s, x);
+    const float bp = __fsub_rn(t, s);
+    c = __fadd_rn(c, __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(x, bp)));
+    s = t;
+}
+
+__device__ __forceinline__ void pp_merge(float& s, float& c, float s2, float c2)
+{
+    pp_add(s, c, s2);
+    c = __fadd_rn(c, c2);
+}
+
+// Half-warp h sums lane k of b_cur over the edges e0 + 2i + h of [e0, e1).
+__device__ __forceinline__ void pp_gather(const PpArgs& a, uint64_t e0, uint64_t e1, bool on, float& s, float& c)
+{
+    const int lane = threadIdx.x & 31, k = lane & 15, h = lane >> 4;
+    for (uint64_t e = e0; e < e1; e += 32) {
+        const uint32_t uj = (e + lane < e1) ? a.adj[e + lane] : 0u;
+        const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
+        for (int j0 = 0; j0 < nj; j0 += 8) {
+            uint32_t u[4];
+            float q[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) u[r] = __shfl_sync(FULL, uj, (j0 + 2 * r + h) & 31);
+#pragma unroll
+            for (int r = 0; r < 4; r++) q[r] = (on && j0 + 2 * r + h < nj) ? a.b_cur[(uint64_t)u[r] * PP_K + k] : 0.0f;
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                if (on && j0 + 2 * r + h < nj) pp_add(s, c, q[r]);
+        }
+    }
+}
+
+// Threads 0..15 finish vertex v for their lane from (s, c).
+__device__ __forceinline__ void pp_finish(const PpArgs& a, const PpLanes& L, uint64_t v, uint64_t deg, float s, float c)
+{
+    const int k = threadIdx.x & 31;
+    if (k >= PP_K) return;
+    float bn = 0.0f;
+    if ((L.active >> k) & 1u) {
+        const float sum = __fadd_rn(s, c);
+        const float xn = __fadd_rn(L.seed[k] == (uint32_t)v ? 0.15f : 0.0f, __fmul_rn(0.85f, sum));
+        if (L.out[k]) L.out[k][v] = xn;
+        else if (deg) bn = __fdiv_rn(xn, (float)deg);
+    }
+    a.b_next[v * PP_K + k] = bn;
+}
+
+__global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+                                                             uint64_t n)
+{
+    const int lane = threadIdx.x & 31;
+    const bool on = (L.active >> (lane & 15)) & 1u;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint64_t v = list[i];
+        const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
+        float s = 0.0f, c = 0.0f;
+        pp_gather(a, e0, e1, on, s, c);
+        const float s2 = __shfl_down_sync(FULL, s, 16), c2 = __shfl_down_sync(FULL, c, 16);
+        pp_merge(s, c, s2, c2);
+        pp_finish(a, L, v, e1 - e0, s, c);
+    }
+}
+
+__global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+                                                               uint32_t n, const uint32_t* __restrict__ prefix)
+{
+    if (!n) return;
+    const int lane = threadIdx.x & 31;
+    const bool on = (L.active >> (lane & 15)) & 1u;
+    const uint32_t chunks = prefix[n];
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
+        const uint32_t i = hub_of_chunk(prefix, n, (uint32_t)c);
+        const uint64_t v = list[i];
+        const uint64_t e0 = a.row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
+        const uint64_t end = a.row[v + 1];
+        float s = 0.0f, cc = 0.0f;
+        pp_gather(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, on, s, cc);
+        const float s2 = __shfl_down_sync(FULL, s, 16), c2 = __shfl_down_sync(FULL, cc, 16);
+        pp_merge(s, cc, s2, c2);
+        if (lane < PP_K) a.partial[c * PP_K + lane] = make_float2(s, cc);
+    }
+}
+
+__global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_finish(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+                                                               uint32_t n, const uint32_t* __restrict__ prefix)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint64_t v = list[i];
+        float s = 0.0f, c = 0.0f;
+        if (lane < PP_K)
+            for (uint32_t ch = prefix[i]; ch < prefix[i + 1]; ch++) {
+                const float2 p = a.partial[(uint64_t)ch * PP_K + lane];
+                pp_merge(s, c, p.x, p.y);
+            }
+        pp_finish(a, L, v, a.row[v + 1] - a.row[v], s, c);
+    }
+}
+
+// Seed s of lane k: the broadcast of superstep 0, x = 1 at the seed.
+__global__ void k_pp_admit(float* __restrict__ b, const uint64_t* __restrict__ row, uint64_t s, int k)
+{
+    const uint64_t d = row[s + 1] - row[s];
+    b[s * PP_K + k] = d ? __fdiv_rn(1.0f, (float)d) : 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Query {
+    uint64_t id = 0;
+    int gid = 0, kind = 0;
+    uint64_t src = 0;
+    double t_submit = 0, t_start = 0, t_done = 0;
+    int state = 0;  // IPG_QUERY_*
+    void* result = nullptr;
+    uint64_t result_bytes = 0;
+    cudaEvent_t ready = nullptr;  // result complete on the device
+};
+
+struct Group;
+
+struct Graph {
+    int gid = 0;
+    ipg_graph* g = nullptr;
+    ipg_graph_view gv{};
+    Group* mp = nullptr;
+    Group* pp = nullptr;
+};
+
+struct Group {
+    int kind = 0;  // 0 min-plus, 1 PPR
+    Graph* G = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool running = false;
+    uint64_t busy = 0;
+    std::vector<std::vector<uint64_t>> lane_q;  // queries on each lane
+    double last_used = 0;
+    std::vector<std::pair<void*, uint64_t>> allocs;
+    uint64_t bytes = 0;
+    // min-plus
+    uint32_t* dist = nullptr;
+    uint64_t* front[2] = {nullptr, nullptr};
+    int cur = 0;
+    uint32_t* fbm = nullptr;
+    uint32_t* list[3] = {nullptr, nullptr, nullptr};
+    uint32_t* cnt = nullptr;
+    uint32_t* prefix = nullptr;
+    unsigned long long* any_d = nullptr;
+    unsigned long long* any_h = nullptr;
+    uint64_t wmask = 0;
+    int cc_lane = -1;  // CC lane admitted in the current admission round
+    // PPR
+    float* b[2] = {nullptr, nullptr};
+    float2* partial = nullptr;
+    uint32_t* pp_prefix = nullptr;
+    uint32_t* pp_count2 = nullptr;
+    ipg_bins bins{};
+    int it[PP_K] = {0};
+    uint32_t seed[PP_K] = {0};
+    uint32_t grid = 0;
+    uint64_t supersteps = 0;
+};
+
+template <class T>
+int galloc(Group* G, T** p, uint64_t n)
+{
+    void* d = nullptr;
+    const uint64_t bytes = (n ? n : 1) * sizeof(T);
+    int r = ipg_dev_alloc(&d, bytes);
+    if (r != IPG_OK) return r;
+    G->allocs.push_back({d, bytes});
+    G->bytes += bytes;
+    *p = (T*)d;
+    return IPG_OK;
+}
+
+}  // namespace
+
+struct ipg_server {
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    uint32_t rounds = 20;
+    std::vector<std::unique_ptr<Graph>> graphs;
+    std::vector<Group*> groups;
+    std::map<uint64_t, Query> queries;
+    std::vector<std::deque<uint64_t>> pending;  // per graph and group kind: gid * 2 + kind
+    uint64_t n_pending = 0;
+    std::vector<uint64_t> finishing;            // results being extracted
+    std::vector<uint64_t> completed;            // done since the last drain
+    std::multimap<uint64_t, void*> pool;  // released result buffers by size
+    uint64_t next_id = 1;
+    std::mutex mu;
+    ipg_server_stats stats{};
+    int sms = 148;
+};
+
+namespace {
+
+void free_group(ipg_server* S, Group* G)
+{
+    if (G->st) cudaStreamSynchronize(G->st);
+    for (auto& a : G->allocs) ipg_dev_free(a.first, a.second);
+    if (G->any_h) cudaFreeHost(G->any_h);
+    if (G->ev) cudaEventDestroy(G->ev);
+    if (G->st) cudaStreamDestroy(G->st);
+    S->in_use -= G->bytes;
+    if (G->G->mp == G) G->G->mp = nullptr;
+    if (G->G->pp == G) G->G->pp = nullptr;
+    S->groups.erase(std::find(S->groups.begin(), S->groups.end(), G));
+    S->stats.groups_freed++;
+    delete G;
+}
+
+uint64_t group_bytes(const Graph* G, int kind)
+{
+    const uint64_t V = G->gv.V, E = G->gv.E;
+    if (kind == 0) return V * (MP_K * 4 + 16 + 12) + V / 8 + (E / (MP_T1 + 1) + 2) * 4 + 4096;
+    return V * (PP_K * 4 * 2) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8 + 4) + 4096;
+}
+
+// Frees idle groups (least recently used first) until `need` more bytes fit.
+bool make_room(ipg_server* S, uint64_t need)
+{
+    if (!S->budget) return true;
+    while (S->in_use + need > S->budget) {
+        Group* victim = nullptr;
+        for (Group* G : S->groups)
+            if (!G->busy && !G->running && (!victim || G->last_used < victim->last_used)) victim = G;
+        if (victim) {
+            free_group(S, victim);
+            continue;
+        }
+        // cached result buffers go next
+        if (!S->pool.empty()) {
+            auto it = S->pool.begin();
+            ipg_dev_free(it->second, it->first);
+            S->in_use -= it->first;
+            S->pool.erase(it);
+            continue;
+        }
+        return false;
+    }
+    return true;
+}
+
+int create_group(ipg_server* S, Graph* Gr, int kind, Group** out)
+{
+    *out = nullptr;
+    const uint64_t need = group_bytes(Gr, kind);
+    if (!make_room(S, need)) return IPG_EBUDGET;
+    Group* G = new Group();
+    G->kind = kind;
+    G->G = Gr;
+    G->lane_q.resize(kind == 0 ? MP_K : PP_K);
+    const uint64_t V = Gr->gv.V, E = Gr->gv.E;
+    int r = IPG_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&G->ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+    int occ = 0;
+    if (kind == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mp_vertices, SRV_THREADS, 0);
+        if (r == IPG_OK) r = galloc(G, &G->dist, V * MP_K);
+        if (r == IPG_OK) r = galloc(G, &G->front[0], V);
+        if (r == IPG_OK) r = galloc(G, &G->front[1], V);
+        if (r == IPG_OK) r = galloc(G, &G->fbm, (V + 31) / 32 + 1);
+        for (int k = 0; k < 3 && r == IPG_OK; k++) r = galloc(G, &G->list[k], V);
+        if (r == IPG_OK) r = galloc(G, &G->cnt, 8);
+        if (r == IPG_OK) r = galloc(G, &G->prefix, E / (MP_T1 + 1) + 2);
+        if (r == IPG_OK) r = galloc(G, &G->any_d, 1);
+        if (r == IPG_OK && cudaHostAlloc((void**)&G->any_h, 8, cudaHostAllocDefault) != cudaSuccess)
+            r = ipg_internal_fail(IPG_ENOMEM, "serve: pinned allocation failed");
+        if (r == IPG_OK) {
+            cudaMemsetAsync(G->front[0], 0, V * 8, G->st);
+            cudaMemsetAsync(G->front[1], 0, V * 8, G->st);
+            cudaMemsetAsync(G->fbm, 0, ((V + 31) / 32 + 1) * 4, G->st);
+            cudaMemsetAsync(G->cnt, 0, 32, G->st);
+        }
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pp_vertices, SRV_THREADS, 0);
+        if (r == IPG_OK) r = ipg_graph_bins(Gr->g, 0, MP_T0, MP_T1, &G->bins);
+        if (r == IPG_OK) r = galloc(G, &G->b[0], V * PP_K);
+        if (r == IPG_OK) r = galloc(G, &G->b[1], V * PP_K);
+        const uint64_t nh = G->bins.count[2];
+        if (r == IPG_OK) r = galloc(G, &G->pp_prefix, nh + 2);
+        if (r == IPG_OK) r = galloc(G, &G->pp_count2, 1);
+        uint32_t chunks = 0;
+        if (r == IPG_OK) {
+            const uint32_t n2 = (uint32_t)nh;
+            cudaMemcpyAsync(G->pp_count2, &n2, 4, cudaMemcpyHostToDevice, G->st);
+            k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->bins.d_list[2], G->pp_count2, Gr->gv.d_row, G->pp_prefix);
+            cudaMemcpyAsync(&chunks, G->pp_prefix + nh, 4, cudaMemcpyDeviceToHost, G->st);
+            if (cudaStreamSynchronize(G->st) != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, "serve: hub prefix failed");
+        }
+        if (r == IPG_OK) r = galloc(G, &G->partial, (uint64_t)chunks * PP_K);
+        if (r == IPG_OK) {
+            cudaMemsetAsync(G->b[0], 0, V * PP_K * 4, G->st);
+            cudaMemsetAsync(G->b[1], 0, V * PP_K * 4, G->st);
+        }
+    }
+    G->grid = (uint32_t)S->sms * (uint32_t)std::max(1, std::min(occ, 8));
+    if (r == IPG_OK && cudaGetLastError() != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, "serve: group setup failed");
+    S->in_use += G->bytes;
+    S->groups.push_back(G);
+    if (r != IPG_OK) {
+        free_group(S, G);
+        return r;
+    }
+    (kind == 0 ? Gr->mp : Gr->pp) = G;
+    G->last_used = now_s();
+    S->stats.groups_created++;
+    return IPG_OK;
+}
+
+int take_result(ipg_server* S, Query& q, uint64_t bytes)
+{
+    auto it = S->pool.find(bytes);
+    if (it != S->pool.end()) {
+        q.result = it->second;
+        S->pool.erase(it);
+    } else {
+        if (!make_room(S, bytes)) return IPG_EBUDGET;
+        int r = ipg_dev_alloc(&q.result, bytes);
+        if (r != IPG_OK) return r;
+        S->in_use += bytes;
+    }
+    q.result_bytes = bytes;
+    return IPG_OK;
+}
+
+void release_result(ipg_server* S, Query& q)
+{
+    if (q.result) S->pool.insert({q.result_bytes, q.result});
+    q.result = nullptr;
+}
+
+// Pending queries of group G's graph and kind take free lanes.
+void admit(ipg_server* S, Group* G, double now)
+{
+    std::deque<uint64_t>& queue = S->pending[(size_t)G->G->gid * 2 + G->kind];
+    const uint64_t V = G->G->gv.V;
+    const int K = G->kind == 0 ? MP_K : PP_K;
+    const uint64_t full = K == 64 ? ~0ULL : ((1ULL << K) - 1);
+    G->cc_lane = -1;
+    bool rebuild = false;
+    for (auto it = queue.begin(); it != queue.end();) {
+        Query& q = S->queries[*it];
+        const bool joins_cc = q.kind == IPG_QUERY_CC && G->cc_lane >= 0;
+        if (!joins_cc && (G->busy & full) == full) break;  // no lane free
+        const uint64_t rbytes = V * 4;
+        if (take_result(S, q, rbytes) != IPG_OK) {
+            ++it;
+            continue;
+        }
+        int k;
+        if (joins_cc) {
+            k = G->cc_lane;
+        } else {
+            k = __builtin_ctzll(~G->busy);
+            G->busy |= 1ULL << k;
+            const uint32_t g = G->grid;
+            if (q.kind == IPG_QUERY_PPR) {
+                k_pp_admit<<<1, 1, 0, G->st>>>(G->b[G->cur], G->G->gv.d_row, q.src, k);
+                G->it[k] = 0;
+                G->seed[k] = (uint32_t)q.src;
+            } else if (q.kind == IPG_QUERY_CC) {
+                k_mp_init_lane<<<g, SRV_THREADS, 0, G->st>>>(G->dist, G->front[G->cur], V, k, 1);
+                G->wmask &= ~(1ULL << k);
+                G->cc_lane = k;
+                rebuild = true;
+            } else {
+                k_mp_init_lane<<<g, SRV_THREADS, 0, G->st>>>(G->dist, G->front[G->cur], V, k, 0);
+                k_mp_admit_source<<<1, 1, 0, G->st>>>(G->dist, G->front[G->cur], G->G->gv.d_row, q.src, k,
+                                                       G->list[0], G->list[1], G->list[2], G->cnt);
+                G->wmask |= 1ULL << k;
+            }
+            S->stats.lanes_admitted++;
+        }
+        G->lane_q[k].push_back(q.id);
+        q.state = IPG_QUERY_RUNNING;
+        q.t_start = now;
+        it = queue.erase(it);
+        S->n_pending--;
+    }
+    if (rebuild) {
+        // a CC lane puts every vertex into the frontier: rebuild the lists
+        k_mp_mark_all<<<G->grid, SRV_THREADS, 0, G->st>>>(G->front[G->cur], V, G->fbm);
+        cudaMemsetAsync(G->cnt, 0, 12, G->st);
+        ipg_compact(G->fbm, V, G->G->gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
+                    G->st);
+    }
+}
+
+int launch_superstep(ipg_server* S, Group* G)
+{
+    const uint32_t g = G->grid;
+    const ipg_graph_view& gv = G->G->gv;
+    if (G->kind == 0) {
+        MpArgs a;
+        a.row = gv.d_row;
+        a.adj = (const uint32_t*)gv.d_adj;
+        a.wgt = (const uint32_t*)gv.d_wgt;
+        a.dist = G->dist;
+        a.front = G->front[G->cur];
+        a.next = G->front[G->cur ^ 1];
+        a.fbm = G->fbm;
+        a.any = G->any_d;
+        a.wmask = G->wmask;
+        cudaMemsetAsync(G->any_d, 0, 8, G->st);
+        k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix);
+        k_mp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[0], G->cnt + 0);
+        k_mp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[1], G->cnt + 1);
+        k_mp_hubs<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[2], G->cnt + 2, G->prefix);
+        k_mp_clear<<<g, SRV_THREADS, 0, G->st>>>(G->front[G->cur], G->list[0], G->list[1], G->list[2], G->cnt);
+        cudaMemsetAsync(G->cnt, 0, 12, G->st);
+        ipg_compact(G->fbm, gv.V, gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
+                    G->st);
+        cudaMemcpyAsync(G->any_h, G->any_d, 8, cudaMemcpyDeviceToHost, G->st);
+        G->cur ^= 1;
+        S->stats.kernel_launches += 6;
+    } else {
+        PpArgs a;
+        a.row = gv.d_row;
+        a.adj = (const uint32_t*)gv.d_adj;
+        a.b_cur = G->b[G->cur];
+        a.b_next = G->b[G->cur ^ 1];
+        a.partial = G->partial;
+        PpLanes L;
+        L.active = (uint32_t)G->busy;
+        for (int k = 0; k < PP_K; k++) {
+            L.seed[k] = G->seed[k];
+            L.out[k] = nullptr;
+            if (((G->busy >> k) & 1) && G->it[k] + 1 == (int)S->rounds)
+                L.out[k] = (float*)S->queries[G->lane_q[k][0]].result;
+        }
+        const ipg_bins& B = G->bins;
+        if (B.count[0]) k_pp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], B.count[0]);
+        if (B.count[1]) k_pp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[1], B.count[1]);
+        if (B.count[2]) {
+            k_pp_hub_chunks<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[2], (uint32_t)B.count[2], G->pp_prefix);
+            k_pp_hub_finish<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[2], (uint32_t)B.count[2], G->pp_prefix);
+        }
+        G->cur ^= 1;
+        S->stats.kernel_launches += 4;
+    }
+    cudaEventRecord(G->ev, G->st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+    G->running = true;
+    G->supersteps++;
+    S->stats.supersteps++;
+    return IPG_OK;
+}
+
+// A completed superstep: retire finished lanes.
+void retire(ipg_server* S, Group* G, double now)
+{
+    if (G->kind == 0) {
+        const uint64_t live = *G->any_h;
+        const uint64_t done = G->busy & ~live;
+        for (int k = 0; k < MP_K; k++) {
+            if (!((done >> k) & 1)) continue;
+            for (uint64_t qid : G->lane_q[k]) {
+                Query& q = S->queries[qid];
+                k_mp_extract<<<G->grid, SRV_THREADS, 0, G->st>>>(G->dist, G->G->gv.V, k, (uint32_t*)q.result);
+                cudaEventCreateWithFlags(&q.ready, cudaEventDisableTiming);
+                cudaEventRecord(q.ready, G->st);
+                q.state = IPG_QUERY_FINISHING;
+                S->finishing.push_back(qid);
+            }
+            G->lane_q[k].clear();
+            if (G->cc_lane == k) G->cc_lane = -1;
+        }
+        G->busy &= ~done;
+    } else {
+        for (int k = 0; k < PP_K; k++) {
+            if (!((G->busy >> k) & 1)) continue;
+            if (++G->it[k] < (int)S->rounds) continue;
+            Query& q = S->queries[G->lane_q[k][0]];
+            q.state = IPG_QUERY_DONE;
+            q.t_done = now;
+            S->completed.push_back(q.id);
+            G->lane_q[k].clear();
+            G->busy &= ~(1ULL << k);
+        }
+    }
+    G->last_used = now;
+}
+
+}  // namespace
+
+extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_server** out)
+{
+    if (!out) return ipg_internal_fail(IPG_EINVAL, "ipg_server_create: null output");
+    if (ppr_rounds < 1) return ipg_internal_fail(IPG_EINVAL, "ipg_server_create: ppr_rounds must be at least 1");
+    ipg_server* S = new (std::nothrow) ipg_server();
+    if (!S) return ipg_internal_fail(IPG_ENOMEM, "ipg_server_create: out of host memory");
+    S->budget = hbm_budget;
+    S->rounds = ppr_rounds;
+    S->sms = ipg_sm_count();
+    *out = S;
+    return IPG_OK;
+}
+
+extern "C" void ipg_server_free(ipg_server* S)
+{
+    if (!S) return;
+    while (!S->groups.empty()) free_group(S, S->groups.back());
+    for (auto& kv : S->queries) {
+        if (kv.second.ready) cudaEventDestroy(kv.second.ready);
+        if (kv.second.result) ipg_dev_free(kv.second.result, kv.second.result_bytes);
+    }
+    for (auto& kv : S->pool) ipg_dev_free(kv.second, kv.first);
+    delete S;
+}
+
+extern "C" int ipg_server_add_graph(ipg_server* S, ipg_graph* g, int* gid)
+{
+    if (!S || !g || !gid) return ipg_internal_fail(IPG_EINVAL, "ipg_server_add_graph: null argument");
+    std::unique_ptr<Graph> G(new Graph());
+    G->g = g;
+    int r = ipg_graph_view_get(g, &G->gv);
+    if (r != IPG_OK) return r;
+    if (G->gv.id_bytes != 4) return ipg_internal_fail(IPG_EINVAL, "ipg_server_add_graph: 32-bit vertex ids only");
+    if (G->gv.d_wgt && G->gv.weight_bytes != 4)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_add_graph: weights must be u32");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *gid = (int)S->graphs.size();
+    G->gid = *gid;
+    S->graphs.push_back(std::move(G));
+    S->pending.resize(S->graphs.size() * 2);
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_submit(ipg_server* S, int gid, int kind, uint64_t source, uint64_t* qid)
+{
+    if (!S || !qid) return ipg_internal_fail(IPG_EINVAL, "ipg_server_submit: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (gid < 0 || gid >= (int)S->graphs.size()) return ipg_internal_fail(IPG_EINVAL, "ipg_server_submit: no such graph");
+    const Graph* G = S->graphs[gid].get();
+    if (kind != IPG_QUERY_SSSP && kind != IPG_QUERY_PPR && kind != IPG_QUERY_CC)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_submit: unknown query kind");
+    if (kind != IPG_QUERY_CC && source >= G->gv.V)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_submit: source out of range");
+    if (kind == IPG_QUERY_SSSP && !G->gv.d_wgt)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_submit: SSSP needs a weighted graph");
+    Query q;
+    q.id = S->next_id++;
+    q.gid = gid;
+    q.kind = kind;
+    q.src = source;
+    q.t_submit = now_s();
+    q.state = IPG_QUERY_PENDING;
+    S->queries[q.id] = q;
+    S->pending[(size_t)gid * 2 + (kind == IPG_QUERY_PPR ? 1 : 0)].push_back(q.id);
+    S->n_pending++;
+    S->stats.submitted++;
+    *qid = q.id;
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
+{
+    if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_poll: null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    const double now = now_s();
+    // results whose extraction finished
+    for (size_t i = 0; i < S->finishing.size();) {
+        Query& q = S->queries[S->finishing[i]];
+        if (cudaEventQuery(q.ready) == cudaSuccess) {
+            cudaEventDestroy(q.ready);
+            q.ready = nullptr;
+            q.state = IPG_QUERY_DONE;
+            q.t_done = now;
+            S->completed.push_back(q.id);
+            S->finishing[i] = S->finishing.back();
+            S->finishing.pop_back();
+        } else {
+            i++;
+        }
+    }
+    // groups for pending queries that have none (HBM budget permitting)
+    for (size_t i = 0; i < S->pending.size(); i++) {
+        if (S->pending[i].empty()) continue;
+        Graph* Gr = S->graphs[i / 2].get();
+        const int kind = (int)(i % 2);
+        if (!(kind ? Gr->pp : Gr->mp)) {
+            Group* G = nullptr;
+            int r = create_group(S, Gr, kind, &G);
+            if (r != IPG_OK && r != IPG_EBUDGET && r != IPG_ENOMEM) return r;
+        }
+    }
+    // every group: retire, admit, launch
+    for (size_t i = 0; i < S->groups.size(); i++) {
+        Group* G = S->groups[i];
+        if (G->running) {
+            if (cudaEventQuery(G->ev) != cudaSuccess) continue;
+            G->running = false;
+            retire(S, G, now);
+        }
+        admit(S, G, now);
+        if (G->busy) {
+            int r = launch_superstep(S, G);
+            if (r != IPG_OK) return r;
+        }
+    }
+    uint64_t n = S->n_pending + S->finishing.size();
+    for (Group* G : S->groups)
+        for (auto& l : G->lane_q) n += l.size();
+    if (outstanding) *outstanding = n;
+    S->stats.bytes_in_use = S->in_use;
+    if (S->in_use > S->stats.peak_bytes) S->stats.peak_bytes = S->in_use;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_query(ipg_server* S, uint64_t qid, int* state, double* latency, double* queued)
+{
+    if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_query: null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->queries.find(qid);
+    if (it == S->queries.end()) return ipg_internal_fail(IPG_EINVAL, "ipg_server_query: no such query");
+    const Query& q = it->second;
+    if (state) *state = q.state;
+    if (latency) *latency = q.state == IPG_QUERY_DONE ? q.t_done - q.t_submit : 0.0;
+    if (queued) *queued = q.t_start > 0 ? q.t_start - q.t_submit : 0.0;
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_result(ipg_server* S, uint64_t qid, void* out, uint64_t cap_bytes)
+{
+    if (!S || !out) return ipg_internal_fail(IPG_EINVAL, "ipg_server_result: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->queries.find(qid);
+    if (it == S->queries.end()) return ipg_internal_fail(IPG_EINVAL, "ipg_server_result: no such query");
+    const Query& q = it->second;
+    if (q.state != IPG_QUERY_DONE || !q.result) return ipg_internal_fail(IPG_EINVAL, "ipg_server_result: not available");
+    if (cap_bytes < q.result_bytes) return ipg_internal_fail(IPG_EINVAL, "ipg_server_result: buffer too small");
+    if (cudaMemcpy(out, q.result, q.result_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ipg_internal_fail(IPG_ECUDA, "ipg_server_result: copy failed");
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_result_device(ipg_server* S, uint64_t qid, const void** d_ptr, uint64_t* bytes)
+{
+    if (!S || !d_ptr) return ipg_internal_fail(IPG_EINVAL, "ipg_server_result_device: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->queries.find(qid);
+    if (it == S->queries.end() || it->second.state != IPG_QUERY_DONE)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_result_device: not available");
+    *d_ptr = it->second.result;
+    if (bytes) *bytes = it->second.result_bytes;
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_release(ipg_server* S, uint64_t qid)
+{
+    if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_release: null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->queries.find(qid);
+    if (it == S->queries.end()) return ipg_internal_fail(IPG_EINVAL, "ipg_server_release: no such query");
+    if (it->second.state != IPG_QUERY_DONE) return ipg_internal_fail(IPG_EINVAL, "ipg_server_release: still running");
+    release_result(S, it->second);
+    S->queries.erase(it);
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_get_stats(ipg_server* S, ipg_server_stats* out)
+{
+    if (!S || !out) return ipg_internal_fail(IPG_EINVAL, "ipg_server_get_stats: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *out = S->stats;
+    out->bytes_in_use = S->in_use;
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_run_trace(ipg_server* S, uint64_t n, const double* arrival, const int* gid, const int* kind,
+                                    const uint64_t* source, int keep_results, uint64_t* qids, double* latency,
+                                    double* makespan)
+{
+    if (!S || (n && (!arrival || !gid || !kind || !source)))
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_run_trace: null argument");
+    std::vector<uint64_t> ids(n, 0);
+    std::map<uint64_t, uint64_t> index;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->completed.clear();
+    }
+    const double t0 = now_s();
+    double last_progress = t0;
+    uint64_t next = 0, done = 0;
+    while (done < n) {
+        const double t = now_s() - t0;
+        while (next < n && arrival[next] <= t) {
+            int r = ipg_server_submit(S, gid[next], kind[next], source[next], &ids[next]);
+            if (r != IPG_OK) return r;
+            {
+                // latency counts from the scheduled arrival
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->queries[ids[next]].t_submit = t0 + arrival[next];
+            }
+            index[ids[next]] = next;
+            next++;
+        }
+        uint64_t outstanding = 0;
+        int r = ipg_server_poll(S, &outstanding);
+        if (r != IPG_OK) return r;
+        std::vector<uint64_t> fresh;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            fresh.swap(S->completed);
+        }
+        for (uint64_t qid : fresh) {
+            auto it = index.find(qid);
+            if (it == index.end()) continue;
+            double lat = 0;
+            ipg_server_query(S, qid, nullptr, &lat, nullptr);
+            if (latency) latency[it->second] = lat;
+            if (!keep_results) ipg_server_release(S, qid);
+            done++;
+            last_progress = now_s();
+        }
+        if (outstanding && next == n && now_s() - last_progress > 60.0)
+            return ipg_internal_fail(IPG_EBUDGET, "ipg_server_run_trace: no progress for 60 s (HBM budget too small?)");
+    }
+    if (makespan) *makespan = now_s() - t0;
+    if (qids)
+        for (uint64_t i = 0; i < n; i++) qids[i] = ids[i];
+    return IPG_OK;
+}

@@ -1,0 +1,176 @@
+"""Request server: every served query equals the oracle (SSSP and CC exactly,
+PPR within 2e-6 max abs against the FP64 ppr program), a query's result is
+bitwise the same alone and in a mix, queries joining while others run
+(continuous batching) stay correct, and a tight HBM budget still serves
+everything by evicting idle lane groups."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PPR_TOL = 2e-6  # FP32 lanes against the FP64 oracle, max abs per vertex
+
+
+def _graphs():
+    gs = [O.add_weights(O.gen_rmat(10, 8, seed=1, undirected=True), wmax=255, seed=1),
+          O.add_weights(O.gen_er(3000, 12000, seed=2, undirected=True), wmax=255, seed=2),
+          O.add_weights(O.gen_rmat(12, 16, seed=3, undirected=True), wmax=255, seed=3)]
+    return gs
+
+
+def _device(gs):
+    import ipregel_b200 as ip
+    return [ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, wgt=g.wgt) for g in gs]
+
+
+def _want(g, kind, src):
+    from ipregel_b200 import serve as S
+    if kind == S.SSSP:
+        return O.dijkstra(g, src)
+    if kind == S.CC:
+        return O.run(g, "cc", "spread")[0]
+    return O.run(g, "ppr", "single_broadcast", source=src, rounds=20)[0]
+
+
+def _check(g, kind, src, got):
+    from ipregel_b200 import serve as S
+    want = _want(g, kind, src)
+    if kind == S.PPR:
+        assert np.max(np.abs(got.astype(np.float64) - want)) <= PPR_TOL
+    else:
+        np.testing.assert_array_equal(got, want)
+
+
+def _queries(gs, n, seed):
+    from ipregel_b200 import serve as S
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        gid = int(rng.integers(len(gs)))
+        kind = int(rng.choice([S.SSSP, S.PPR, S.CC], p=[0.6, 0.3, 0.1]))
+        src = 0 if kind == S.CC else int(rng.integers(gs[gid].V))
+        out.append((gid, kind, src))
+    return out
+
+
+def test_mixed_batch_matches_oracle_and_alone():
+    from ipregel_b200 import serve as S
+    gs = _graphs()
+    dg = _device(gs)
+    srv = S.Server(ppr_rounds=20)
+    try:
+        for d in dg:
+            srv.add_graph(d)
+        qs = _queries(gs, 60, seed=1)
+        ids = [srv.submit(*q) for q in qs]
+        srv.drain()
+        mix = []
+        for qid, (gid, kind, src) in zip(ids, qs):
+            assert srv.query(qid)["state"] == S.DONE
+            r = srv.result(qid, kind, gs[gid].V)
+            _check(gs[gid], kind, src, r)
+            mix.append(r)
+            srv.release(qid)
+        st = srv.stats()
+        assert st["submitted"] == 60 and st["lanes_admitted"] <= 60
+        # alone: bitwise the same
+        for (gid, kind, src), r in list(zip(qs, mix))[:12]:
+            alone, _ = S.run_alone(srv, gid, kind, src, gs[gid].V)
+            np.testing.assert_array_equal(alone.view(np.uint32), r.view(np.uint32))
+    finally:
+        srv.free()
+        for d in dg:
+            d.free()
+
+
+def test_continuous_batching_trace():
+    """Staggered arrivals: queries join lanes while others are in flight."""
+    from ipregel_b200 import serve as S
+    gs = _graphs()
+    dg = _device(gs)
+    srv = S.Server(ppr_rounds=20)
+    try:
+        for d in dg:
+            srv.add_graph(d)
+        tr = S.poisson_trace(120, 4000.0, [g.V for g in gs], seed=5)
+        qids, lat, mk = srv.run_trace(tr, keep_results=True)
+        assert mk > 0 and np.all(lat > 0)
+        for i in range(len(tr)):
+            gid, kind, src = int(tr.gid[i]), int(tr.kind[i]), int(tr.source[i])
+            _check(gs[gid], kind, src, srv.result(int(qids[i]), kind, gs[gid].V))
+            srv.release(int(qids[i]))
+        st = srv.stats()
+        assert st["supersteps"] > 0 and st["kernel_launches"] > 0
+    finally:
+        srv.free()
+        for d in dg:
+            d.free()
+
+
+def test_more_queries_than_lanes():
+    """100 SSSP queries on one graph: lanes (64) are reused as queries finish."""
+    from ipregel_b200 import serve as S
+    g = O.add_weights(O.gen_rmat(11, 16, seed=7, undirected=True), wmax=255, seed=7)
+    (d,) = _device([g])
+    srv = S.Server()
+    try:
+        gid = srv.add_graph(d)
+        srcs = list(range(0, 2000, 20))
+        ids = [srv.submit(gid, S.SSSP, s) for s in srcs]
+        srv.drain()
+        for qid, s in zip(ids, srcs):
+            np.testing.assert_array_equal(srv.result(qid, S.SSSP, g.V), O.dijkstra(g, s))
+    finally:
+        srv.free()
+        d.free()
+
+
+def test_tight_hbm_budget_evicts_idle_groups():
+    from ipregel_b200 import serve as S
+    gs = _graphs()
+    dg = _device(gs)
+    # room for the largest group and its results, not for all groups at once
+    V = max(g.V for g in gs)
+    budget = V * 300 + 8 * V * 4 + (1 << 20)
+    srv = S.Server(hbm_budget=budget)
+    try:
+        for d in dg:
+            srv.add_graph(d)
+        qs = [(gid, S.SSSP, 1) for gid in range(3)] + [(gid, S.PPR, 2) for gid in range(3)]
+        ids = [srv.submit(*q) for q in qs]
+        srv.drain()
+        for qid, (gid, kind, src) in zip(ids, qs):
+            _check(gs[gid], kind, src, srv.result(qid, kind, gs[gid].V))
+        st = srv.stats()
+        assert st["peak_bytes"] <= budget
+        assert st["groups_freed"] > 0
+    finally:
+        srv.free()
+        for d in dg:
+            d.free()
+
+
+def test_bad_requests_raise():
+    import ipregel_b200 as ip
+    from ipregel_b200 import serve as S
+    g = O.gen_rmat(8, 8, seed=1, undirected=True)
+    unweighted = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+    srv = S.Server()
+    try:
+        gid = srv.add_graph(unweighted)
+        with pytest.raises(ip.IPregelError, match="weighted"):
+            srv.submit(gid, S.SSSP, 0)
+        with pytest.raises(ip.IPregelError, match="no such graph"):
+            srv.submit(gid + 1, S.CC, 0)
+        with pytest.raises(ip.IPregelError, match="out of range"):
+            srv.submit(gid, S.PPR, g.V)
+        with pytest.raises(ip.IPregelError, match="kind"):
+            srv.submit(gid, 7, 0)
+        q = srv.submit(gid, S.CC, 0)  # CC needs no weights
+        srv.drain()
+        np.testing.assert_array_equal(srv.result(q, S.CC, g.V), O.run(g, "cc", "spread")[0])
+    finally:
+        srv.free()
+        unweighted.free()
