@@ -259,8 +259,10 @@ int ipg_error_f32_f64(const float* d_a, const double* d_ref, uint64_t n, double*
  * per process).  Resident graphs (32-bit ids, u32 weights for SSSP) answer
  * single-source shortest-path, connected-component and personalised-PageRank
  * queries.  Concurrent queries on one graph run as lanes of one fused
- * superstep kernel (64 min-plus lanes for SSSP and CC, 16 FP32 lanes for
- * PPR); queries join free lanes whenever their group finishes a superstep
+ * superstep kernel (64 min-plus lanes for SSSP, and for CC on graphs not
+ * declared symmetric; 16 FP32 lanes for PPR); CC on a symmetric graph runs
+ * as one union-find pass shared by the CC queries admitted together.
+ * Queries join free lanes whenever their group finishes a superstep
  * (continuous batching), and lane groups plus result buffers are admitted
  * under an HBM budget.  Results: u32 per vertex (SSSP distance, UINT32_MAX
  * unreached; CC label = least vertex id reaching it, as benchmarks/cc.c), or
@@ -297,6 +299,11 @@ int ipg_server_result_device(ipg_server* srv, uint64_t qid, const void** d_ptr, 
 /* Forgets a done query; its result buffer returns to the server's pool. */
 int ipg_server_release(ipg_server* srv, uint64_t qid);
 int ipg_server_get_stats(ipg_server* srv, ipg_server_stats* out);
+/* Per graph and group kind (0 min-plus, 1 PPR): summed device time of its
+ * supersteps (groups run concurrently, so times overlap), supersteps, lanes
+ * admitted. */
+int ipg_server_group_stats(ipg_server* srv, int gid, int group_kind, double* busy_s,
+                           uint64_t* supersteps, uint64_t* lanes);
 /* Replays an arrival trace in real time (arrival[i] seconds from the start,
  * ascending): submits each query at its time, polls until all are done.
  * latency[i] counts from the scheduled arrival; keep_results = 0 releases

@@ -2,33 +2,40 @@
 // reference, which runs one program on one graph per process).
 //
 // Queries: single-source shortest paths (integer weights), connected
-// components (min-label propagation, as benchmarks/cc.c), and personalised
-// PageRank (x' = 0.15 [v == seed] + 0.85 * sum of x_u / deg u over the row,
-// as the ppr application, in FP32 with compensated sums).  Graphs and
-// per-query vertex state stay in HBM.  Concurrent queries on one graph share
-// a lane group and advance together, one fused superstep kernel for all
-// their lanes:
+// components (labels as benchmarks/cc.c: the least vertex id that reaches a
+// vertex), and personalised PageRank (x' = 0.15 [v == seed] + 0.85 * sum of
+// x_u / deg u over the row, as the ppr application, in FP32 with compensated
+// sums).  Graphs and per-query vertex state stay in HBM.  Concurrent queries
+// on one graph share a lane group and advance together, one fused superstep
+// kernel for all their lanes:
 //
-//   min-plus group (SSSP, CC): 64 lanes; dist[v][lane] (u32, 256 bytes per
-//     vertex, so the lanes of one vertex are one coalesced line), a bit-packed
-//     frontier mask per vertex (u64, a bit per lane) double-buffered, and the
-//     frontier as degree-class lists.  A warp relaxes one edge for 32 lanes
-//     at a time: nd = dist[v][k] + w (w = 0 for a CC lane), atomicMin into
-//     dist[u][k], improved lanes OR-ed into u's next mask.  A lane whose
+//   min-plus group (SSSP; CC on graphs not declared symmetric): 64 lanes;
+//     dist[v][lane] (u32, 256 bytes per vertex, so the lanes of one vertex
+//     are one coalesced line), a bit-packed frontier mask per vertex (u64, a
+//     bit per lane) double-buffered, and the frontier as degree-class lists.
+//     A vertex with few frontier lanes has a thread per edge relax all its
+//     lanes; one with many has a thread per lane relax each edge in turn.
+//     nd = dist[v][k] + w (w = 0 for a CC lane) goes into dist[u][k] by
+//     atomicMin, and the improved lanes into u's next mask.  A lane whose
 //     frontier empties is finished.
+//   CC on a graph declared symmetric: union-find over the edges, one pass
+//     (the labels of min-label propagation are the least id of each
+//     component); CC queries admitted together share the pass.
 //   PPR group: 16 lanes; the broadcast quotients b[v][lane] = x/deg (FP32,
-//     64 bytes per vertex) double-buffered; a pull gather over every row,
-//     each half-warp summing 16 lanes of one in-neighbour.  A lane runs
-//     exactly `rounds` gathers after admission and writes its last values
-//     into the query's result buffer.
+//     64 bytes per vertex) double-buffered; a pull gather over every row: a
+//     thread per low-degree vertex reading whole lane rows as float4 quads,
+//     a half-warp per lane row for higher degrees.  A lane runs exactly
+//     `rounds` gathers after admission and writes its last values into the
+//     query's result buffer.
 //
 // Continuous batching: each group advances on its own stream; whenever its
 // superstep has completed, finished lanes retire and pending queries take the
 // free lanes before the next superstep is launched, so queries join and leave
 // while others are in flight, and groups of different graphs overlap on the
 // device.  A lane's arithmetic depends on nothing but its own query (min-plus
-// is order independent; the PPR sums run in a fixed per-vertex order), so a
-// query's result is the same alone and in any mix.
+// and union-find are order independent; the PPR sums run in a fixed
+// per-vertex order whatever the other lanes do), so a query's result is the
+// same alone and in any mix.
 //
 // Admission is bounded by an HBM budget over the server's lane groups and
 // result buffers; groups without busy lanes are freed, least recently used
@@ -55,10 +62,14 @@ namespace {
 constexpr int MP_K = 64;
 constexpr int PP_K = 16;
 constexpr int SRV_THREADS = 256;
-constexpr uint64_t MP_T0 = 64, MP_T1 = 4096;
+constexpr uint64_t MP_T0 = 8, MP_T1 = 4096;
 constexpr uint32_t HUB_CHUNK = 1024;
 constexpr uint32_t SRV_INF = 0xffffffffu;
 constexpr unsigned FULL = 0xffffffffu;
+// Up to MP_SPARSE lanes of a vertex: a thread per edge, each relaxing all.
+constexpr int MP_SPARSE = 8;
+// Resident CTAs per SM the min-plus kernels are compiled for (64 registers).
+#define MP_CTAS 4
 
 double now_s()
 {
@@ -69,9 +80,48 @@ double now_s()
 // Shared helpers
 // ---------------------------------------------------------------------------
 
-// prefix[i] = sum over j < i of ceil(deg(list[j]) / HUB_CHUNK); prefix[n] = total.
+// Status of a min-plus group after a superstep, copied to the host in one
+// transfer: lanes that improved something, list sizes, hub chunks of list 2.
+struct MpStatus {
+    unsigned long long any;
+    uint32_t cnt[3];
+    uint32_t chunks;
+};
+
+inline uint32_t warp_grid(uint64_t tasks)
+{
+    const uint64_t ctas = (tasks + (SRV_THREADS / 32) - 1) / (SRV_THREADS / 32);
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(ctas, 1), 0x7fffffffULL);
+}
+
+inline uint32_t thread_grid(uint64_t n)
+{
+    const uint64_t ctas = (n + SRV_THREADS - 1) / SRV_THREADS;
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(ctas, 1), 0x7fffffffULL);
+}
+
+// At most the CTAs of `kernel` resident at once on the device: the kernels
+// stride over their work, and CTAs beyond that would run as a second wave.
+template <class K>
+uint32_t resident_cap(K kernel, uint32_t want)
+{
+    static std::mutex mu;
+    static std::map<const void*, uint32_t> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find((const void*)kernel);
+    if (it == cache.end()) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, SRV_THREADS, 0) != cudaSuccess || n <= 0) n = 1;
+        it = cache.emplace((const void*)kernel, (uint32_t)(n * ipg_sm_count())).first;
+    }
+    return std::min(want, it->second);
+}
+
+// prefix[i] = sum over j < i of ceil(deg(list[j]) / HUB_CHUNK); prefix[n] =
+// total, also written to *total when given.
 __global__ void __launch_bounds__(1024) k_chunk_prefix(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                                       const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix)
+                                                       const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix,
+                                                       uint32_t* __restrict__ total)
 {
     __shared__ uint32_t s[1024];
     __shared__ uint32_t carry;
@@ -99,7 +149,10 @@ __global__ void __launch_bounds__(1024) k_chunk_prefix(const uint32_t* __restric
         if (t == 1023) carry += s[1023];
         __syncthreads();
     }
-    if (t == 0) prefix[n] = carry;
+    if (t == 0) {
+        prefix[n] = carry;
+        if (total) *total = carry;
+    }
 }
 
 __device__ __forceinline__ uint32_t hub_of_chunk(const uint32_t* __restrict__ prefix, uint32_t n, uint32_t c)
@@ -114,7 +167,7 @@ __device__ __forceinline__ uint32_t hub_of_chunk(const uint32_t* __restrict__ pr
 }
 
 // ---------------------------------------------------------------------------
-// Min-plus lanes (SSSP, CC)
+// Min-plus lanes (SSSP, CC by label propagation)
 // ---------------------------------------------------------------------------
 struct MpArgs {
     const uint64_t* __restrict__ row;
@@ -123,18 +176,81 @@ struct MpArgs {
     uint32_t* __restrict__ dist;
     const uint64_t* __restrict__ front;
     uint64_t* __restrict__ next;
-    uint32_t* __restrict__ fbm;        // bit per vertex: next mask became nonzero
+    uint32_t* __restrict__ fbm;        // bit per vertex: in the next frontier
     unsigned long long* __restrict__ any;
     uint64_t wmask;                    // lanes whose edges carry their weight (SSSP)
 };
 
-// One warp relaxes the edges [e0, e1) of v for all of v's frontier lanes.
+// Relaxes edge (v -> u, weight t) for the lanes ks[0..m) of v (distances
+// ds); returns the lanes whose distance at u may have dropped.  The
+// atomicMin is issued only when a plain read of u's distance (possibly stale,
+// and then only larger) shows an improvement, and its result is not waited
+// for: a lane another thread improved further meanwhile is marked needlessly,
+// which costs one redundant relaxation and changes no distance.
+template <int MAXL>
+__device__ __forceinline__ unsigned long long mp_relax_edge(const MpArgs& a, uint32_t u, uint32_t t, int m,
+                                                            const int* ks, const uint32_t* ds)
+{
+    uint32_t cur[MAXL];
+#pragma unroll
+    for (int j = 0; j < MAXL; j++) cur[j] = j < m ? a.dist[(uint64_t)u * MP_K + ks[j]] : 0u;
+    unsigned long long bits = 0;
+#pragma unroll
+    for (int j = 0; j < MAXL; j++) {
+        if (j >= m) break;
+        const uint32_t nd = ds[j] + (((a.wmask >> ks[j]) & 1ULL) ? t : 0u);
+        if (nd < cur[j]) {
+            atomicMin(&a.dist[(uint64_t)u * MP_K + ks[j]], nd);
+            bits |= 1ULL << ks[j];
+        }
+    }
+    return bits;
+}
+
+// Lanes `bits` of u join the next frontier.
+__device__ __forceinline__ void mp_mark(const MpArgs& a, uint32_t u, unsigned long long bits,
+                                        unsigned long long& any_acc)
+{
+    atomicOr((unsigned long long*)&a.next[u], bits);
+    const uint32_t fb = 1u << (u & 31);
+    if (!(a.fbm[u >> 5] & fb)) atomicOr(&a.fbm[u >> 5], fb);
+    any_acc |= bits;
+}
+
+// The first MP_SPARSE lanes of mask M and v's distances in them.
+__device__ __forceinline__ int mp_lanes(const MpArgs& a, uint64_t v, uint64_t M, int* ks, uint32_t* ds)
+{
+    int m = 0;
+    while (M && m < MP_SPARSE) {
+        const int k = __ffsll((long long)M) - 1;
+        M &= M - 1;
+        ks[m] = k;
+        ds[m] = a.dist[v * MP_K + k];
+        m++;
+    }
+    return m;
+}
+
+// One warp relaxes the edges [e0, e1) of v for all of v's frontier lanes:
+// a thread per edge when few lanes are active, else a thread per lane.
 __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e0, uint64_t e1,
                                          unsigned long long& any_acc)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t M = a.front[v];
     if (!M) return;
+    if (__popcll(M) <= MP_SPARSE) {
+        int ks[MP_SPARSE];
+        uint32_t ds[MP_SPARSE];
+        const int m = mp_lanes(a, v, M, ks, ds);
+        for (uint64_t e = e0 + lane; e < e1; e += 32) {
+            const uint32_t u = a.adj[e];
+            const uint32_t t = a.wgt ? a.wgt[e] : 0u;
+            const unsigned long long bits = mp_relax_edge<MP_SPARSE>(a, u, t, m, ks, ds);
+            if (bits) mp_mark(a, u, bits, any_acc);
+        }
+        return;
+    }
     const uint32_t Mlo = (uint32_t)M, Mhi = (uint32_t)(M >> 32);
     const bool act0 = (Mlo >> lane) & 1u, act1 = (Mhi >> lane) & 1u;
     const bool w0 = ((uint32_t)a.wmask >> lane) & 1u, w1 = ((uint32_t)(a.wmask >> 32) >> lane) & 1u;
@@ -164,20 +280,22 @@ __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e
                 bool i0 = false, i1 = false;
                 if (act0) {
                     const uint32_t nd = d0 + (w0 ? t[q] : 0u);
-                    if (nd < c0[q]) i0 = nd < atomicMin(&a.dist[(uint64_t)u[q] * MP_K + lane], nd);
+                    if (nd < c0[q]) {
+                        atomicMin(&a.dist[(uint64_t)u[q] * MP_K + lane], nd);
+                        i0 = true;
+                    }
                 }
                 if (act1) {
                     const uint32_t nd = d1 + (w1 ? t[q] : 0u);
-                    if (nd < c1[q]) i1 = nd < atomicMin(&a.dist[(uint64_t)u[q] * MP_K + 32 + lane], nd);
+                    if (nd < c1[q]) {
+                        atomicMin(&a.dist[(uint64_t)u[q] * MP_K + 32 + lane], nd);
+                        i1 = true;
+                    }
                 }
                 const uint32_t b0 = Mlo ? __ballot_sync(FULL, i0) : 0u;
                 const uint32_t b1 = Mhi ? __ballot_sync(FULL, i1) : 0u;
-                if ((b0 | b1) && lane == 0) {
-                    const unsigned long long bits = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
-                    const unsigned long long old = atomicOr((unsigned long long*)&a.next[u[q]], bits);
-                    if (!old) atomicOr(&a.fbm[u[q] >> 5], 1u << (u[q] & 31));
-                    any_acc |= bits;
-                }
+                if ((b0 | b1) && lane == 0)
+                    mp_mark(a, u[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32), any_acc);
             }
         }
     }
@@ -196,9 +314,36 @@ __device__ __forceinline__ void mp_block_any(unsigned long long x, unsigned long
     }
 }
 
-// A warp per frontier vertex (classes 0 and 1).
-__global__ void __launch_bounds__(SRV_THREADS) k_mp_vertices(MpArgs a, const uint32_t* __restrict__ list,
-                                                             const uint32_t* __restrict__ count)
+// A thread per low-degree frontier vertex (class 0): its edges one by one,
+// all its lanes at each, MP_SPARSE at a time.
+__global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_thread(MpArgs a, const uint32_t* __restrict__ list,
+                                                                     const uint32_t* __restrict__ count)
+{
+    const uint32_t n = *count;
+    unsigned long long acc = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = list[i];
+        uint64_t M = a.front[v];
+        const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
+        while (M) {
+            int ks[MP_SPARSE];
+            uint32_t ds[MP_SPARSE];
+            const int m = mp_lanes(a, v, M, ks, ds);
+            for (int j = 0; j < m; j++) M &= ~(1ULL << ks[j]);
+            for (uint64_t e = e0; e < e1; e++) {
+                const uint32_t u = a.adj[e];
+                const uint32_t t = a.wgt ? a.wgt[e] : 0u;
+                const unsigned long long bits = mp_relax_edge<MP_SPARSE>(a, u, t, m, ks, ds);
+                if (bits) mp_mark(a, u, bits, acc);
+            }
+        }
+    }
+    mp_block_any(acc, a.any);
+}
+
+// A warp per frontier vertex (class 1).
+__global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_vertices(MpArgs a, const uint32_t* __restrict__ list,
+                                                                       const uint32_t* __restrict__ count)
 {
     const uint32_t n = *count;
     unsigned long long acc = 0;
@@ -211,9 +356,9 @@ __global__ void __launch_bounds__(SRV_THREADS) k_mp_vertices(MpArgs a, const uin
 }
 
 // A warp per HUB_CHUNK edges of a frontier hub (class 2).
-__global__ void __launch_bounds__(SRV_THREADS) k_mp_hubs(MpArgs a, const uint32_t* __restrict__ list,
-                                                         const uint32_t* __restrict__ count,
-                                                         const uint32_t* __restrict__ prefix)
+__global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_hubs(MpArgs a, const uint32_t* __restrict__ list,
+                                                                   const uint32_t* __restrict__ count,
+                                                                   const uint32_t* __restrict__ prefix)
 {
     const uint32_t n = *count;
     unsigned long long acc = 0;
@@ -243,8 +388,8 @@ __global__ void k_mp_clear(uint64_t* __restrict__ front, const uint32_t* __restr
     }
 }
 
-// Lane k of every vertex to `init` (INF for SSSP, the vertex id for CC, which
-// also joins every vertex to the frontier of lane k).
+// Lane k of every vertex to INF (SSSP), or to the vertex id with every vertex
+// in lane k's frontier (CC by label propagation).
 __global__ void k_mp_init_lane(uint32_t* __restrict__ dist, uint64_t* __restrict__ front, uint64_t V, int k, int cc)
 {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
@@ -290,6 +435,111 @@ __global__ void k_mp_extract(const uint32_t* __restrict__ dist, uint64_t V, int 
 }
 
 // ---------------------------------------------------------------------------
+// Connected components of a symmetric graph by union-find
+// ---------------------------------------------------------------------------
+// On a symmetric graph min-label propagation (benchmarks/cc.c) ends with every
+// vertex labelled by the least id of its component.  Union-find reaches the
+// same labels in one pass over the edges: a root is only ever hooked under a
+// smaller root (so parents point to smaller ids and the root of a component
+// is its least id), then every vertex is pointed at its root.  Parents are
+// read through L2 (__ldcg); a stale parent is still an ancestor, and a failed
+// compare-and-swap returns the current parent.
+constexpr uint32_t CC_RETRIES = 1u << 24;  // hook attempts before an error
+
+__device__ __forceinline__ uint32_t cc_find(uint32_t* p, uint32_t v)
+{
+    uint32_t x = __ldcg(&p[v]);
+    while (x != v) {
+        const uint32_t y = __ldcg(&p[x]);
+        if (y != x) p[v] = y;  // path halving: y is an ancestor of v too
+        v = x;
+        x = y;
+    }
+    return v;
+}
+
+__device__ __forceinline__ void cc_hook(uint32_t* p, uint32_t a, uint32_t b, uint32_t* err)
+{
+    uint32_t ra = cc_find(p, a), rb = cc_find(p, b);
+    for (uint32_t tries = 0; ra != rb; tries++) {
+        if (tries == CC_RETRIES) {
+            atomicOr(err, 1u);
+            return;
+        }
+        if (ra > rb) {
+            const uint32_t t = ra;
+            ra = rb;
+            rb = t;
+        }
+        const uint32_t old = atomicCAS(&p[rb], rb, ra);
+        if (old == rb) return;
+        rb = cc_find(p, old);
+        ra = cc_find(p, ra);
+    }
+}
+
+__global__ void k_cc_init(uint32_t* __restrict__ p, uint64_t V, uint32_t* __restrict__ err)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        p[v] = (uint32_t)v;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
+}
+
+// Each undirected edge once, from its larger end: a thread per vertex of
+// class 0, a warp per vertex of class 1, a warp per HUB_CHUNK edges of a hub.
+__global__ void k_cc_hook_thread(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
+                                 const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = list[i];
+        for (uint64_t e = row[v]; e < row[v + 1]; e++) {
+            const uint32_t u = adj[e];
+            if (u < v) cc_hook(p, v, u, err);
+        }
+    }
+}
+
+__global__ void k_cc_hook_warp(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
+                               const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint32_t v = list[i];
+        for (uint64_t e = row[v] + lane; e < row[v + 1]; e += 32) {
+            const uint32_t u = adj[e];
+            if (u < v) cc_hook(p, v, u, err);
+        }
+    }
+}
+
+__global__ void k_cc_hook_hub(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
+                              const uint32_t* __restrict__ list, uint32_t n, const uint32_t* __restrict__ prefix,
+                              uint32_t* p, uint32_t* err)
+{
+    if (!n) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = prefix[n];
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
+        const uint32_t i = hub_of_chunk(prefix, n, (uint32_t)c);
+        const uint32_t v = list[i];
+        const uint64_t e0 = row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
+        const uint64_t e1 = e0 + HUB_CHUNK < row[v + 1] ? e0 + HUB_CHUNK : row[v + 1];
+        for (uint64_t e = e0 + lane; e < e1; e += 32) {
+            const uint32_t u = adj[e];
+            if (u < v) cc_hook(p, v, u, err);
+        }
+    }
+}
+
+__global__ void k_cc_compress(uint32_t* p, uint64_t V)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        p[v] = cc_find(p, (uint32_t)v);
+}
+
+// ---------------------------------------------------------------------------
 // PPR lanes
 // ---------------------------------------------------------------------------
 struct PpLanes {
@@ -306,6 +556,7 @@ struct PpArgs {
     float2* __restrict__ partial;  // (sum, compensation) per hub chunk and lane
 };
 
+// Compensated addition (TwoSum carries the rounding error of s + x in c).
 __device__ __forceinline__ void pp_add(float& s, float& c, float x)
 {
     const float t = __fadd_rn(s, x);
@@ -318,6 +569,12 @@ __device__ __forceinline__ void pp_merge(float& s, float& c, float s2, float c2)
 {
     pp_add(s, c, s2);
     c = __fadd_rn(c, c2);
+}
+
+// x of lane k at v from its gathered sum (ppr application: 0.15 at the seed).
+__device__ __forceinline__ float pp_value(const PpLanes& L, int k, uint64_t v, float sum)
+{
+    return __fadd_rn(L.seed[k] == (uint32_t)v ? 0.15f : 0.0f, __fmul_rn(0.85f, sum));
 }
 
 // Half-warp h sums lane k of b_cur over the edges e0 + 2i + h of [e0, e1).
@@ -348,14 +605,55 @@ __device__ __forceinline__ void pp_finish(const PpArgs& a, const PpLanes& L, uin
     if (k >= PP_K) return;
     float bn = 0.0f;
     if ((L.active >> k) & 1u) {
-        const float sum = __fadd_rn(s, c);
-        const float xn = __fadd_rn(L.seed[k] == (uint32_t)v ? 0.15f : 0.0f, __fmul_rn(0.85f, sum));
+        const float xn = pp_value(L, k, v, __fadd_rn(s, c));
         if (L.out[k]) L.out[k][v] = xn;
         else if (deg) bn = __fdiv_rn(xn, (float)deg);
     }
     a.b_next[v * PP_K + k] = bn;
 }
 
+// A thread per low-degree vertex (class 0): each in-neighbour's lane row
+// read as NQ float4 quads (lanes 4 NQ and up are idle, their quotients 0)
+// and summed per lane in edge order.
+template <int NQ>
+__global__ void __launch_bounds__(SRV_THREADS, 4) k_pp_thread(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+                                                              uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = list[i];
+        const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
+        float s[4 * NQ], c[4 * NQ];
+#pragma unroll
+        for (int k = 0; k < 4 * NQ; k++) s[k] = c[k] = 0.0f;
+        for (uint64_t e = e0; e < e1; e++) {
+            const float4* r = reinterpret_cast<const float4*>(a.b_cur + (uint64_t)a.adj[e] * PP_K);
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const float4 x = r[q];
+                pp_add(s[4 * q + 0], c[4 * q + 0], x.x);
+                pp_add(s[4 * q + 1], c[4 * q + 1], x.y);
+                pp_add(s[4 * q + 2], c[4 * q + 2], x.z);
+                pp_add(s[4 * q + 3], c[4 * q + 3], x.w);
+            }
+        }
+        const uint64_t deg = e1 - e0;
+        float bn[PP_K];
+#pragma unroll
+        for (int k = 0; k < PP_K; k++) {
+            bn[k] = 0.0f;
+            if (k < 4 * NQ && ((L.active >> k) & 1u)) {
+                const float xn = pp_value(L, k, v, __fadd_rn(s[k], c[k]));
+                if (L.out[k]) L.out[k][v] = xn;
+                else if (deg) bn[k] = __fdiv_rn(xn, (float)deg);
+            }
+        }
+        float4* w = reinterpret_cast<float4*>(a.b_next + v * PP_K);
+#pragma unroll
+        for (int q = 0; q < PP_K / 4; q++) w[q] = make_float4(bn[4 * q], bn[4 * q + 1], bn[4 * q + 2], bn[4 * q + 3]);
+    }
+}
+
+// A warp per vertex (class 1): half-warps over alternate edges, a lane each.
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                              uint64_t n)
 {
@@ -373,6 +671,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L
     }
 }
 
+// Hubs (class 2): a warp per HUB_CHUNK edges, partial sums per chunk and lane...
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                                uint32_t n, const uint32_t* __restrict__ prefix)
 {
@@ -394,6 +693,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes
     }
 }
 
+// ...then a warp per hub merges its chunks' partials in chunk order.
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_finish(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                                uint32_t n, const uint32_t* __restrict__ prefix)
 {
@@ -440,13 +740,21 @@ struct Graph {
     ipg_graph_view gv{};
     Group* mp = nullptr;
     Group* pp = nullptr;
+    // degree classes over all vertices and the chunk prefix of their hubs,
+    // built at first use by the PPR gathers and the union-find pass
+    ipg_bins bins{};
+    uint32_t* hub_prefix = nullptr;  // nh + 1 entries, then the hub count and the union-find error word
+    uint64_t hub_chunks = 0;
+    uint32_t* cc_err = nullptr;
+    bool classes = false;
 };
 
 struct Group {
     int kind = 0;  // 0 min-plus, 1 PPR
     Graph* G = nullptr;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr;   // end of the superstep in flight
+    cudaEvent_t ev0 = nullptr;  // its start
     bool running = false;
     uint64_t busy = 0;
     std::vector<std::vector<uint64_t>> lane_q;  // queries on each lane
@@ -459,21 +767,21 @@ struct Group {
     int cur = 0;
     uint32_t* fbm = nullptr;
     uint32_t* list[3] = {nullptr, nullptr, nullptr};
-    uint32_t* cnt = nullptr;
+    uint32_t* cnt = nullptr;              // into stat_d
     uint32_t* prefix = nullptr;
-    unsigned long long* any_d = nullptr;
-    unsigned long long* any_h = nullptr;
+    unsigned long long* any_d = nullptr;  // into stat_d
+    MpStatus* stat_d = nullptr;
+    MpStatus* stat_h = nullptr;           // pinned copy after each superstep
+    uint32_t hn[3] = {0, 0, 0};           // list sizes the host knows of
+    uint32_t hchunks = 0;                 // hub chunks of list 2
+    uint32_t appended = 0;                // sources appended since
     uint64_t wmask = 0;
-    int cc_lane = -1;  // CC lane admitted in the current admission round
+    int cc_lane = -1;  // label-propagation CC lane admitted in this round
     // PPR
     float* b[2] = {nullptr, nullptr};
     float2* partial = nullptr;
-    uint32_t* pp_prefix = nullptr;
-    uint32_t* pp_count2 = nullptr;
-    ipg_bins bins{};
     int it[PP_K] = {0};
     uint32_t seed[PP_K] = {0};
-    uint32_t grid = 0;
     uint64_t supersteps = 0;
 };
 
@@ -501,13 +809,14 @@ struct ipg_server {
     std::map<uint64_t, Query> queries;
     std::vector<std::deque<uint64_t>> pending;  // per graph and group kind: gid * 2 + kind
     uint64_t n_pending = 0;
-    std::vector<uint64_t> finishing;            // results being extracted
+    std::vector<uint64_t> finishing;            // results being completed on the device
     std::vector<uint64_t> completed;            // done since the last drain
-    std::multimap<uint64_t, void*> pool;  // released result buffers by size
+    std::vector<double> busy_s;                 // per graph and group kind: superstep device time
+    std::vector<uint64_t> steps, lanes;         // supersteps, lanes admitted
+    std::multimap<uint64_t, void*> pool;        // released result buffers by size
     uint64_t next_id = 1;
     std::mutex mu;
     ipg_server_stats stats{};
-    int sms = 148;
 };
 
 namespace {
@@ -516,8 +825,9 @@ void free_group(ipg_server* S, Group* G)
 {
     if (G->st) cudaStreamSynchronize(G->st);
     for (auto& a : G->allocs) ipg_dev_free(a.first, a.second);
-    if (G->any_h) cudaFreeHost(G->any_h);
+    if (G->stat_h) cudaFreeHost(G->stat_h);
     if (G->ev) cudaEventDestroy(G->ev);
+    if (G->ev0) cudaEventDestroy(G->ev0);
     if (G->st) cudaStreamDestroy(G->st);
     S->in_use -= G->bytes;
     if (G->G->mp == G) G->G->mp = nullptr;
@@ -531,10 +841,11 @@ uint64_t group_bytes(const Graph* G, int kind)
 {
     const uint64_t V = G->gv.V, E = G->gv.E;
     if (kind == 0) return V * (MP_K * 4 + 16 + 12) + V / 8 + (E / (MP_T1 + 1) + 2) * 4 + 4096;
-    return V * (PP_K * 4 * 2) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8 + 4) + 4096;
+    return V * (PP_K * 4 * 2) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8) + 4096;
 }
 
-// Frees idle groups (least recently used first) until `need` more bytes fit.
+// Frees idle groups (least recently used first), then cached result buffers,
+// until `need` more bytes fit the budget.
 bool make_room(ipg_server* S, uint64_t need)
 {
     if (!S->budget) return true;
@@ -546,7 +857,6 @@ bool make_room(ipg_server* S, uint64_t need)
             free_group(S, victim);
             continue;
         }
-        // cached result buffers go next
         if (!S->pool.empty()) {
             auto it = S->pool.begin();
             ipg_dev_free(it->second, it->first);
@@ -559,9 +869,51 @@ bool make_room(ipg_server* S, uint64_t need)
     return true;
 }
 
-int create_group(ipg_server* S, Graph* Gr, int kind, Group** out)
+// Degree classes of all vertices of a graph and the chunk prefix of its hubs
+// (built once; the PPR gathers and the union-find pass use them).
+int graph_classes(Graph* Gr, cudaStream_t st)
 {
-    *out = nullptr;
+    if (Gr->classes) return IPG_OK;
+    int r = ipg_graph_bins(Gr->g, 0, MP_T0, MP_T1, &Gr->bins);
+    if (r != IPG_OK) return r;
+    const uint64_t nh = Gr->bins.count[2];
+    void* p = nullptr;
+    if ((r = ipg_dev_alloc(&p, (nh + 4) * 4)) != IPG_OK) return r;
+    Gr->hub_prefix = (uint32_t*)p;
+    uint32_t* count = Gr->hub_prefix + nh + 2;
+    Gr->cc_err = count + 1;
+    const uint32_t n2 = (uint32_t)nh;
+    uint32_t chunks = 0;
+    cudaMemcpyAsync(count, &n2, 4, cudaMemcpyHostToDevice, st);
+    k_chunk_prefix<<<1, 1024, 0, st>>>(Gr->bins.d_list[2], count, Gr->gv.d_row, Gr->hub_prefix, nullptr);
+    cudaMemcpyAsync(&chunks, Gr->hub_prefix + nh, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return ipg_internal_fail(IPG_ECUDA, "serve: hub prefix failed");
+    Gr->hub_chunks = chunks;
+    Gr->classes = true;
+    return IPG_OK;
+}
+
+// Union-find CC of a symmetric graph into p (V labels).
+void run_union_find(Graph* Gr, uint32_t* p, cudaStream_t st)
+{
+    const ipg_graph_view& gv = Gr->gv;
+    const ipg_bins& B = Gr->bins;
+    const uint32_t* adj = (const uint32_t*)gv.d_adj;
+    k_cc_init<<<resident_cap(k_cc_init, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(p, gv.V, Gr->cc_err);
+    if (B.count[0])
+        k_cc_hook_thread<<<resident_cap(k_cc_hook_thread, thread_grid(B.count[0])), SRV_THREADS, 0, st>>>(
+            gv.d_row, adj, B.d_list[0], B.count[0], p, Gr->cc_err);
+    if (B.count[1])
+        k_cc_hook_warp<<<resident_cap(k_cc_hook_warp, warp_grid(B.count[1])), SRV_THREADS, 0, st>>>(
+            gv.d_row, adj, B.d_list[1], B.count[1], p, Gr->cc_err);
+    if (B.count[2])
+        k_cc_hook_hub<<<resident_cap(k_cc_hook_hub, warp_grid(Gr->hub_chunks)), SRV_THREADS, 0, st>>>(
+            gv.d_row, adj, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix, p, Gr->cc_err);
+    k_cc_compress<<<resident_cap(k_cc_compress, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(p, gv.V);
+}
+
+int create_group(ipg_server* S, Graph* Gr, int kind)
+{
     const uint64_t need = group_bytes(Gr, kind);
     if (!make_room(S, need)) return IPG_EBUDGET;
     Group* G = new Group();
@@ -570,51 +922,49 @@ int create_group(ipg_server* S, Graph* Gr, int kind, Group** out)
     G->lane_q.resize(kind == 0 ? MP_K : PP_K);
     const uint64_t V = Gr->gv.V, E = Gr->gv.E;
     int r = IPG_OK;
-    cudaError_t e = cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&G->ev, cudaEventDisableTiming);
+    // smaller graphs get higher-priority streams: their supersteps are short,
+    // and their CTAs go first whenever SMs free up
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    int lg = 0;
+    while ((1ULL << (lg + 1)) <= V) lg++;
+    const int prio = std::min(least, greatest + std::max(0, lg - 18));
+    cudaError_t e = cudaStreamCreateWithPriority(&G->st, cudaStreamNonBlocking, prio);
+    if (e == cudaSuccess) e = cudaEventCreate(&G->ev);
+    if (e == cudaSuccess) e = cudaEventCreate(&G->ev0);
     if (e != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
-    int occ = 0;
     if (kind == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mp_vertices, SRV_THREADS, 0);
         if (r == IPG_OK) r = galloc(G, &G->dist, V * MP_K);
         if (r == IPG_OK) r = galloc(G, &G->front[0], V);
         if (r == IPG_OK) r = galloc(G, &G->front[1], V);
         if (r == IPG_OK) r = galloc(G, &G->fbm, (V + 31) / 32 + 1);
         for (int k = 0; k < 3 && r == IPG_OK; k++) r = galloc(G, &G->list[k], V);
-        if (r == IPG_OK) r = galloc(G, &G->cnt, 8);
+        if (r == IPG_OK) r = galloc(G, &G->stat_d, 1);
+        if (r == IPG_OK) {
+            G->cnt = G->stat_d->cnt;
+            G->any_d = &G->stat_d->any;
+        }
         if (r == IPG_OK) r = galloc(G, &G->prefix, E / (MP_T1 + 1) + 2);
-        if (r == IPG_OK) r = galloc(G, &G->any_d, 1);
-        if (r == IPG_OK && cudaHostAlloc((void**)&G->any_h, 8, cudaHostAllocDefault) != cudaSuccess)
+        if (r == IPG_OK && cudaHostAlloc((void**)&G->stat_h, sizeof(MpStatus), cudaHostAllocDefault) != cudaSuccess)
             r = ipg_internal_fail(IPG_ENOMEM, "serve: pinned allocation failed");
         if (r == IPG_OK) {
             cudaMemsetAsync(G->front[0], 0, V * 8, G->st);
             cudaMemsetAsync(G->front[1], 0, V * 8, G->st);
             cudaMemsetAsync(G->fbm, 0, ((V + 31) / 32 + 1) * 4, G->st);
-            cudaMemsetAsync(G->cnt, 0, 32, G->st);
+            cudaMemsetAsync(G->stat_d, 0, sizeof(MpStatus), G->st);
+            cudaMemsetAsync(G->prefix, 0, 8, G->st);
         }
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pp_vertices, SRV_THREADS, 0);
-        if (r == IPG_OK) r = ipg_graph_bins(Gr->g, 0, MP_T0, MP_T1, &G->bins);
+        if (r == IPG_OK) r = graph_classes(Gr, G->st);
         if (r == IPG_OK) r = galloc(G, &G->b[0], V * PP_K);
         if (r == IPG_OK) r = galloc(G, &G->b[1], V * PP_K);
-        const uint64_t nh = G->bins.count[2];
-        if (r == IPG_OK) r = galloc(G, &G->pp_prefix, nh + 2);
-        if (r == IPG_OK) r = galloc(G, &G->pp_count2, 1);
-        uint32_t chunks = 0;
+        if (r == IPG_OK) r = galloc(G, &G->partial, Gr->hub_chunks * PP_K);
         if (r == IPG_OK) {
-            const uint32_t n2 = (uint32_t)nh;
-            cudaMemcpyAsync(G->pp_count2, &n2, 4, cudaMemcpyHostToDevice, G->st);
-            k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->bins.d_list[2], G->pp_count2, Gr->gv.d_row, G->pp_prefix);
-            cudaMemcpyAsync(&chunks, G->pp_prefix + nh, 4, cudaMemcpyDeviceToHost, G->st);
-            if (cudaStreamSynchronize(G->st) != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, "serve: hub prefix failed");
-        }
-        if (r == IPG_OK) r = galloc(G, &G->partial, (uint64_t)chunks * PP_K);
-        if (r == IPG_OK) {
+            // quotients of idle lanes are 0: an admitted lane sets its seed only
             cudaMemsetAsync(G->b[0], 0, V * PP_K * 4, G->st);
             cudaMemsetAsync(G->b[1], 0, V * PP_K * 4, G->st);
         }
     }
-    G->grid = (uint32_t)S->sms * (uint32_t)std::max(1, std::min(occ, 8));
     if (r == IPG_OK && cudaGetLastError() != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, "serve: group setup failed");
     S->in_use += G->bytes;
     S->groups.push_back(G);
@@ -650,6 +1000,14 @@ void release_result(ipg_server* S, Query& q)
     q.result = nullptr;
 }
 
+void finishing(ipg_server* S, Query& q, cudaStream_t st)
+{
+    cudaEventCreateWithFlags(&q.ready, cudaEventDisableTiming);
+    cudaEventRecord(q.ready, st);
+    q.state = IPG_QUERY_FINISHING;
+    S->finishing.push_back(q.id);
+}
+
 // Pending queries of group G's graph and kind take free lanes.
 void admit(ipg_server* S, Group* G, double now)
 {
@@ -659,13 +1017,37 @@ void admit(ipg_server* S, Group* G, double now)
     const uint64_t full = K == 64 ? ~0ULL : ((1ULL << K) - 1);
     G->cc_lane = -1;
     bool rebuild = false;
+    void* cc_first = nullptr;  // result of this round's union-find pass
     for (auto it = queue.begin(); it != queue.end();) {
         Query& q = S->queries[*it];
+        const bool union_find = q.kind == IPG_QUERY_CC && G->G->gv.symmetric;
         const bool joins_cc = q.kind == IPG_QUERY_CC && G->cc_lane >= 0;
-        if (!joins_cc && (G->busy & full) == full) break;  // no lane free
+        if (!union_find && !joins_cc && (G->busy & full) == full) break;  // no lane free
         const uint64_t rbytes = V * 4;
         if (take_result(S, q, rbytes) != IPG_OK) {
             ++it;
+            continue;
+        }
+        q.state = IPG_QUERY_RUNNING;
+        q.t_start = now;
+        if (union_find) {
+            // CC queries admitted together share one union-find pass
+            if (!cc_first) {
+                if (graph_classes(G->G, G->st) != IPG_OK) {
+                    release_result(S, q);
+                    q.state = IPG_QUERY_PENDING;
+                    ++it;
+                    continue;
+                }
+                run_union_find(G->G, (uint32_t*)q.result, G->st);
+                cc_first = q.result;
+                S->stats.kernel_launches += 5;
+            } else {
+                cudaMemcpyAsync(q.result, cc_first, rbytes, cudaMemcpyDeviceToDevice, G->st);
+            }
+            finishing(S, q, G->st);
+            it = queue.erase(it);
+            S->n_pending--;
             continue;
         }
         int k;
@@ -674,7 +1056,7 @@ void admit(ipg_server* S, Group* G, double now)
         } else {
             k = __builtin_ctzll(~G->busy);
             G->busy |= 1ULL << k;
-            const uint32_t g = G->grid;
+            const uint32_t g = resident_cap(k_mp_init_lane, thread_grid(V));
             if (q.kind == IPG_QUERY_PPR) {
                 k_pp_admit<<<1, 1, 0, G->st>>>(G->b[G->cur], G->G->gv.d_row, q.src, k);
                 G->it[k] = 0;
@@ -689,28 +1071,36 @@ void admit(ipg_server* S, Group* G, double now)
                 k_mp_admit_source<<<1, 1, 0, G->st>>>(G->dist, G->front[G->cur], G->G->gv.d_row, q.src, k,
                                                        G->list[0], G->list[1], G->list[2], G->cnt);
                 G->wmask |= 1ULL << k;
+                G->appended++;
             }
             S->stats.lanes_admitted++;
+            S->lanes[(size_t)G->G->gid * 2 + G->kind]++;
         }
         G->lane_q[k].push_back(q.id);
-        q.state = IPG_QUERY_RUNNING;
-        q.t_start = now;
         it = queue.erase(it);
         S->n_pending--;
     }
     if (rebuild) {
-        // a CC lane puts every vertex into the frontier: rebuild the lists
-        k_mp_mark_all<<<G->grid, SRV_THREADS, 0, G->st>>>(G->front[G->cur], V, G->fbm);
+        // a label-propagation CC lane puts every vertex into the frontier:
+        // rebuild the lists and read their sizes back (grids are sized by them)
+        k_mp_mark_all<<<resident_cap(k_mp_mark_all, thread_grid((V + 31) / 32)), SRV_THREADS, 0, G->st>>>(
+            G->front[G->cur], V, G->fbm);
         cudaMemsetAsync(G->cnt, 0, 12, G->st);
         ipg_compact(G->fbm, V, G->G->gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
                     G->st);
+        k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, G->G->gv.d_row, G->prefix, &G->stat_d->chunks);
+        cudaMemcpyAsync(G->stat_h, G->stat_d, sizeof(MpStatus), cudaMemcpyDeviceToHost, G->st);
+        cudaStreamSynchronize(G->st);
+        for (int c = 0; c < 3; c++) G->hn[c] = G->stat_h->cnt[c];
+        G->hchunks = G->stat_h->chunks;
+        G->appended = 0;
     }
 }
 
 int launch_superstep(ipg_server* S, Group* G)
 {
-    const uint32_t g = G->grid;
     const ipg_graph_view& gv = G->G->gv;
+    cudaEventRecord(G->ev0, G->st);
     if (G->kind == 0) {
         MpArgs a;
         a.row = gv.d_row;
@@ -722,19 +1112,30 @@ int launch_superstep(ipg_server* S, Group* G)
         a.fbm = G->fbm;
         a.any = G->any_d;
         a.wmask = G->wmask;
+        // grids from the list sizes of the last status plus the sources
+        // appended since (each in some list; a hub one adds its chunks)
+        const uint64_t add = G->appended;
+        const uint64_t hub_chunks_max = (gv.max_out_degree + HUB_CHUNK - 1) / HUB_CHUNK;
+        const uint64_t n0 = G->hn[0] + add, n1 = G->hn[1] + add;
+        const uint64_t chunks = G->hchunks + add * hub_chunks_max;
         cudaMemsetAsync(G->any_d, 0, 8, G->st);
-        k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix);
-        k_mp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[0], G->cnt + 0);
-        k_mp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[1], G->cnt + 1);
-        k_mp_hubs<<<g, SRV_THREADS, 0, G->st>>>(a, G->list[2], G->cnt + 2, G->prefix);
-        k_mp_clear<<<g, SRV_THREADS, 0, G->st>>>(G->front[G->cur], G->list[0], G->list[1], G->list[2], G->cnt);
+        if (add) k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, nullptr);
+        k_mp_thread<<<resident_cap(k_mp_thread, thread_grid(n0)), SRV_THREADS, 0, G->st>>>(a, G->list[0], G->cnt + 0);
+        k_mp_vertices<<<resident_cap(k_mp_vertices, warp_grid(n1)), SRV_THREADS, 0, G->st>>>(a, G->list[1],
+                                                                                          G->cnt + 1);
+        k_mp_hubs<<<resident_cap(k_mp_hubs, warp_grid(chunks)), SRV_THREADS, 0, G->st>>>(a, G->list[2], G->cnt + 2,
+                                                                                      G->prefix);
+        k_mp_clear<<<resident_cap(k_mp_clear, thread_grid(G->hn[0] + G->hn[1] + G->hn[2] + add)), SRV_THREADS, 0,
+                     G->st>>>(G->front[G->cur], G->list[0], G->list[1], G->list[2], G->cnt);
         cudaMemsetAsync(G->cnt, 0, 12, G->st);
         ipg_compact(G->fbm, gv.V, gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
                     G->st);
-        cudaMemcpyAsync(G->any_h, G->any_d, 8, cudaMemcpyDeviceToHost, G->st);
+        k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, &G->stat_d->chunks);
+        cudaMemcpyAsync(G->stat_h, G->stat_d, sizeof(MpStatus), cudaMemcpyDeviceToHost, G->st);
         G->cur ^= 1;
-        S->stats.kernel_launches += 6;
+        S->stats.kernel_launches += 7 + (add ? 1 : 0);
     } else {
+        const Graph* Gr = G->G;
         PpArgs a;
         a.row = gv.d_row;
         a.adj = (const uint32_t*)gv.d_adj;
@@ -749,12 +1150,30 @@ int launch_superstep(ipg_server* S, Group* G)
             if (((G->busy >> k) & 1) && G->it[k] + 1 == (int)S->rounds)
                 L.out[k] = (float*)S->queries[G->lane_q[k][0]].result;
         }
-        const ipg_bins& B = G->bins;
-        if (B.count[0]) k_pp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], B.count[0]);
-        if (B.count[1]) k_pp_vertices<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[1], B.count[1]);
+        const ipg_bins& B = Gr->bins;
+        // quads of lanes in use: lanes are taken lowest first
+        const int top = 32 - __builtin_clz((uint32_t)G->busy | 1u);
+        const int nq = (top + 3) / 4;
+        const uint64_t n0 = B.count[0];
+        if (n0) {
+            const uint32_t gt = thread_grid(n0);
+            if (nq <= 1)
+                k_pp_thread<1><<<resident_cap(k_pp_thread<1>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
+            else if (nq == 2)
+                k_pp_thread<2><<<resident_cap(k_pp_thread<2>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
+            else if (nq == 3)
+                k_pp_thread<3><<<resident_cap(k_pp_thread<3>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
+            else
+                k_pp_thread<4><<<resident_cap(k_pp_thread<4>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
+        }
+        if (B.count[1])
+            k_pp_vertices<<<resident_cap(k_pp_vertices, warp_grid(B.count[1])), SRV_THREADS, 0, G->st>>>(
+                a, L, B.d_list[1], B.count[1]);
         if (B.count[2]) {
-            k_pp_hub_chunks<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[2], (uint32_t)B.count[2], G->pp_prefix);
-            k_pp_hub_finish<<<g, SRV_THREADS, 0, G->st>>>(a, L, B.d_list[2], (uint32_t)B.count[2], G->pp_prefix);
+            k_pp_hub_chunks<<<resident_cap(k_pp_hub_chunks, warp_grid(Gr->hub_chunks)), SRV_THREADS, 0, G->st>>>(
+                a, L, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix);
+            k_pp_hub_finish<<<resident_cap(k_pp_hub_finish, warp_grid(B.count[2])), SRV_THREADS, 0, G->st>>>(
+                a, L, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix);
         }
         G->cur ^= 1;
         S->stats.kernel_launches += 4;
@@ -772,17 +1191,18 @@ int launch_superstep(ipg_server* S, Group* G)
 void retire(ipg_server* S, Group* G, double now)
 {
     if (G->kind == 0) {
-        const uint64_t live = *G->any_h;
+        const uint64_t live = G->stat_h->any;
+        for (int c = 0; c < 3; c++) G->hn[c] = G->stat_h->cnt[c];
+        G->hchunks = G->stat_h->chunks;
+        G->appended = 0;
         const uint64_t done = G->busy & ~live;
         for (int k = 0; k < MP_K; k++) {
             if (!((done >> k) & 1)) continue;
             for (uint64_t qid : G->lane_q[k]) {
                 Query& q = S->queries[qid];
-                k_mp_extract<<<G->grid, SRV_THREADS, 0, G->st>>>(G->dist, G->G->gv.V, k, (uint32_t*)q.result);
-                cudaEventCreateWithFlags(&q.ready, cudaEventDisableTiming);
-                cudaEventRecord(q.ready, G->st);
-                q.state = IPG_QUERY_FINISHING;
-                S->finishing.push_back(qid);
+                k_mp_extract<<<resident_cap(k_mp_extract, thread_grid(G->G->gv.V)), SRV_THREADS, 0, G->st>>>(
+                    G->dist, G->G->gv.V, k, (uint32_t*)q.result);
+                finishing(S, q, G->st);
             }
             G->lane_q[k].clear();
             if (G->cc_lane == k) G->cc_lane = -1;
@@ -813,7 +1233,6 @@ extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_s
     if (!S) return ipg_internal_fail(IPG_ENOMEM, "ipg_server_create: out of host memory");
     S->budget = hbm_budget;
     S->rounds = ppr_rounds;
-    S->sms = ipg_sm_count();
     *out = S;
     return IPG_OK;
 }
@@ -823,10 +1242,15 @@ extern "C" void ipg_server_free(ipg_server* S)
     if (!S) return;
     while (!S->groups.empty()) free_group(S, S->groups.back());
     for (auto& kv : S->queries) {
-        if (kv.second.ready) cudaEventDestroy(kv.second.ready);
+        if (kv.second.ready) {
+            cudaEventSynchronize(kv.second.ready);
+            cudaEventDestroy(kv.second.ready);
+        }
         if (kv.second.result) ipg_dev_free(kv.second.result, kv.second.result_bytes);
     }
     for (auto& kv : S->pool) ipg_dev_free(kv.second, kv.first);
+    for (auto& g : S->graphs)
+        if (g->hub_prefix) ipg_dev_free(g->hub_prefix, (g->bins.count[2] + 4) * 4);
     delete S;
 }
 
@@ -845,6 +1269,9 @@ extern "C" int ipg_server_add_graph(ipg_server* S, ipg_graph* g, int* gid)
     G->gid = *gid;
     S->graphs.push_back(std::move(G));
     S->pending.resize(S->graphs.size() * 2);
+    S->busy_s.resize(S->graphs.size() * 2, 0.0);
+    S->steps.resize(S->graphs.size() * 2, 0);
+    S->lanes.resize(S->graphs.size() * 2, 0);
     return IPG_OK;
 }
 
@@ -880,20 +1307,26 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
     if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_poll: null server");
     std::lock_guard<std::mutex> lk(S->mu);
     const double now = now_s();
-    // results whose extraction finished
+    // results completed on the device
     for (size_t i = 0; i < S->finishing.size();) {
         Query& q = S->queries[S->finishing[i]];
-        if (cudaEventQuery(q.ready) == cudaSuccess) {
-            cudaEventDestroy(q.ready);
-            q.ready = nullptr;
-            q.state = IPG_QUERY_DONE;
-            q.t_done = now;
-            S->completed.push_back(q.id);
-            S->finishing[i] = S->finishing.back();
-            S->finishing.pop_back();
-        } else {
+        if (cudaEventQuery(q.ready) != cudaSuccess) {
             i++;
+            continue;
         }
+        cudaEventDestroy(q.ready);
+        q.ready = nullptr;
+        const Graph* Gr = S->graphs[q.gid].get();
+        if (q.kind == IPG_QUERY_CC && Gr->gv.symmetric && Gr->cc_err) {
+            uint32_t err = 0;
+            cudaMemcpy(&err, Gr->cc_err, 4, cudaMemcpyDeviceToHost);
+            if (err) return ipg_internal_fail(IPG_EDEVICE, "ipg_server_poll: union-find hook retries exhausted");
+        }
+        q.state = IPG_QUERY_DONE;
+        q.t_done = now;
+        S->completed.push_back(q.id);
+        S->finishing[i] = S->finishing.back();
+        S->finishing.pop_back();
     }
     // groups for pending queries that have none (HBM budget permitting)
     for (size_t i = 0; i < S->pending.size(); i++) {
@@ -901,8 +1334,7 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
         Graph* Gr = S->graphs[i / 2].get();
         const int kind = (int)(i % 2);
         if (!(kind ? Gr->pp : Gr->mp)) {
-            Group* G = nullptr;
-            int r = create_group(S, Gr, kind, &G);
+            int r = create_group(S, Gr, kind);
             if (r != IPG_OK && r != IPG_EBUDGET && r != IPG_ENOMEM) return r;
         }
     }
@@ -912,6 +1344,12 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
         if (G->running) {
             if (cudaEventQuery(G->ev) != cudaSuccess) continue;
             G->running = false;
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, G->ev0, G->ev) == cudaSuccess) {
+                const size_t slot = (size_t)G->G->gid * 2 + G->kind;
+                S->busy_s[slot] += ms * 1e-3;
+                S->steps[slot]++;
+            }
             retire(S, G, now);
         }
         admit(S, G, now);
@@ -988,6 +1426,20 @@ extern "C" int ipg_server_get_stats(ipg_server* S, ipg_server_stats* out)
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->stats;
     out->bytes_in_use = S->in_use;
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_group_stats(ipg_server* S, int gid, int group_kind, double* busy_s, uint64_t* supersteps,
+                                      uint64_t* lanes)
+{
+    if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_group_stats: null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (gid < 0 || gid >= (int)S->graphs.size() || group_kind < 0 || group_kind > 1)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_group_stats: no such group");
+    const size_t slot = (size_t)gid * 2 + group_kind;
+    if (busy_s) *busy_s = S->busy_s[slot];
+    if (supersteps) *supersteps = S->steps[slot];
+    if (lanes) *lanes = S->lanes[slot];
     return IPG_OK;
 }
 

@@ -41,6 +41,8 @@ def _lib():
         L.ipg_server_release.argtypes = [vp, u64]
         L.ipg_server_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
         L.ipg_server_run_trace.argtypes = [vp, u64, vp, vp, vp, vp, i32, vp, vp, ctypes.POINTER(dbl)]
+        L.ipg_server_group_stats.argtypes = [vp, i32, i32, ctypes.POINTER(dbl), ctypes.POINTER(u64),
+                                             ctypes.POINTER(u64)]
         L._serve_typed = True
     return L
 
@@ -135,6 +137,19 @@ class Server:
         s = _Stats()
         _check(_lib().ipg_server_get_stats(self._p, ctypes.byref(s)), where="ipg_server_get_stats")
         return {n: getattr(s, n) for n, _ in _Stats._fields_}
+
+    def group_stats(self) -> list:
+        """[(gid, "minplus"|"ppr", busy seconds, supersteps, lanes)] of the
+        groups that ran (busy times of concurrent groups overlap)."""
+        out = []
+        for gid in range(len(self.graphs)):
+            for gk, name in ((0, "minplus"), (1, "ppr")):
+                b, s, n = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+                _check(_lib().ipg_server_group_stats(self._p, gid, gk, ctypes.byref(b), ctypes.byref(s),
+                                                     ctypes.byref(n)), where="ipg_server_group_stats")
+                if s.value:
+                    out.append((gid, name, b.value, s.value, n.value))
+        return out
 
     def run_trace(self, trace: Trace, keep_results=False):
         """Replays the trace in real time; returns (qids, latencies s, makespan s)."""

@@ -152,6 +152,33 @@ def test_tight_hbm_budget_evicts_idle_groups():
             d.free()
 
 
+def test_cc_union_find_and_label_propagation():
+    """CC on a graph declared symmetric runs by union-find (the labels of
+    min-label propagation); on a directed graph by label-propagation lanes."""
+    from ipregel_b200 import serve as S
+    gs = _graphs()
+    dg = _device(gs)
+    directed = O.gen_rmat(10, 8, seed=5, undirected=False)
+    dd = _device([directed])[0]
+    srv = S.Server()
+    try:
+        for d in dg:
+            d.set_symmetric(True)
+            srv.add_graph(d)
+        gd = srv.add_graph(dd)
+        qs = [(gid, S.CC, 0) for gid in range(3) for _ in range(3)] + [(gid, S.SSSP, 5) for gid in range(3)]
+        ids = [srv.submit(*q) for q in qs]
+        qd = srv.submit(gd, S.CC, 0)
+        srv.drain()
+        for qid, (gid, kind, src) in zip(ids, qs):
+            _check(gs[gid], kind, src, srv.result(qid, kind, gs[gid].V))
+        np.testing.assert_array_equal(srv.result(qd, S.CC, directed.V), O.run(directed, "cc", "spread")[0])
+    finally:
+        srv.free()
+        for d in dg + [dd]:
+            d.free()
+
+
 def test_bad_requests_raise():
     import ipregel_b200 as ip
     from ipregel_b200 import serve as S
