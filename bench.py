@@ -7,11 +7,16 @@ duplicates removed, symmetrised, u32 ids, u32 weights uniform in [1, 255]),
   - min-label connected components with the spread version (app cc), and
   - single-source shortest paths from vertex 0 with atomicMin delivery
     (app sssp_weighted, spread version),
-each to quiescence.  Metric: Graph500-style GTEPS = stored edges x runs /
-time.  `value` times the runs with the graph resident in HBM; `e2e` times the
-same through the C ABI with host buffers (graph upload and result download
-inside the timed region).  Inputs are 3.8 GB, larger than the 126 MB L2, so no
+each to quiescence, each run one captured CUDA-graph launch.  Metric:
+Graph500-style GTEPS = stored edges x runs / time.  `value` times the runs
+with the graph resident in HBM; `e2e` times the same through the C ABI with
+host buffers (graph upload and result download inside the timed region).  Inputs are 3.8 GB, larger than the 126 MB L2, so no
 L2 flush is needed between steps.
+
+At N=1 the line also carries the other workloads (--no-extra skips them):
+PageRank's precision split (FP32 compensated vs FP64, directed R-MAT scale
+25, 30 rounds), the batched launch of 4,096 ER graphs against the per-graph
+loop, and the request server on 16 resident graphs against the plain loop.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -19,6 +24,7 @@ With --gpus N > 1 (torchrun), every rank runs the same workload on its own GPU
 (replicas: the path does not shard), and value is the sum over ranks.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -44,6 +50,8 @@ def parse_args():
     p.add_argument("--cpu-scale", type=int, default=22, help="scale of the bounded CPU sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extra", action="store_true",
+                   help="skip the PageRank precision-split, batched and serving workloads")
     return p.parse_args()
 
 
@@ -212,6 +220,165 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def pagerank_row(peak):
+    """PageRank precision split on directed R-MAT scale 25, 30 rounds: FP32
+    compensated pull (ipg_pr_run_f32) against the FP64 engine (pagerank,
+    single broadcast), per-vertex error of FP32 against FP64 on the GPU."""
+    import numpy as np
+    import torch
+    import ipregel_b200 as ip
+    scale, rounds = 25, 30
+    g = ip.Graph.generate_rmat(scale, 16, seed=1, undirected=False)
+    g.set_directed(False)  # the stored rows are the gather lists, as the reference loads them
+    V, E = g.V, g.E
+    pr = ip.PageRankF32(g)
+    x = ip.DeviceArray(V, np.float32)
+    d = ip.DeviceArray((rounds + 1) * 3, np.float64)
+    for _ in range(2):
+        pr.run_device(x, d, rounds, 0.85, True)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    t0.record()
+    for _ in range(reps):
+        pr.run_device(x, d, rounds, 0.85, True)
+    t1.record()
+    torch.cuda.synchronize()
+    ms32 = t0.elapsed_time(t1) / reps
+    diag = d.to_host().reshape(rounds + 1, 3)
+    eng = ip.Engine("pagerank", "single_broadcast")
+    eng.set_quiet(True)
+    eng.set_param("rounds", rounds)
+    eng.set_graph_loop(True)
+    eng.attach(g)
+    eng.run_only()
+    ms64 = []
+    for _ in range(2):
+        eng.run_only()
+        ms64.append(eng.stats()[0] * 1e3)
+    ptr = ctypes.c_void_p()
+    eng._check(eng.lib.ipg_app_values_device(ctypes.byref(ptr)), "ipg_app_values_device")
+    err = ip.error_f32_f64(x, ip.DeviceArray.wrap(ptr.value, V, np.float64))
+    eng.set_graph_loop(False)
+    eng.set_param("rounds", 10)
+    eng.release()
+    byts = 8 * E + 24 * V
+    achieved = byts / (ms32 / rounds * 1e-3) / 1e9
+    launches = launches_per_run_f32(pr.info(), rounds)
+    out = {"workload": f"PageRank, directed R-MAT scale {scale}, edge factor 16, seed 1, {rounds} rounds, d=0.85",
+           "vertices": V, "edges": E,
+           "fp32_compensated": {"ms": round(ms32, 3), "gteps": round(E * rounds / (ms32 * 1e-3) / 1e9, 2),
+                                "algorithmic_gbs": round(achieved, 1), "frac_hbm": round(achieved / peak, 4),
+                                "bytes_per_superstep": "8E + 24V (ids, quotient gathers; row, value, quotient)",
+                                "gpu_launches": launches},
+           "fp64_engine": {"ms": round(min(ms64), 3), "gteps": round(E * rounds / (min(ms64) * 1e-3) / 1e9, 2)},
+           "fp32_vs_fp64": {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in err.items()},
+           "fp64_diagnostics_last": {"mass": float(diag[-1, 0]), "dangling": float(diag[-1, 1]),
+                                     "residual_l1": float(diag[-1, 2])}}
+    x.free()
+    d.free()
+    pr.free()
+    g.free()
+    return out
+
+
+def launches_per_run_f32(info, rounds):
+    per = (1 if info["class_counts"][0] else 0) + (1 if info["class_counts"][1] else 0) + \
+          (2 if info["class_counts"][2] else 0) + 1
+    return 2 + rounds * per
+
+
+def batch_row():
+    """4,096 directed ER graphs (n log-uniform in [1024, 65536], out-degree 8,
+    weights U[1,64]): CC + SSSP(0) of every graph in one fused CUDA-graph
+    launch after autotuning, against the plain loop (attach and run per graph)."""
+    import numpy as np
+    from ipregel_b200 import batch as B
+    sizes = B.log_uniform_sizes(4096, 1024, 65536, seed=1)
+    parts = B.generate_er_parts(sizes, degree=8, seed=1, wmax=64)
+    bt = B.Batch(parts, directed=True)
+    r = B.BatchRunner(bt)
+    best = r.autotune()
+    for _ in range(2):
+        r.run()
+    ts = [r.run() for _ in range(5)]
+    res = r.results()
+    fused = min(ts)
+    launches = r.cc.launches() + r.sp.launches()
+    pcc, psp, wall, dev = B.run_plain(parts)
+    same = all(np.array_equal(pcc[i], res.cc[i]) and np.array_equal(psp[i], res.sssp[i]) for i in range(len(parts)))
+    E = bt.union.E
+    out = {"workload": "4096 directed ER graphs, n log-uniform [1024, 65536], m = 8n, weights U[1,64], seed 1; "
+                       "CC + SSSP(0) per graph",
+           "vertices": int(bt.union.V), "edges": int(E),
+           "fused_launch_ms": round(fused * 1e3, 2), "fused_gteps_2runs": round(2 * E / fused / 1e9, 3),
+           "plain_loop_wall_s": round(wall, 3), "plain_loop_device_s": round(dev, 3),
+           "speedup_vs_plain_wall": round(wall / fused, 1), "speedup_vs_plain_device": round(dev / fused, 1),
+           "results_equal_plain": bool(same),
+           "tuning": {k: v[0] for k, v in best.items()}, "supersteps": list(res.supersteps)}
+    r.release()
+    bt.free()
+    return out
+
+
+def serving_row():
+    """16 resident undirected R-MAT graphs, scales 18..25 (two each), weights
+    U[1,255]; 2,000 queries with Poisson arrivals at 2,000/s, 60% SSSP, 30%
+    PPR (FP32, 20 rounds), 10% CC; served throughput and latency, against the
+    plain loop run serially on a sample of the same trace."""
+    import numpy as np
+    import ipregel_b200 as ip
+    from ipregel_b200 import serve as S
+    scales = [s for s in range(18, 26) for _ in range(2)]
+    graphs = [ip.Graph.generate_rmat(s, 16, seed=100 + i, undirected=True, wmax=255) for i, s in enumerate(scales)]
+    sizes = [g.V for g in graphs]
+    srv = S.Server(hbm_budget=0, ppr_rounds=20)
+    for g in graphs:
+        srv.add_graph(g)
+    srv.run_trace(S.poisson_trace(64, 2000.0, sizes, seed=99))
+    tr = S.poisson_trace(2000, 2000.0, sizes, seed=1)
+    _, lat, mk = srv.run_trace(tr)
+    summ = S.summarize(lat, mk, tr.kind)
+    st = srv.stats()
+    srv.free()
+    m = 150
+    tot, per = 0.0, {0: [], 1: [], 2: []}
+    engines = {S.SSSP: ("sssp_weighted", "spread"), S.PPR: ("ppr", "single_broadcast"), S.CC: ("cc", "spread")}
+    for kind, (app, ver) in engines.items():
+        eng = ip.Engine(app, ver)
+        eng.set_quiet(True)
+        if app == "ppr":
+            eng.set_param("rounds", 20)
+        for gid in range(len(graphs)):
+            sel = [i for i in range(m) if tr.kind[i] == kind and tr.gid[i] == gid]
+            if not sel:
+                continue
+            eng.attach(graphs[gid])
+            for i in sel:
+                if kind != S.CC:
+                    eng.set_param("source", int(tr.source[i]))
+                eng.run_only()
+                sec = eng.stats()[0]
+                tot += sec
+                per[kind].append(sec)
+        eng.release()
+    plain_qps = m / tot
+    for g in graphs:
+        g.free()
+    return {"workload": "16 undirected R-MAT graphs, scales 18-25 (two each), edge factor 16, weights U[1,255]; "
+                        "2000 queries, Poisson 2000/s, 60% SSSP / 30% PPR FP32 20 rounds / 10% CC, seed 1",
+            "served_qps": round(summ["qps"], 1), "p50_ms": round(summ["p50_ms"], 1), "p99_ms": round(summ["p99_ms"], 1),
+            "per_kind_ms": {k: round(v, 1) for k, v in summ.items() if k.endswith("_ms") and "_" in k[:-3]},
+            "plain_serial_qps": round(plain_qps, 1),
+            "plain_sample": f"first {m} queries of the trace, run one at a time through the plain engine "
+                            f"(sssp_weighted/spread, ppr/single_broadcast FP64, cc/spread), graph attached "
+                            f"once per graph, device loop time only",
+            "speedup_vs_plain": round(summ["qps"] / plain_qps, 2),
+            "lanes_admitted": st["lanes_admitted"], "supersteps": st["supersteps"],
+            "kernel_launches": st["kernel_launches"], "peak_hbm_bytes": st["peak_bytes"],
+            "note": "arrivals exceed capacity: latency includes queueing"}
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_setup(args.gpus)
@@ -235,6 +402,7 @@ def main():
     sp = ip.Engine("sssp_weighted", "spread")
     for eng in (cc, sp):
         eng.set_quiet(True)
+        eng.set_graph_loop(True)  # each run: one captured CUDA-graph launch
     sp.set_param("source", 0)
     cc.attach(g)
     sp.attach(g)
@@ -254,9 +422,8 @@ def main():
     def max_over_ranks(x):
         return reduce_max(x, world, "cuda")
 
-    # ---- device-resident timed region (per-kernel events on) ----
+    # ---- device-resident timed region ----
     for eng in (cc, sp):
-        eng.set_profile(True)
         eng.profile_reset()
     clocks = ClockSampler(local)
     clocks.start()
@@ -275,16 +442,23 @@ def main():
     clk = clocks.stop()
     ms = max_over_ranks(t0.elapsed_time(t1))
     launches = cc.launches() + sp.launches()
+
+    runs = 2 * args.steps
+    value = replica_gteps(world, E, runs, ms)
+    traversed_gteps = world * edges_traversed / (ms * 1e-3) / 1e9
+
+    # ---- one profiled step (host-driven loop, events around every launch) ----
+    for eng in (cc, sp):
+        eng.set_graph_loop(False)
+        eng.set_profile(True)
+        eng.profile_reset()
+    step()
     prof = {}
     for tag, eng in (("cc", cc), ("sssp", sp)):
         for k, v in eng.profile().items():
             prof[f"{tag}:{k}"] = v
     for eng in (cc, sp):
         eng.set_profile(False)
-
-    runs = 2 * args.steps
-    value = replica_gteps(world, E, runs, ms)
-    traversed_gteps = world * edges_traversed / (ms * 1e-3) / 1e9
 
     # dominant kernel and its roofline
     peak, peak_kind = measured_peaks()
@@ -298,7 +472,8 @@ def main():
                 "frac": round(achieved / peak, 4), "traffic": None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "bytes_per_launch": round(bytes_per_launch), "avg_launch_ms": round(avg_ms, 4),
-                "share_of_kernel_time": round(top_rec["ms"] / total_kernel_ms, 3) if total_kernel_ms else None}
+                "share_of_kernel_time": round(top_rec["ms"] / total_kernel_ms, 3) if total_kernel_ms else None,
+                "timing": "CUDA events around each launch of one separate profiled step"}
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_path):
         try:
@@ -311,6 +486,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
+    cc_labels_components = reached = None
     if not args.no_e2e:
         idx, adj, wgt = g.to_host()
         p_idx = ip.PinnedArray(V, np.uint64)
@@ -345,13 +521,13 @@ def main():
         e2e = {"value": round(replica_gteps(world, E, runs, ms_e2e), 4), "unit": "GTEPS",
                "h2d_bytes_per_step": int(V * 8 + E * 4 + E * 4), "d2h_bytes_per_step": int(2 * V * 4),
                "ms_per_step": round(ms_e2e / args.steps, 3)}
-        # the results of the last end-to-end step are the results of the workload
         cc_labels_components = int(len(np.unique(out_cc.array)))
         reached = int(np.count_nonzero(out_sp.array != 0xFFFFFFFF))
         for a in (p_idx, p_adj, p_wgt, out_cc, out_sp):
             a.free()
-    else:
-        cc_labels_components = reached = None
+    cc.release()
+    sp.release()
+    g.free()
 
     # ---- CPU baseline: the reference's binaries on a bounded sample ----
     cpu = None
@@ -375,6 +551,16 @@ def main():
             cpu = {"value": None, "unit": "GTEPS", "cores": cores, "kind": "reference",
                    "sample": "reference binaries not built"}
 
+    # ---- the other workloads (one GPU only; each frees what it held) ----
+    extra = {}
+    if world == 1 and not args.no_extra:
+        for name, fn in (("pagerank_precision_split", lambda: pagerank_row(peak)), ("batched_many_graph", batch_row),
+                         ("serving", serving_row)):
+            try:
+                extra[name] = fn()
+            except Exception as exc:  # report, keep the headline
+                extra[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
@@ -383,6 +569,7 @@ def main():
             "config": {"workload": f"cc (spread) + weighted sssp from 0 (spread, atomicMin), undirected R-MAT "
                                    f"scale {scale}, edge factor 16, a/b/c=0.57/0.19/0.19, seed 1, weights U[1,255]",
                        "vertices": V, "edges_stored": E, "parallelism": f"replicas x{world}",
+                       "superstep_loop": "captured CUDA graph with a device-evaluated while condition",
                        "teps": "Graph500: stored edges x runs / time",
                        "l2": "inputs (3.8 GB) larger than L2; no flush",
                        "traversed_gteps": round(traversed_gteps, 4),
@@ -397,10 +584,8 @@ def main():
                             "gbs": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9, 1) if v["ms"] else None}
                         for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
         }
+        line.update(extra)
         print(json.dumps(line))
-    cc.release()
-    sp.release()
-    g.free()
     if world > 1:
         dist.destroy_process_group()
     return 0

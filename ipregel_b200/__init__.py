@@ -199,9 +199,20 @@ class DeviceArray:
         self.dtype = np.dtype(dtype)
         self.n = int(n)
         self.nbytes = max(self.n * self.dtype.itemsize, 16)
+        self._owned = True
         p = ctypes.c_void_p()
         _check(runtime().ipg_dev_alloc(ctypes.byref(p), self.nbytes), where="ipg_dev_alloc")
         self._p = p
+
+    @classmethod
+    def wrap(cls, ptr, n, dtype):
+        """A view of device memory owned elsewhere (free() leaves it alone)."""
+        a = cls.__new__(cls)
+        a.dtype, a.n = np.dtype(dtype), int(n)
+        a.nbytes = a.n * a.dtype.itemsize
+        a._owned = False
+        a._p = ctypes.c_void_p(ptr)
+        return a
 
     @property
     def ptr(self):
@@ -220,7 +231,7 @@ class DeviceArray:
             _check(runtime().ipg_memcpy(self._p, a.ctypes.data, self.n * self.dtype.itemsize), where="ipg_memcpy")
 
     def free(self):
-        if self._p is not None and self._p.value:
+        if self._p is not None and self._p.value and self._owned:
             runtime().ipg_dev_free(self._p, ctypes.c_uint64(self.nbytes))
         self._p = None
 
