@@ -232,90 +232,15 @@ __device__ __forceinline__ void ipx_cas128(ipx_slot128* addr, unsigned long long
 template <int KIND, int MSGBYTES>
 struct ipx_mailbox;
 
-/* Hardware min on a packed word: the high half is 0 for a message and the
- * empty mailbox is all ones, so a delivered UINT_MAX is still "received", and
- * the atomic's old value tells which sender was first. */
-template <>
-struct ipx_mailbox<IP_COMBINE_MIN, 4> {
-    typedef unsigned long long slot;
-    /* A delivered message always differs from the empty slot, so whether a
-     * vertex received mail can be read off its mailbox after delivery. */
-    static constexpr bool kFlagInSlot = true;
-    __device__ static slot empty() { return ~0ULL; }
-    /* The precheck reads through L2 (values only fall within a superstep, so
-     * a stale read can only let a redundant atomic through); the atomic's
-     * result is unused, so it issues as a fire-and-forget reduction. */
-    __device__ static unsigned long long enc(ipx_msg m)
-    {
-        unsigned int b = ipx_to_word(m);
-        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u; /* signed order as unsigned */
-        return (unsigned long long)b;
-    }
-    __device__ static bool precheck(slot* s, ipx_msg m) { return enc(m) < ipx_peek(s); }
-    __device__ static bool commit(slot* s, ipx_msg m)
-    {
-        atomicMin(s, enc(m));
-        return true;
-    }
-    /* merge() is used where one thread owns the mailbox (pull delivery). */
-    __device__ static bool merge(slot* s, ipx_msg m)
-    {
-        const unsigned long long e = enc(m);
-        if (e < *s) *s = e;
-        return true;
-    }
-    __device__ static bool deliver(slot* s, ipx_msg m) { return precheck(s, m) && commit(s, m); }
-    __device__ static ipx_msg take(slot* s)
-    {
-        unsigned long long w = *s;
-        *s = ~0ULL;
-        unsigned int b = (unsigned int)w;
-        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
-        return ipx_from_word<ipx_msg>(b);
-    }
-};
-
-template <>
-struct ipx_mailbox<IP_COMBINE_MAX, 4> {
-    typedef unsigned long long slot;
-    static constexpr bool kFlagInSlot = true;
-    __device__ static slot empty() { return 0ULL; }
-    __device__ static unsigned long long enc(ipx_msg m)
-    {
-        unsigned int b = ipx_to_word(m);
-        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
-        return (1ULL << 32) | b;
-    }
-    __device__ static bool precheck(slot* s, ipx_msg m) { return enc(m) > ipx_peek(s); }
-    __device__ static bool commit(slot* s, ipx_msg m)
-    {
-        atomicMax(s, enc(m));
-        return true;
-    }
-    __device__ static bool merge(slot* s, ipx_msg m)
-    {
-        const unsigned long long e = enc(m);
-        if (e > *s) *s = e;
-        return true;
-    }
-    __device__ static bool deliver(slot* s, ipx_msg m) { return precheck(s, m) && commit(s, m); }
-    __device__ static ipx_msg take(slot* s)
-    {
-        unsigned long long w = *s;
-        *s = 0ULL;
-        unsigned int b = (unsigned int)w;
-        if constexpr (std::is_signed<ipx_msg>::value) b ^= 0x80000000u;
-        return ipx_from_word<ipx_msg>(b);
-    }
-};
-
-template <>
-struct ipx_mailbox<IP_COMBINE_MIN, 8> {
+/* Hardware min / max on the message itself (4 or 8 bytes).  The slot holds
+ * no flag: whether a vertex received mail is its received bit, which the
+ * caller sets whenever deliver/commit return true.  A message equal to the
+ * empty value still passes the precheck and so still sets the bit.  Keeping
+ * the slot at the message's width halves the mailboxes of 4-byte messages
+ * (V x 4 bytes per parity), which then stay in L2 at larger scales. */
+struct ipx_mailbox_min {
     typedef ipx_msg slot;
-    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::max(); }
-    /* No room for a flag: a message equal to the empty value still sets the
-     * received bit (the caller sets it whenever this returns true). */
     __device__ static bool precheck(slot* s, ipx_msg m)
     {
         const ipx_msg c = ipx_peek(s);
@@ -344,10 +269,8 @@ struct ipx_mailbox<IP_COMBINE_MIN, 8> {
     }
 };
 
-template <>
-struct ipx_mailbox<IP_COMBINE_MAX, 8> {
+struct ipx_mailbox_max {
     typedef ipx_msg slot;
-    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return std::numeric_limits<ipx_msg>::lowest(); }
     __device__ static bool precheck(slot* s, ipx_msg m)
     {
@@ -377,10 +300,18 @@ struct ipx_mailbox<IP_COMBINE_MAX, 8> {
     }
 };
 
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 4> : ipx_mailbox_min {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MIN, 8> : ipx_mailbox_min {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 4> : ipx_mailbox_max {};
+template <>
+struct ipx_mailbox<IP_COMBINE_MAX, 8> : ipx_mailbox_max {};
+
 template <int MSGBYTES>
 struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
     typedef ipx_msg slot;
-    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return (ipx_msg)0; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool deliver(slot* s, ipx_msg m)
@@ -408,7 +339,6 @@ struct ipx_mailbox<IP_COMBINE_SUM, MSGBYTES> {
 template <int MSGBYTES>
 struct ipx_mailbox_generic32 {
     typedef unsigned long long slot;
-    static constexpr bool kFlagInSlot = false; /* CAS: the first deliverer knows */
     __device__ static slot empty() { return 0ULL; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
@@ -462,7 +392,6 @@ struct ipx_mailbox<IP_COMBINE_GENERIC, 4> : ipx_mailbox_generic32<4> {};
 template <>
 struct ipx_mailbox<IP_COMBINE_GENERIC, 8> {
     typedef ipx_slot128 slot;
-    static constexpr bool kFlagInSlot = false;
     __device__ static slot empty() { return slot{0ULL, 0ULL}; }
     __device__ static bool precheck(slot*, ipx_msg) { return true; }
     __device__ static bool commit(slot* s, ipx_msg m) { return deliver(s, m); }
@@ -592,14 +521,13 @@ enum {
     IPX_K_PULLD0,
     IPX_K_PULLD1,
     IPX_K_PULLD2,
-    IPX_K_RECV,
     IPX_K_CTRL,
     IPX_K_N
 };
 static const char* const ipx_kname[IPX_K_N] = {
     "compute", "compact_broadcasters", "push_thread", "push_warp", "push_block", "compact_targets",
     "gather_thread", "gather_warp", "gather_block", "mark_thread", "mark_warp", "mark_block", "count_active",
-    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block", "received_from_mailbox",
+    "pull_deliver_thread", "pull_deliver_warp", "pull_deliver_block",
     "superstep_control"};
 
 __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
@@ -670,14 +598,6 @@ __device__ __forceinline__ T ipx_shfl_idx(T x, int src)
 /* A visitor gets batches of U edges: edge index e[k], target w[k], the
  * source's message m[k] (outbox value) and ok[k] (lane holds an edge). */
 
-/* Blind push (IPX_PUSH_BLIND = 1, packed min/max mailboxes only): every
- * message is a fire-and-forget atomic with no precheck read, and the
- * received bitmap is rebuilt from the mailboxes after delivery. */
-#ifndef IPX_PUSH_BLIND
-#define IPX_PUSH_BLIND 0
-#endif
-constexpr bool ipx_blind = IPX_PUSH_BLIND && ipx_mb::kFlagInSlot;
-
 /* Push visitor: prechecks a batch of mailboxes first, then commits. */
 struct ipx_push_visit {
     static constexpr bool kNeedsMessage = true;
@@ -685,18 +605,6 @@ struct ipx_push_visit {
     template <int U>
     __device__ __forceinline__ void batch(const uint64_t* e, const ipx_vid* w, const ipx_msg* m, const bool* ok) const
     {
-        if constexpr (ipx_blind) {
-#pragma unroll
-            for (int k = 0; k < U; k++) {
-                if (!ok[k]) continue;
-#if IPX_EDGE_MSG
-                ipx_mb::commit(&ipx_c.mbox[p][(uint64_t)w[k]], IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_c.wgt[e[k]]));
-#else
-                ipx_mb::commit(&ipx_c.mbox[p][(uint64_t)w[k]], m[k]);
-#endif
-            }
-            return;
-        }
         ipx_msg mk[U];
         bool go[U];
 #pragma unroll
@@ -991,27 +899,6 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_push(const u
 {
     if (ipx_c.pull_ok && __ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pulls */
     ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{ipx_parity()});
-}
-
-template <class S>
-__device__ __forceinline__ bool ipx_filled(const S& s, const S& empty)
-{
-    return !(s == empty);
-}
-__device__ __forceinline__ bool ipx_filled(const ipx_slot128& s, const ipx_slot128&) { return s.flag != 0ULL; }
-
-/* Blind push: received bits of parity p from the mailboxes' flags (one warp
- * per bitmap word; bits set by direct sends are kept). */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_recv_from_mailbox()
-{
-    const int p = ipx_parity();
-    const uint64_t V = ipx_c.V;
-    const uint64_t Vp = (V + 31) & ~31ULL;
-    for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
-        const bool r = ipx_mb::kFlagInSlot && v < V && ipx_filled(ipx_c.mbox[p][v], ipx_mb::empty());
-        const uint32_t bits = __ballot_sync(IPX_FULL, r);
-        if ((threadIdx.x & 31) == 0 && bits) ipx_c.recv[p][v >> 5] |= bits;
-    }
 }
 
 /* Direction of the superstep's delivery: pull when the broadcasters' out-edges

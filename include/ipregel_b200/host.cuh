@@ -472,7 +472,6 @@ static int ipx_deliver_superstep(uint32_t ge)
                                                                                    ipx_h.pull_prefix));
         IPX_CU(cudaMemsetAsync(c.bcaster, 0, c.W * 4 + 4, st));
     }
-    if constexpr (ipx_blind) IPX_LAUNCH(IPX_K_RECV, ipx_k_recv_from_mailbox<<<ipx_grid(), IPX_THREADS, 0, st>>>());
     IPX_CU(cudaGetLastError());
 #else
     (void)ge;
