@@ -81,11 +81,15 @@ double now_s()
 // ---------------------------------------------------------------------------
 
 // Status of a min-plus group after a superstep, copied to the host in one
-// transfer: lanes that improved something, list sizes, hub chunks of list 2.
+// transfer: lane flags, list sizes, hub chunks of list 2, least deferred
+// distance of each lane.
 struct MpStatus {
-    unsigned long long any;
+    unsigned long long any;   // lanes that improved a distance
+    unsigned long long near;  // lanes that relaxed a vertex below their threshold
+    unsigned long long far;   // lanes that deferred a vertex
     uint32_t cnt[3];
     uint32_t chunks;
+    uint32_t far_min[64];     // least deferred distance per lane
 };
 
 inline uint32_t warp_grid(uint64_t tasks)
@@ -177,8 +181,14 @@ struct MpArgs {
     const uint64_t* __restrict__ front;
     uint64_t* __restrict__ next;
     uint32_t* __restrict__ fbm;        // bit per vertex: in the next frontier
-    unsigned long long* __restrict__ any;
+    const uint32_t* __restrict__ thr;  // per lane: distances below it relax now
+    MpStatus* __restrict__ st;
     uint64_t wmask;                    // lanes whose edges carry their weight (SSSP)
+};
+
+// Per-thread flags of a superstep, reduced per CTA into the status.
+struct MpAcc {
+    unsigned long long any = 0, near = 0, far = 0;
 };
 
 // Relaxes edge (v -> u, weight t) for the lanes ks[0..m) of v (distances
@@ -208,54 +218,95 @@ __device__ __forceinline__ unsigned long long mp_relax_edge(const MpArgs& a, uin
 }
 
 // Lanes `bits` of u join the next frontier.
-__device__ __forceinline__ void mp_mark(const MpArgs& a, uint32_t u, unsigned long long bits,
-                                        unsigned long long& any_acc)
+__device__ __forceinline__ void mp_mark(const MpArgs& a, uint32_t u, unsigned long long bits)
 {
     atomicOr((unsigned long long*)&a.next[u], bits);
     const uint32_t fb = 1u << (u & 31);
     if (!(a.fbm[u >> 5] & fb)) atomicOr(&a.fbm[u >> 5], fb);
-    any_acc |= bits;
 }
 
-// The first MP_SPARSE lanes of mask M and v's distances in them.
-__device__ __forceinline__ int mp_lanes(const MpArgs& a, uint64_t v, uint64_t M, int* ks, uint32_t* ds)
+// Edges e0 + lane, e0 + lane + stride, ... of v for its m <= L lanes; L is
+// the smallest of 1, 2, 4, 8 holding m, so no instruction is issued for
+// lanes v does not have.
+template <int L>
+__device__ __forceinline__ void mp_edges_sparse(const MpArgs& a, uint64_t e0, uint64_t e1, uint64_t lane,
+                                                uint64_t stride, int m, const int* ks, const uint32_t* ds,
+                                                MpAcc& acc)
 {
-    int m = 0;
-    while (M && m < MP_SPARSE) {
-        const int k = __ffsll((long long)M) - 1;
-        M &= M - 1;
-        ks[m] = k;
-        ds[m] = a.dist[v * MP_K + k];
-        m++;
+    for (uint64_t e = e0 + lane; e < e1; e += stride) {
+        const uint32_t u = a.adj[e];
+        const uint32_t t = a.wgt ? a.wgt[e] : 0u;
+        const unsigned long long bits = mp_relax_edge<L>(a, u, t, m, ks, ds);
+        if (bits) {
+            mp_mark(a, u, bits);
+            acc.any |= bits;
+        }
     }
-    return m;
 }
 
-// One warp relaxes the edges [e0, e1) of v for all of v's frontier lanes:
-// a thread per edge when few lanes are active, else a thread per lane.
-__device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e0, uint64_t e1,
-                                         unsigned long long& any_acc)
+__device__ __forceinline__ void mp_edges_sparse_any(const MpArgs& a, uint64_t e0, uint64_t e1, uint64_t lane,
+                                                    uint64_t stride, int m, const int* ks, const uint32_t* ds,
+                                                    MpAcc& acc)
+{
+    if (m == 1) mp_edges_sparse<1>(a, e0, e1, lane, stride, m, ks, ds, acc);
+    else if (m == 2) mp_edges_sparse<2>(a, e0, e1, lane, stride, m, ks, ds, acc);
+    else if (m <= 4) mp_edges_sparse<4>(a, e0, e1, lane, stride, m, ks, ds, acc);
+    else mp_edges_sparse<MP_SPARSE>(a, e0, e1, lane, stride, m, ks, ds, acc);
+}
+
+// Near-far ordering per lane.  A frontier lane whose distance at v is below
+// the lane's threshold relaxes v's edges now; one at or above it stays in the
+// frontier untouched (deferred), and the least deferred distance of each lane
+// is kept (s_fmin, per CTA).  A lane with no vertex below its threshold in a
+// superstep has its threshold raised (host side); one with neither is done.
+// Relaxing in rough distance order leaves fewer vertices to be relaxed again
+// after their distance drops; the fixpoint, and so every result, is the same.
+__device__ __forceinline__ void mp_defer(const MpArgs& a, uint32_t v, unsigned long long lanes, MpAcc& acc)
+{
+    mp_mark(a, v, lanes);
+    acc.far |= lanes;
+}
+
+// One warp relaxes the edges [e0, e1) of v for all of v's frontier lanes
+// below their thresholds: a thread per edge when few lanes remain, else a
+// thread per lane.  The warp classifies the lanes itself (a lane each).
+__device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e0, uint64_t e1, bool mark_deferred,
+                                         MpAcc& acc, uint32_t* s_fmin)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t M = a.front[v];
     if (!M) return;
-    if (__popcll(M) <= MP_SPARSE) {
+    const bool in0 = (M >> lane) & 1ULL, in1 = (M >> (lane + 32)) & 1ULL;
+    const uint32_t d0 = in0 ? a.dist[v * MP_K + lane] : SRV_INF;
+    const uint32_t d1 = in1 ? a.dist[v * MP_K + 32 + lane] : SRV_INF;
+    const bool act0 = in0 && d0 < __ldg(&a.thr[lane]);
+    const bool act1 = in1 && d1 < __ldg(&a.thr[lane + 32]);
+    const uint32_t Mlo = __ballot_sync(FULL, act0), Mhi = __ballot_sync(FULL, act1);
+    const uint32_t Dlo = __ballot_sync(FULL, in0 && !act0), Dhi = __ballot_sync(FULL, in1 && !act1);
+    if (Dlo | Dhi) {
+        if (in0 && !act0) atomicMin(&s_fmin[lane], d0);
+        if (in1 && !act1) atomicMin(&s_fmin[lane + 32], d1);
+        if (mark_deferred && lane == 0) mp_defer(a, (uint32_t)v, (unsigned long long)Dlo | ((unsigned long long)Dhi << 32), acc);
+    }
+    const unsigned long long R = (unsigned long long)Mlo | ((unsigned long long)Mhi << 32);
+    if (!R) return;
+    if (lane == 0) acc.near |= R;
+    if (__popcll(R) <= MP_SPARSE) {
         int ks[MP_SPARSE];
         uint32_t ds[MP_SPARSE];
-        const int m = mp_lanes(a, v, M, ks, ds);
-        for (uint64_t e = e0 + lane; e < e1; e += 32) {
-            const uint32_t u = a.adj[e];
-            const uint32_t t = a.wgt ? a.wgt[e] : 0u;
-            const unsigned long long bits = mp_relax_edge<MP_SPARSE>(a, u, t, m, ks, ds);
-            if (bits) mp_mark(a, u, bits, any_acc);
+        int m = 0;
+        unsigned long long rest = R;
+        while (rest && m < MP_SPARSE) {
+            const int k = __ffsll((long long)rest) - 1;
+            rest &= rest - 1;
+            ks[m] = k;
+            ds[m] = __shfl_sync(FULL, k < 32 ? d0 : d1, k & 31);
+            m++;
         }
+        mp_edges_sparse_any(a, e0, e1, lane, 32, m, ks, ds, acc);
         return;
     }
-    const uint32_t Mlo = (uint32_t)M, Mhi = (uint32_t)(M >> 32);
-    const bool act0 = (Mlo >> lane) & 1u, act1 = (Mhi >> lane) & 1u;
     const bool w0 = ((uint32_t)a.wmask >> lane) & 1u, w1 = ((uint32_t)(a.wmask >> 32) >> lane) & 1u;
-    const uint32_t d0 = act0 ? a.dist[v * MP_K + lane] : SRV_INF;
-    const uint32_t d1 = act1 ? a.dist[v * MP_K + 32 + lane] : SRV_INF;
     for (uint64_t e = e0; e < e1; e += 32) {
         const uint64_t ee = e + lane;
         const uint32_t wj = ee < e1 ? a.adj[ee] : 0u;
@@ -294,74 +345,116 @@ __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e
                 }
                 const uint32_t b0 = Mlo ? __ballot_sync(FULL, i0) : 0u;
                 const uint32_t b1 = Mhi ? __ballot_sync(FULL, i1) : 0u;
-                if ((b0 | b1) && lane == 0)
-                    mp_mark(a, u[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32), any_acc);
+                if ((b0 | b1) && lane == 0) {
+                    const unsigned long long bits = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+                    mp_mark(a, u[q], bits);
+                    acc.any |= bits;
+                }
             }
         }
     }
 }
 
-__device__ __forceinline__ void mp_block_any(unsigned long long x, unsigned long long* any)
+// The CTA's flags and least deferred distances into the status.
+__device__ __forceinline__ void mp_block_flush(MpAcc acc, const MpArgs& a, uint32_t* s_fmin)
 {
-    for (int o = 16; o > 0; o >>= 1) x |= __shfl_down_sync(FULL, x, o);
-    __shared__ unsigned long long s[SRV_THREADS / 32];
-    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t |= s[w];
-        if (t) atomicOr(any, t);
+    __shared__ unsigned long long s[3][SRV_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        acc.any |= __shfl_down_sync(FULL, acc.any, o);
+        acc.near |= __shfl_down_sync(FULL, acc.near, o);
+        acc.far |= __shfl_down_sync(FULL, acc.far, o);
     }
+    if ((threadIdx.x & 31) == 0) {
+        s[0][threadIdx.x >> 5] = acc.any;
+        s[1][threadIdx.x >> 5] = acc.near;
+        s[2][threadIdx.x >> 5] = acc.far;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t |= s[threadIdx.x][w];
+        unsigned long long* dst = threadIdx.x == 0 ? &a.st->any : (threadIdx.x == 1 ? &a.st->near : &a.st->far);
+        if (t) atomicOr(dst, t);
+    }
+    if (threadIdx.x < MP_K && s_fmin[threadIdx.x] != SRV_INF) atomicMin(&a.st->far_min[threadIdx.x], s_fmin[threadIdx.x]);
 }
 
-// A thread per low-degree frontier vertex (class 0): its edges one by one,
-// all its lanes at each, MP_SPARSE at a time.
+__device__ __forceinline__ void mp_fmin_init(uint32_t* s_fmin)
+{
+    if (threadIdx.x < MP_K) s_fmin[threadIdx.x] = SRV_INF;
+    __syncthreads();
+}
+
+// A thread per low-degree frontier vertex (class 0): its lanes one at a
+// time, each over the vertex's few edges.
 __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_thread(MpArgs a, const uint32_t* __restrict__ list,
                                                                      const uint32_t* __restrict__ count)
 {
+    __shared__ uint32_t s_fmin[MP_K];
+    mp_fmin_init(s_fmin);
     const uint32_t n = *count;
-    unsigned long long acc = 0;
+    MpAcc acc;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t v = list[i];
+        const uint32_t v = list[i];
         uint64_t M = a.front[v];
         const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
+        unsigned long long deferred = 0;
         while (M) {
-            int ks[MP_SPARSE];
-            uint32_t ds[MP_SPARSE];
-            const int m = mp_lanes(a, v, M, ks, ds);
-            for (int j = 0; j < m; j++) M &= ~(1ULL << ks[j]);
+            const int k = __ffsll((long long)M) - 1;
+            M &= M - 1;
+            const unsigned long long bit = 1ULL << k;
+            const uint32_t d = a.dist[(uint64_t)v * MP_K + k];
+            if (d >= __ldg(&a.thr[k])) {
+                deferred |= bit;
+                atomicMin(&s_fmin[k], d);
+                continue;
+            }
+            acc.near |= bit;
+            const bool weighted = (a.wmask >> k) & 1ULL;
             for (uint64_t e = e0; e < e1; e++) {
                 const uint32_t u = a.adj[e];
-                const uint32_t t = a.wgt ? a.wgt[e] : 0u;
-                const unsigned long long bits = mp_relax_edge<MP_SPARSE>(a, u, t, m, ks, ds);
-                if (bits) mp_mark(a, u, bits, acc);
+                const uint32_t nd = d + ((weighted && a.wgt) ? a.wgt[e] : 0u);
+                uint32_t* p = &a.dist[(uint64_t)u * MP_K + k];
+                if (nd < *p) {
+                    atomicMin(p, nd);
+                    mp_mark(a, u, bit);
+                    acc.any |= bit;
+                }
             }
         }
+        if (deferred) mp_defer(a, v, deferred, acc);
     }
-    mp_block_any(acc, a.any);
+    __syncthreads();
+    mp_block_flush(acc, a, s_fmin);
 }
 
 // A warp per frontier vertex (class 1).
 __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_vertices(MpArgs a, const uint32_t* __restrict__ list,
                                                                        const uint32_t* __restrict__ count)
 {
+    __shared__ uint32_t s_fmin[MP_K];
+    mp_fmin_init(s_fmin);
     const uint32_t n = *count;
-    unsigned long long acc = 0;
+    MpAcc acc;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
-        mp_relax(a, v, a.row[v], a.row[v + 1], acc);
+        mp_relax(a, v, a.row[v], a.row[v + 1], true, acc, s_fmin);
     }
-    mp_block_any(acc, a.any);
+    __syncthreads();
+    mp_block_flush(acc, a, s_fmin);
 }
 
-// A warp per HUB_CHUNK edges of a frontier hub (class 2).
+// A warp per HUB_CHUNK edges of a frontier hub (class 2); the chunk holding
+// the hub's first edge marks its deferred lanes.
 __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_hubs(MpArgs a, const uint32_t* __restrict__ list,
                                                                    const uint32_t* __restrict__ count,
                                                                    const uint32_t* __restrict__ prefix)
 {
+    __shared__ uint32_t s_fmin[MP_K];
+    mp_fmin_init(s_fmin);
     const uint32_t n = *count;
-    unsigned long long acc = 0;
+    MpAcc acc;
     if (n) {
         const uint32_t chunks = prefix[n];
         const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -370,10 +463,11 @@ __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_hubs(MpArgs a, cons
             const uint64_t v = list[i];
             const uint64_t e0 = a.row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
             const uint64_t end = a.row[v + 1];
-            mp_relax(a, v, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, acc);
+            mp_relax(a, v, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, (uint32_t)c == prefix[i], acc, s_fmin);
         }
     }
-    mp_block_any(acc, a.any);
+    __syncthreads();
+    mp_block_flush(acc, a, s_fmin);
 }
 
 // After a superstep: the consumed frontier masks back to zero.
@@ -388,8 +482,8 @@ __global__ void k_mp_clear(uint64_t* __restrict__ front, const uint32_t* __restr
     }
 }
 
-// Lane k of every vertex to INF (SSSP), or to the vertex id with every vertex
-// in lane k's frontier (CC by label propagation).
+// Lane k of every vertex to the vertex id, every vertex in lane k's frontier
+// (CC by label propagation); with cc = 0, lane k to INF.
 __global__ void k_mp_init_lane(uint32_t* __restrict__ dist, uint64_t* __restrict__ front, uint64_t V, int k, int cc)
 {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
@@ -428,10 +522,14 @@ __global__ void k_mp_mark_all(const uint64_t* __restrict__ front, uint64_t V, ui
     }
 }
 
-__global__ void k_mp_extract(const uint32_t* __restrict__ dist, uint64_t V, int k, uint32_t* __restrict__ out)
+// Lane k's values out, and the lane back to INF for its next query (so an
+// SSSP admission writes only its source).
+__global__ void k_mp_extract(uint32_t* __restrict__ dist, uint64_t V, int k, uint32_t* __restrict__ out)
 {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
         out[v] = dist[v * MP_K + k];
+        dist[v * MP_K + k] = SRV_INF;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -485,37 +583,85 @@ __global__ void k_cc_init(uint32_t* __restrict__ p, uint64_t V, uint32_t* __rest
     if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
 }
 
-// Each undirected edge once, from its larger end: a thread per vertex of
-// class 0, a warp per vertex of class 1, a warp per HUB_CHUNK edges of a hub.
+// The union-find pass runs in three steps (the sampling idea of Sutton et
+// al., "Optimizing Parallel Graph Connectivity Computation via Subgraph
+// Sampling", 2018): hook every vertex to its first CC_SAMPLE neighbours,
+// find the component most sampled vertices ended in (on R-MAT graphs the
+// giant one), then hook the remaining edges of the vertices outside it only.
+// An edge between two vertices of that component needs no hook, and an edge
+// with one end outside is hooked from that end, so the components (and their
+// least-id roots) are those of a full pass.
+constexpr uint32_t CC_SAMPLE = 2;
+constexpr uint32_t CC_PROBES = 1024;
+
+__global__ void k_cc_sample(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj, uint64_t V, uint32_t* p,
+                            uint32_t* err)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e1 = row[v + 1];
+        for (uint64_t e = row[v]; e < e1 && e < row[v] + CC_SAMPLE; e++) cc_hook(p, (uint32_t)v, adj[e], err);
+    }
+}
+
+// *giant = the root shared by most of CC_PROBES spread vertices (ties: the
+// smaller root).  One CTA of CC_PROBES threads; V > 0.
+__global__ void __launch_bounds__(CC_PROBES) k_cc_giant(uint32_t* p, uint64_t V, uint32_t* __restrict__ giant)
+{
+    __shared__ uint32_t r[CC_PROBES];
+    __shared__ unsigned long long best;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) best = 0;
+    r[t] = cc_find(p, (uint32_t)(((uint64_t)t * 2654435761ULL) % V));
+    __syncthreads();
+    uint32_t c = 0;
+    for (uint32_t j = 0; j < CC_PROBES; j++) c += r[j] == r[t];
+    atomicMax(&best, ((unsigned long long)c << 32) | (0xffffffffu - r[t]));
+    __syncthreads();
+    if (t == 0) *giant = 0xffffffffu - (uint32_t)best;
+}
+
+// The edges from index `skip` of each listed vertex: all of them when `giant`
+// is given (vertices in that component are skipped), else the edges to smaller
+// ids only (each undirected edge once).  A thread per vertex of class 0, a
+// warp per vertex of class 1, a warp per HUB_CHUNK edges of a hub.
+__device__ __forceinline__ bool cc_wanted(uint32_t v, uint32_t u, bool all) { return all || u < v; }
+
 __global__ void k_cc_hook_thread(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
-                                 const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err)
+                                 const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err,
+                                 const uint32_t* __restrict__ giant, uint32_t skip)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = list[i];
-        for (uint64_t e = row[v]; e < row[v + 1]; e++) {
+        if (giant && cc_find(p, v) == *giant) continue;
+        for (uint64_t e = row[v] + skip; e < row[v + 1]; e++) {
             const uint32_t u = adj[e];
-            if (u < v) cc_hook(p, v, u, err);
+            if (cc_wanted(v, u, giant != nullptr)) cc_hook(p, v, u, err);
         }
     }
 }
 
 __global__ void k_cc_hook_warp(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
-                               const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err)
+                               const uint32_t* __restrict__ list, uint64_t n, uint32_t* p, uint32_t* err,
+                               const uint32_t* __restrict__ giant, uint32_t skip)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint32_t v = list[i];
-        for (uint64_t e = row[v] + lane; e < row[v + 1]; e += 32) {
+        if (giant) {
+            const uint32_t root = __shfl_sync(FULL, lane == 0 ? cc_find(p, v) : 0u, 0);
+            if (root == *giant) continue;
+        }
+        for (uint64_t e = row[v] + skip + lane; e < row[v + 1]; e += 32) {
             const uint32_t u = adj[e];
-            if (u < v) cc_hook(p, v, u, err);
+            if (cc_wanted(v, u, giant != nullptr)) cc_hook(p, v, u, err);
         }
     }
 }
 
 __global__ void k_cc_hook_hub(const uint64_t* __restrict__ row, const uint32_t* __restrict__ adj,
                               const uint32_t* __restrict__ list, uint32_t n, const uint32_t* __restrict__ prefix,
-                              uint32_t* p, uint32_t* err)
+                              uint32_t* p, uint32_t* err, const uint32_t* __restrict__ giant, uint32_t skip)
 {
     if (!n) return;
     const int lane = threadIdx.x & 31;
@@ -524,11 +670,17 @@ __global__ void k_cc_hook_hub(const uint64_t* __restrict__ row, const uint32_t* 
     for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
         const uint32_t i = hub_of_chunk(prefix, n, (uint32_t)c);
         const uint32_t v = list[i];
-        const uint64_t e0 = row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
+        if (giant) {
+            const uint32_t root = __shfl_sync(FULL, lane == 0 ? cc_find(p, v) : 0u, 0);
+            if (root == *giant) continue;
+        }
+        const uint64_t first = row[v] + skip;
+        uint64_t e0 = row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
         const uint64_t e1 = e0 + HUB_CHUNK < row[v + 1] ? e0 + HUB_CHUNK : row[v + 1];
+        if (e0 < first) e0 = first;
         for (uint64_t e = e0 + lane; e < e1; e += 32) {
             const uint32_t u = adj[e];
-            if (u < v) cc_hook(p, v, u, err);
+            if (cc_wanted(v, u, giant != nullptr)) cc_hook(p, v, u, err);
         }
     }
 }
@@ -746,6 +898,7 @@ struct Graph {
     uint32_t* hub_prefix = nullptr;  // nh + 1 entries, then the hub count and the union-find error word
     uint64_t hub_chunks = 0;
     uint32_t* cc_err = nullptr;
+    uint32_t* cc_giant = nullptr;
     bool classes = false;
 };
 
@@ -769,7 +922,9 @@ struct Group {
     uint32_t* list[3] = {nullptr, nullptr, nullptr};
     uint32_t* cnt = nullptr;              // into stat_d
     uint32_t* prefix = nullptr;
-    unsigned long long* any_d = nullptr;  // into stat_d
+    uint32_t* thr_d = nullptr;            // lane thresholds of the next superstep
+    uint32_t* thr_pin = nullptr;          // their pinned staging copy
+    uint32_t thr_h[MP_K];
     MpStatus* stat_d = nullptr;
     MpStatus* stat_h = nullptr;           // pinned copy after each superstep
     uint32_t hn[3] = {0, 0, 0};           // list sizes the host knows of
@@ -815,6 +970,9 @@ struct ipg_server {
     std::vector<uint64_t> steps, lanes;         // supersteps, lanes admitted
     std::multimap<uint64_t, void*> pool;        // released result buffers by size
     uint64_t next_id = 1;
+    // near-far bucket width of SSSP lanes (IPG_SERVE_DELTA); on R-MAT graphs
+    // with weights in [1, 255], 256..1024 measured best, 7 % faster than none
+    uint32_t delta = 1024;
     std::mutex mu;
     ipg_server_stats stats{};
 };
@@ -826,6 +984,7 @@ void free_group(ipg_server* S, Group* G)
     if (G->st) cudaStreamSynchronize(G->st);
     for (auto& a : G->allocs) ipg_dev_free(a.first, a.second);
     if (G->stat_h) cudaFreeHost(G->stat_h);
+    if (G->thr_pin) cudaFreeHost(G->thr_pin);
     if (G->ev) cudaEventDestroy(G->ev);
     if (G->ev0) cudaEventDestroy(G->ev0);
     if (G->st) cudaStreamDestroy(G->st);
@@ -878,10 +1037,11 @@ int graph_classes(Graph* Gr, cudaStream_t st)
     if (r != IPG_OK) return r;
     const uint64_t nh = Gr->bins.count[2];
     void* p = nullptr;
-    if ((r = ipg_dev_alloc(&p, (nh + 4) * 4)) != IPG_OK) return r;
+    if ((r = ipg_dev_alloc(&p, (nh + 5) * 4)) != IPG_OK) return r;
     Gr->hub_prefix = (uint32_t*)p;
     uint32_t* count = Gr->hub_prefix + nh + 2;
     Gr->cc_err = count + 1;
+    Gr->cc_giant = count + 2;
     const uint32_t n2 = (uint32_t)nh;
     uint32_t chunks = 0;
     cudaMemcpyAsync(count, &n2, 4, cudaMemcpyHostToDevice, st);
@@ -900,15 +1060,21 @@ void run_union_find(Graph* Gr, uint32_t* p, cudaStream_t st)
     const ipg_bins& B = Gr->bins;
     const uint32_t* adj = (const uint32_t*)gv.d_adj;
     k_cc_init<<<resident_cap(k_cc_init, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(p, gv.V, Gr->cc_err);
+    if (gv.V == 0) return;
+    k_cc_sample<<<resident_cap(k_cc_sample, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(gv.d_row, adj, gv.V, p,
+                                                                                     Gr->cc_err);
+    k_cc_compress<<<resident_cap(k_cc_compress, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(p, gv.V);
+    k_cc_giant<<<1, CC_PROBES, 0, st>>>(p, gv.V, Gr->cc_giant);
     if (B.count[0])
         k_cc_hook_thread<<<resident_cap(k_cc_hook_thread, thread_grid(B.count[0])), SRV_THREADS, 0, st>>>(
-            gv.d_row, adj, B.d_list[0], B.count[0], p, Gr->cc_err);
+            gv.d_row, adj, B.d_list[0], B.count[0], p, Gr->cc_err, Gr->cc_giant, CC_SAMPLE);
     if (B.count[1])
         k_cc_hook_warp<<<resident_cap(k_cc_hook_warp, warp_grid(B.count[1])), SRV_THREADS, 0, st>>>(
-            gv.d_row, adj, B.d_list[1], B.count[1], p, Gr->cc_err);
+            gv.d_row, adj, B.d_list[1], B.count[1], p, Gr->cc_err, Gr->cc_giant, CC_SAMPLE);
     if (B.count[2])
         k_cc_hook_hub<<<resident_cap(k_cc_hook_hub, warp_grid(Gr->hub_chunks)), SRV_THREADS, 0, st>>>(
-            gv.d_row, adj, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix, p, Gr->cc_err);
+            gv.d_row, adj, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix, p, Gr->cc_err, Gr->cc_giant,
+            CC_SAMPLE);
     k_cc_compress<<<resident_cap(k_cc_compress, thread_grid(gv.V)), SRV_THREADS, 0, st>>>(p, gv.V);
 }
 
@@ -940,14 +1106,15 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
         if (r == IPG_OK) r = galloc(G, &G->fbm, (V + 31) / 32 + 1);
         for (int k = 0; k < 3 && r == IPG_OK; k++) r = galloc(G, &G->list[k], V);
         if (r == IPG_OK) r = galloc(G, &G->stat_d, 1);
-        if (r == IPG_OK) {
-            G->cnt = G->stat_d->cnt;
-            G->any_d = &G->stat_d->any;
-        }
+        if (r == IPG_OK) G->cnt = G->stat_d->cnt;
+        if (r == IPG_OK) r = galloc(G, &G->thr_d, MP_K);
+        if (r == IPG_OK && cudaHostAlloc((void**)&G->thr_pin, MP_K * 4, cudaHostAllocDefault) != cudaSuccess)
+            r = ipg_internal_fail(IPG_ENOMEM, "serve: pinned allocation failed");
         if (r == IPG_OK) r = galloc(G, &G->prefix, E / (MP_T1 + 1) + 2);
         if (r == IPG_OK && cudaHostAlloc((void**)&G->stat_h, sizeof(MpStatus), cudaHostAllocDefault) != cudaSuccess)
             r = ipg_internal_fail(IPG_ENOMEM, "serve: pinned allocation failed");
         if (r == IPG_OK) {
+            cudaMemsetAsync(G->dist, 0xff, V * MP_K * 4, G->st);  // every lane INF
             cudaMemsetAsync(G->front[0], 0, V * 8, G->st);
             cudaMemsetAsync(G->front[1], 0, V * 8, G->st);
             cudaMemsetAsync(G->fbm, 0, ((V + 31) / 32 + 1) * 4, G->st);
@@ -1041,7 +1208,7 @@ void admit(ipg_server* S, Group* G, double now)
                 }
                 run_union_find(G->G, (uint32_t*)q.result, G->st);
                 cc_first = q.result;
-                S->stats.kernel_launches += 5;
+                S->stats.kernel_launches += 8;
             } else {
                 cudaMemcpyAsync(q.result, cc_first, rbytes, cudaMemcpyDeviceToDevice, G->st);
             }
@@ -1064,13 +1231,15 @@ void admit(ipg_server* S, Group* G, double now)
             } else if (q.kind == IPG_QUERY_CC) {
                 k_mp_init_lane<<<g, SRV_THREADS, 0, G->st>>>(G->dist, G->front[G->cur], V, k, 1);
                 G->wmask &= ~(1ULL << k);
+                G->thr_h[k] = SRV_INF;  // labels are no distances: never deferred
                 G->cc_lane = k;
                 rebuild = true;
             } else {
-                k_mp_init_lane<<<g, SRV_THREADS, 0, G->st>>>(G->dist, G->front[G->cur], V, k, 0);
+                // the lane is INF everywhere (cleared when its last query was extracted)
                 k_mp_admit_source<<<1, 1, 0, G->st>>>(G->dist, G->front[G->cur], G->G->gv.d_row, q.src, k,
                                                        G->list[0], G->list[1], G->list[2], G->cnt);
                 G->wmask |= 1ULL << k;
+                G->thr_h[k] = S->delta;
                 G->appended++;
             }
             S->stats.lanes_admitted++;
@@ -1110,7 +1279,8 @@ int launch_superstep(ipg_server* S, Group* G)
         a.front = G->front[G->cur];
         a.next = G->front[G->cur ^ 1];
         a.fbm = G->fbm;
-        a.any = G->any_d;
+        a.thr = G->thr_d;
+        a.st = G->stat_d;
         a.wmask = G->wmask;
         // grids from the list sizes of the last status plus the sources
         // appended since (each in some list; a hub one adds its chunks)
@@ -1118,7 +1288,10 @@ int launch_superstep(ipg_server* S, Group* G)
         const uint64_t hub_chunks_max = (gv.max_out_degree + HUB_CHUNK - 1) / HUB_CHUNK;
         const uint64_t n0 = G->hn[0] + add, n1 = G->hn[1] + add;
         const uint64_t chunks = G->hchunks + add * hub_chunks_max;
-        cudaMemsetAsync(G->any_d, 0, 8, G->st);
+        memcpy(G->thr_pin, G->thr_h, sizeof G->thr_h);  // the last copy finished with the last superstep
+        cudaMemcpyAsync(G->thr_d, G->thr_pin, sizeof G->thr_h, cudaMemcpyHostToDevice, G->st);
+        cudaMemsetAsync(G->stat_d, 0, 3 * sizeof(unsigned long long), G->st);
+        cudaMemsetAsync(G->stat_d->far_min, 0xff, sizeof G->stat_d->far_min, G->st);
         if (add) k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, nullptr);
         k_mp_thread<<<resident_cap(k_mp_thread, thread_grid(n0)), SRV_THREADS, 0, G->st>>>(a, G->list[0], G->cnt + 0);
         k_mp_vertices<<<resident_cap(k_mp_vertices, warp_grid(n1)), SRV_THREADS, 0, G->st>>>(a, G->list[1],
@@ -1191,17 +1364,32 @@ int launch_superstep(ipg_server* S, Group* G)
 void retire(ipg_server* S, Group* G, double now)
 {
     if (G->kind == 0) {
-        const uint64_t live = G->stat_h->any;
-        for (int c = 0; c < 3; c++) G->hn[c] = G->stat_h->cnt[c];
-        G->hchunks = G->stat_h->chunks;
+        const MpStatus& st = *G->stat_h;
+        for (int c = 0; c < 3; c++) G->hn[c] = st.cnt[c];
+        G->hchunks = st.chunks;
         G->appended = 0;
+        const uint64_t live = st.any | st.far;
         const uint64_t done = G->busy & ~live;
+        // lanes with deferred vertices only: the threshold moves past the
+        // least of them
+        const uint64_t raise = G->busy & st.far & ~st.near;
+        for (int k = 0; k < MP_K; k++)
+            if ((raise >> k) & 1) {
+                const uint64_t base = st.far_min[k] != SRV_INF ? st.far_min[k] : G->thr_h[k];
+                G->thr_h[k] = (uint32_t)std::min<uint64_t>(base + S->delta, SRV_INF);
+            }
         for (int k = 0; k < MP_K; k++) {
             if (!((done >> k) & 1)) continue;
+            const void* first = nullptr;
             for (uint64_t qid : G->lane_q[k]) {
                 Query& q = S->queries[qid];
-                k_mp_extract<<<resident_cap(k_mp_extract, thread_grid(G->G->gv.V)), SRV_THREADS, 0, G->st>>>(
-                    G->dist, G->G->gv.V, k, (uint32_t*)q.result);
+                if (!first) {
+                    k_mp_extract<<<resident_cap(k_mp_extract, thread_grid(G->G->gv.V)), SRV_THREADS, 0, G->st>>>(
+                        G->dist, G->G->gv.V, k, (uint32_t*)q.result);
+                    first = q.result;
+                } else {
+                    cudaMemcpyAsync(q.result, first, q.result_bytes, cudaMemcpyDeviceToDevice, G->st);
+                }
                 finishing(S, q, G->st);
             }
             G->lane_q[k].clear();
@@ -1233,6 +1421,8 @@ extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_s
     if (!S) return ipg_internal_fail(IPG_ENOMEM, "ipg_server_create: out of host memory");
     S->budget = hbm_budget;
     S->rounds = ppr_rounds;
+    if (const char* d = getenv("IPG_SERVE_DELTA"))
+        if (*d) S->delta = (uint32_t)std::max(1UL, strtoul(d, nullptr, 10));
     *out = S;
     return IPG_OK;
 }
@@ -1250,7 +1440,7 @@ extern "C" void ipg_server_free(ipg_server* S)
     }
     for (auto& kv : S->pool) ipg_dev_free(kv.second, kv.first);
     for (auto& g : S->graphs)
-        if (g->hub_prefix) ipg_dev_free(g->hub_prefix, (g->bins.count[2] + 4) * 4);
+        if (g->hub_prefix) ipg_dev_free(g->hub_prefix, (g->bins.count[2] + 5) * 4);
     delete S;
 }
 

@@ -179,6 +179,30 @@ def test_cc_union_find_and_label_propagation():
             d.free()
 
 
+def test_cc_union_find_with_hubs():
+    """Union-find on a graph with hub rows split into chunks and a giant
+    component whose remaining edges are skipped: the labels of label
+    propagation, on two CC queries admitted together."""
+    import ipregel_b200 as ip
+    from ipregel_b200 import serve as S
+    g = O.gen_rmat(16, 16, seed=4, undirected=True)
+    d = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+    d.set_symmetric(True)
+    want = O.run(g, "cc", "spread")[0]
+    srv = S.Server()
+    try:
+        gid = srv.add_graph(d)
+        for _ in range(2):
+            qs = [srv.submit(gid, S.CC, 0) for _ in range(2)]
+            srv.drain()
+            for q in qs:
+                np.testing.assert_array_equal(srv.result(q, S.CC, g.V), want)
+                srv.release(q)
+    finally:
+        srv.free()
+        d.free()
+
+
 def test_bad_requests_raise():
     import ipregel_b200 as ip
     from ipregel_b200 import serve as S
