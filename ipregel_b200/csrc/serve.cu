@@ -708,19 +708,26 @@ struct PpArgs {
     float2* __restrict__ partial;  // (sum, compensation) per hub chunk and lane
 };
 
-// Compensated addition (TwoSum carries the rounding error of s + x in c).
+// Compensated summation; the value of a pair is s + c.  Per term, Kahan's
+// algorithm (4 operations: the gathers issue one per lane and edge, and the
+// ncu profile of the PPR kernels shows them issue-bound, not memory-bound);
+// pairs of partial sums merge with Knuth's TwoSum, which is exact whatever
+// their magnitudes.
 __device__ __forceinline__ void pp_add(float& s, float& c, float x)
 {
-    const float t = __fadd_rn(s, x);
-    const float bp = __fsub_rn(t, s);
-    c = __fadd_rn(c, __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(x, bp)));
+    const float y = __fadd_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(y, __fsub_rn(t, s));
     s = t;
 }
 
 __device__ __forceinline__ void pp_merge(float& s, float& c, float s2, float c2)
 {
-    pp_add(s, c, s2);
-    c = __fadd_rn(c, c2);
+    const float t = __fadd_rn(s, s2);
+    const float bp = __fsub_rn(t, s);
+    const float err = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(s2, bp));
+    c = __fadd_rn(__fadd_rn(c, c2), err);
+    s = t;
 }
 
 // x of lane k at v from its gathered sum (ppr application: 0.15 at the seed).
@@ -729,25 +736,59 @@ __device__ __forceinline__ float pp_value(const PpLanes& L, int k, uint64_t v, f
     return __fadd_rn(L.seed[k] == (uint32_t)v ? 0.15f : 0.0f, __fmul_rn(0.85f, sum));
 }
 
-// Half-warp h sums lane k of b_cur over the edges e0 + 2i + h of [e0, e1).
-__device__ __forceinline__ void pp_gather(const PpArgs& a, uint64_t e0, uint64_t e1, bool on, float& s, float& c)
+// A warp gathers [e0, e1): thread t takes edge slot t / 4 of every group of
+// 8 edges and lane quad t % 4, reading the neighbour's quad as one float4 and
+// summing its 4 lanes; then the 8 slots of each quad merge.  Threads 0..3 end
+// with the totals of lanes 4t..4t+3.  The order of a lane's terms depends on
+// the edge list only, not on which other lanes are active.
+__device__ __forceinline__ void pp_gather4(const PpArgs& a, uint64_t e0, uint64_t e1, bool quad_on, float* s, float* c)
 {
-    const int lane = threadIdx.x & 31, k = lane & 15, h = lane >> 4;
+    const int lane = threadIdx.x & 31, slot = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[i] = c[i] = 0.0f;
     for (uint64_t e = e0; e < e1; e += 32) {
         const uint32_t uj = (e + lane < e1) ? a.adj[e + lane] : 0u;
         const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
-        for (int j0 = 0; j0 < nj; j0 += 8) {
-            uint32_t u[4];
-            float q[4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) u[r] = __shfl_sync(FULL, uj, (j0 + 2 * r + h) & 31);
-#pragma unroll
-            for (int r = 0; r < 4; r++) q[r] = (on && j0 + 2 * r + h < nj) ? a.b_cur[(uint64_t)u[r] * PP_K + k] : 0.0f;
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-                if (on && j0 + 2 * r + h < nj) pp_add(s, c, q[r]);
+        for (int r = 0; r < 4; r++) {
+            const int jj = r * 8 + slot;
+            const uint32_t u = __shfl_sync(FULL, uj, jj);
+            if (quad_on && jj < nj) {
+                const float4 x = reinterpret_cast<const float4*>(a.b_cur + (uint64_t)u * PP_K)[q];
+                pp_add(s[0], c[0], x.x);
+                pp_add(s[1], c[1], x.y);
+                pp_add(s[2], c[2], x.z);
+                pp_add(s[3], c[3], x.w);
+            }
         }
     }
+#pragma unroll
+    for (int off = 4; off < 32; off <<= 1)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float s2 = __shfl_xor_sync(FULL, s[i], off), c2 = __shfl_xor_sync(FULL, c[i], off);
+            pp_merge(s[i], c[i], s2, c2);
+        }
+}
+
+// Threads 0..3 finish lanes 4t..4t+3 of vertex v.
+__device__ __forceinline__ void pp_finish4(const PpArgs& a, const PpLanes& L, uint64_t v, uint64_t deg, const float* s,
+                                           const float* c)
+{
+    const int q = threadIdx.x & 31;
+    if (q >= 4) return;
+    float bn[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int k = 4 * q + i;
+        bn[i] = 0.0f;
+        if ((L.active >> k) & 1u) {
+            const float xn = pp_value(L, k, v, __fadd_rn(s[i], c[i]));
+            if (L.out[k]) L.out[k][v] = xn;
+            else if (deg) bn[i] = __fdiv_rn(xn, (float)deg);
+        }
+    }
+    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
 }
 
 // Threads 0..15 finish vertex v for their lane from (s, c).
@@ -805,21 +846,18 @@ __global__ void __launch_bounds__(SRV_THREADS, 4) k_pp_thread(PpArgs a, PpLanes 
     }
 }
 
-// A warp per vertex (class 1): half-warps over alternate edges, a lane each.
+// A warp per vertex (class 1).
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                              uint64_t n)
 {
-    const int lane = threadIdx.x & 31;
-    const bool on = (L.active >> (lane & 15)) & 1u;
+    const bool quad_on = (L.active >> (4 * (threadIdx.x & 3))) & 0xFu;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
         const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
-        float s = 0.0f, c = 0.0f;
-        pp_gather(a, e0, e1, on, s, c);
-        const float s2 = __shfl_down_sync(FULL, s, 16), c2 = __shfl_down_sync(FULL, c, 16);
-        pp_merge(s, c, s2, c2);
-        pp_finish(a, L, v, e1 - e0, s, c);
+        float s[4], c[4];
+        pp_gather4(a, e0, e1, quad_on, s, c);
+        pp_finish4(a, L, v, e1 - e0, s, c);
     }
 }
 
@@ -829,7 +867,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes
 {
     if (!n) return;
     const int lane = threadIdx.x & 31;
-    const bool on = (L.active >> (lane & 15)) & 1u;
+    const bool quad_on = (L.active >> (4 * (lane & 3))) & 0xFu;
     const uint32_t chunks = prefix[n];
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
@@ -837,11 +875,11 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes
         const uint64_t v = list[i];
         const uint64_t e0 = a.row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
         const uint64_t end = a.row[v + 1];
-        float s = 0.0f, cc = 0.0f;
-        pp_gather(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, on, s, cc);
-        const float s2 = __shfl_down_sync(FULL, s, 16), c2 = __shfl_down_sync(FULL, cc, 16);
-        pp_merge(s, cc, s2, c2);
-        if (lane < PP_K) a.partial[c * PP_K + lane] = make_float2(s, cc);
+        float s[4], cc[4];
+        pp_gather4(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, quad_on, s, cc);
+        if (lane < 4)
+#pragma unroll
+            for (int j = 0; j < 4; j++) a.partial[c * PP_K + 4 * lane + j] = make_float2(s[j], cc[j]);
     }
 }
 
