@@ -111,19 +111,62 @@ def measured_peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
+NVML_REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+                ("sw_power_cap", 0x4))
+
+
+def nvml_reasons(mask):
+    return [n for n, bit in NVML_REASONS if mask & bit]
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clock and clock-event reasons during the timed region: NVML read
+    queries every 10 ms on a thread (the timed regions are a fraction of a
+    second), else nvidia-smi every 200 ms.  Reads only; no setting changes."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.01
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+        self.mask = 0
+        self.max_mhz = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.gpu)
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        self.mask |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(self.PERIOD_S)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -134,6 +177,12 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                    "sm_max_mhz": self.max_mhz, "reasons": nvml_reasons(self.mask),
+                    "samples": len(self.samples), "source": "NVML, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -142,6 +191,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         out = parse_clock_csv(self.path)
+        out["source"] = "nvidia-smi, 200 ms"
         os.unlink(self.path)
         return out
 
@@ -265,12 +315,21 @@ def pagerank_row(peak):
     byts = 8 * E + 24 * V
     achieved = byts / (ms32 / rounds * 1e-3) / 1e9
     launches = launches_per_run_f32(pr.info(), rounds)
+    # the gathers' access pattern alone: one scattered 4-byte quotient per edge
+    ceil = ip.measure_gather(4 * V, 4, 1 << 28, 5)
+    edge_rate = E * rounds / (ms32 * 1e-3)
     out = {"workload": f"PageRank, directed R-MAT scale {scale}, edge factor 16, seed 1, {rounds} rounds, d=0.85",
            "vertices": V, "edges": E,
            "fp32_compensated": {"ms": round(ms32, 3), "gteps": round(E * rounds / (ms32 * 1e-3) / 1e9, 2),
                                 "algorithmic_gbs": round(achieved, 1), "frac_hbm": round(achieved / peak, 4),
                                 "bytes_per_superstep": "8E + 24V (ids, quotient gathers; row, value, quotient)",
-                                "gpu_launches": launches},
+                                "gpu_launches": launches,
+                                "gather_ceiling": {
+                                    "pattern": f"u32 index stream + one scattered 4-byte read per index, table "
+                                               f"{4 * V >> 20} MiB (the quotients), ipg_measure_gather",
+                                    "rows_per_s": round(ceil["rows_per_s"] / 1e9, 2),
+                                    "edges_per_s": round(edge_rate / 1e9, 2), "unit": "G/s",
+                                    "frac": round(edge_rate / ceil["rows_per_s"], 4) if ceil["rows_per_s"] else None}},
            "fp64_engine": {"ms": round(min(ms64), 3), "gteps": round(E * rounds / (min(ms64) * 1e-3) / 1e9, 2)},
            "fp32_vs_fp64": {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in err.items()},
            "fp64_diagnostics_last": {"mass": float(diag[-1, 0]), "dangling": float(diag[-1, 1]),
@@ -474,6 +533,17 @@ def main():
                 "bytes_per_launch": round(bytes_per_launch), "avg_launch_ms": round(avg_ms, 4),
                 "share_of_kernel_time": round(top_rec["ms"] / total_kernel_ms, 3) if total_kernel_ms else None,
                 "timing": "CUDA events around each launch of one separate profiled step"}
+    edges_per_launch = top_rec.get("edges", 0.0) / max(top_rec["timed"], 1)
+    if edges_per_launch > 0 and avg_ms > 0:
+        # the same access pattern alone: a coalesced index stream and one
+        # scattered 4-byte read per index in a table of the mailbox's size
+        ceil = ip.measure_gather(V * 4, 4, 1 << 28, 5)
+        rate = edges_per_launch / (avg_ms * 1e-3)
+        roofline["gather_ceiling"] = {
+            "pattern": f"u32 index stream + one scattered 4-byte read per index, table {V * 4 >> 20} MiB "
+                       "(the 4-byte mailbox), ipg_measure_gather",
+            "rows_per_s": round(ceil["rows_per_s"] / 1e9, 2), "kernel_edges_per_s": round(rate / 1e9, 2),
+            "unit": "G/s", "frac": round(rate / ceil["rows_per_s"], 4) if ceil["rows_per_s"] else None}
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_path):
         try:

@@ -98,6 +98,7 @@ struct ipx_host_state {
     uint64_t prof_timed[IPX_K_N] = {0};
     double prof_ms[IPX_K_N] = {0};
     double prof_bytes[IPX_K_N] = {0};
+    double prof_edges[IPX_K_N] = {0};  /* edges walked (push, mark, gather kernels) */
 #define IPX_PEV 32
     cudaEvent_t pev[2][IPX_PEV];
     int pkid[IPX_PEV];
@@ -490,9 +491,11 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
     [[maybe_unused]] const unsigned long long* ctr = ipx_h.h_ctr;
     [[maybe_unused]] const uint32_t* l = ipx_h.h_lcnt;
     double* B = ipx_h.prof_bytes;
+    double* N = ipx_h.prof_edges;
     (void)s;
     (void)sb;
     (void)wb;
+    (void)N;
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SPREAD
     const double nb = (double)l[0] + l[1] + l[2];
     B[IPX_K_COMPUTE] += (IPX_VERSION == IPX_COMBINER ? V * 3.0 / 8.0 : frontier * 4.0) +
@@ -506,8 +509,10 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
         for (int k = 0; k < 3; k++)
             B[IPX_K_PULLD0 + k] +=
                 b.count[k] * (4.0 + 16.0 + sb) + b.edges[k] * (ib + 0.125) + bedges * (mb + wb) * (b.edges[k] / E);
+        for (int k = 0; k < 3; k++) N[IPX_K_PULLD0 + k] += b.edges[k];
     } else {
         for (int k = 0; k < 3; k++) B[IPX_K_PUSH0 + k] += l[k] * (20.0 + mb) + ctr[8 + k] * (ib + sb + wb);
+        for (int k = 0; k < 3; k++) N[IPX_K_PUSH0 + k] += ctr[8 + k];
     }
 #if IPX_VERSION == IPX_COMBINER
     B[IPX_K_COUNT] += V / 4.0;
@@ -519,14 +524,17 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
     B[IPX_K_COMPUTE] += V * 1.0 / 8.0 + frontier * (2 * vb + mb + 2);
     for (int k = 0; k < 3; k++)
         B[IPX_K_GATHER0 + k] += b.count[k] * (4.0 + 8.0 + 2.0 + mb) + b.edges[k] * (ib + mb + 0.125);
+    for (int k = 0; k < 3; k++) N[IPX_K_GATHER0 + k] += b.edges[k];
 #else
     const double nb = (double)l[0] + l[1] + l[2];
     B[IPX_K_COMPUTE] += frontier * (4.0 + 2 * vb + 1 + mb) + nb * mb;
     B[IPX_K_COMPACT_B] += V / 8.0 + nb * 20.0;
     for (int k = 0; k < 3; k++) B[IPX_K_MARK0 + k] += l[k] * 20.0 + ctr[8 + k] * (ib + 0.125);
+    for (int k = 0; k < 3; k++) N[IPX_K_MARK0 + k] += ctr[8 + k];
     B[IPX_K_COMPACT_T] += V / 8.0 + ((double)l[4] + l[5] + l[6]) * 20.0;
     for (int k = 0; k < 3; k++)
         B[IPX_K_GATHER0 + k] += l[4 + k] * (4.0 + 16.0 + 1.0 + mb) + ctr[11 + k] * (ib + mb + 0.125);
+    for (int k = 0; k < 3; k++) N[IPX_K_GATHER0 + k] += ctr[11 + k];
 #endif
 }
 
@@ -1190,7 +1198,7 @@ void ipg_app_profile_reset(void)
 {
     for (int k = 0; k < IPX_K_N; k++) {
         ipx_h.prof_launches[k] = ipx_h.prof_timed[k] = 0;
-        ipx_h.prof_ms[k] = ipx_h.prof_bytes[k] = 0.0;
+        ipx_h.prof_ms[k] = ipx_h.prof_bytes[k] = ipx_h.prof_edges[k] = 0.0;
     }
 }
 
@@ -1202,15 +1210,16 @@ uint64_t ipg_app_launches(void)
     return n;
 }
 
-/* One line per kernel: "name launches timed_launches total_ms algorithmic_bytes". */
+/* One line per kernel: "name launches timed_launches total_ms algorithmic_bytes
+ * edges_walked" (edges_walked is 0 for kernels that walk no edge lists). */
 int ipg_app_profile(char* buf, int len)
 {
     int off = 0;
     for (int k = 0; k < IPX_K_N && off < len; k++) {
         if (!ipx_h.prof_launches[k]) continue;
-        off += snprintf(buf + off, (size_t)(len - off), "%s %llu %llu %.6f %.0f\n", ipx_kname[k],
+        off += snprintf(buf + off, (size_t)(len - off), "%s %llu %llu %.6f %.0f %.0f\n", ipx_kname[k],
                         (unsigned long long)ipx_h.prof_launches[k], (unsigned long long)ipx_h.prof_timed[k],
-                        ipx_h.prof_ms[k], ipx_h.prof_bytes[k]);
+                        ipx_h.prof_ms[k], ipx_h.prof_bytes[k], ipx_h.prof_edges[k]);
     }
     return off;
 }

@@ -46,7 +46,7 @@ RUNTIME_SYMBOLS = (
     "ipg_error_f32_f64", "ipg_graph_concat", "ipg_fused_create", "ipg_fused_graph", "ipg_fused_launch",
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
-    "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats",
+    "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats", "ipg_measure_gather",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -133,6 +133,7 @@ def runtime():
         L.ipg_pr_run_f32.argtypes = [vp, ctypes.c_uint32, dbl, i32, vp, vp, vp]
         L.ipg_error_f32_f64.argtypes = [vp, vp, u64, ctypes.POINTER(dbl), ctypes.POINTER(dbl),
                                         ctypes.POINTER(dbl), ctypes.POINTER(u64), vp]
+        L.ipg_measure_gather.argtypes = [u64, ctypes.c_uint32, u64, i32, ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
         _rt = L
     return _rt
 
@@ -542,13 +543,14 @@ class Engine:
         return int(self.lib.ipg_app_launches())
 
     def profile(self) -> dict:
-        """{kernel: {launches, timed, ms, bytes}} accumulated while profiling."""
+        """{kernel: {launches, timed, ms, bytes, edges}} accumulated while
+        profiling; edges = edges walked by push, mark and gather kernels."""
         buf = ctypes.create_string_buffer(8192)
         self.lib.ipg_app_profile(buf, 8192)
         out = {}
         for line in buf.value.decode().splitlines():
-            name, n, t, ms, b = line.split()
-            out[name] = {"launches": int(n), "timed": int(t), "ms": float(ms), "bytes": float(b)}
+            name, n, t, ms, b, e = line.split()
+            out[name] = {"launches": int(n), "timed": int(t), "ms": float(ms), "bytes": float(b), "edges": float(e)}
         return out
 
     def run(self) -> RunResult:
@@ -690,6 +692,15 @@ class PageRankF32:
             self.free()
         except Exception:
             pass
+
+
+def measure_gather(table_bytes: int, row_bytes: int = 4, n: int = 1 << 28, reps: int = 5) -> dict:
+    """The random-gather ceiling (ipg_measure_gather): rows/s and GB/s of n
+    scattered reads of row_bytes-byte rows from a table of table_bytes."""
+    rows, gbs = ctypes.c_double(), ctypes.c_double()
+    _check(runtime().ipg_measure_gather(table_bytes, row_bytes, n, reps, ctypes.byref(rows), ctypes.byref(gbs)),
+           where="ipg_measure_gather")
+    return {"table_bytes": table_bytes, "row_bytes": row_bytes, "rows_per_s": rows.value, "gbs": gbs.value}
 
 
 def error_f32_f64(a: DeviceArray, ref: DeviceArray, stream=None) -> dict:

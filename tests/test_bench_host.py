@@ -57,6 +57,22 @@ def test_clock_csv_parsing():
     assert c["reasons"] == ["sw_power_cap"]
 
 
+def test_nvml_reason_bits():
+    import pynvml as n
+    assert bench.nvml_reasons(0) == []
+    assert bench.nvml_reasons(n.nvmlClocksEventReasonSwPowerCap | n.nvmlClocksEventReasonGpuIdle) == ["sw_power_cap"]
+    mask = (n.nvmlClocksEventReasonHwSlowdown | n.nvmlClocksEventReasonSwThermalSlowdown
+            | n.nvmlClocksEventReasonHwThermalSlowdown)
+    assert sorted(bench.nvml_reasons(mask)) == ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"]
+
+
+def test_clock_sampler_without_gpu_reports_unavailable():
+    s = bench.ClockSampler(0)
+    s.start()
+    c = s.stop()
+    assert "sm_mhz" in c and "reasons" in c
+
+
 @pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built")
 def test_reference_sample_timing():
     g = O.gen_rmat(12, 16, seed=1, undirected=True)
