@@ -291,12 +291,17 @@ typedef struct ipg_server_stats {
     uint64_t groups_freed;
     uint64_t bytes_in_use;       /* lane groups and result buffers */
     uint64_t peak_bytes;
+    uint64_t pull_supersteps;    /* min-plus supersteps relaxed by pulling */
 } ipg_server_stats;
 
-/* hbm_budget: bytes for lane groups and results (0 = unbounded). */
+/* hbm_budget: bytes for lane groups and results (0 = unbounded).  The
+ * environment variables IPG_SERVE_DELTA (near-far bucket width of SSSP lanes,
+ * default 1024) and IPG_SERVE_PULL (0: min-plus supersteps never pull) are
+ * read here. */
 int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_server** out);
 void ipg_server_free(ipg_server* srv);
-/* The graph stays owned by the caller and must outlive the server. */
+/* The graph stays owned by the caller and must outlive the server.  Builds
+ * the graph's degree classes, which synchronises the device. */
 int ipg_server_add_graph(ipg_server* srv, ipg_graph* g, int* gid);
 int ipg_server_submit(ipg_server* srv, int gid, int kind, uint64_t source, uint64_t* qid);
 /* One scheduling pass: completed supersteps retire lanes, pending queries
@@ -312,9 +317,10 @@ int ipg_server_release(ipg_server* srv, uint64_t qid);
 int ipg_server_get_stats(ipg_server* srv, ipg_server_stats* out);
 /* Per graph and group kind (0 min-plus, 1 PPR): summed device time of its
  * supersteps (groups run concurrently, so times overlap), supersteps, lanes
- * admitted. */
+ * admitted, and for min-plus groups the lane-edge relaxations examined (an
+ * edge relaxed for m lanes counts m).  Any output may be NULL. */
 int ipg_server_group_stats(ipg_server* srv, int gid, int group_kind, double* busy_s,
-                           uint64_t* supersteps, uint64_t* lanes);
+                           uint64_t* supersteps, uint64_t* lanes, uint64_t* lane_edges);
 /* Replays an arrival trace in real time (arrival[i] seconds from the start,
  * ascending): submits each query at its time, polls until all are done.
  * latency[i] counts from the scheduled arrival; keep_results = 0 releases

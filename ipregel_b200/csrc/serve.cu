@@ -21,10 +21,11 @@
 //   CC on a graph declared symmetric: union-find over the edges, one pass
 //     (the labels of min-label propagation are the least id of each
 //     component); CC queries admitted together share the pass.
-//   PPR group: 16 lanes; the broadcast quotients b[v][lane] = x/deg (FP32,
-//     64 bytes per vertex) double-buffered; a pull gather over every row: a
-//     thread per low-degree vertex reading whole lane rows as float4 quads,
-//     a half-warp per lane row for higher degrees.  A lane runs exactly
+//   PPR group: 32 lanes; the broadcast quotients b[v][lane] = x/deg (FP32,
+//     128 bytes per vertex, one line) double-buffered; a pull gather over
+//     every row: 8 threads per low-degree vertex, each reading one float4
+//     quad of every in-neighbour's row, a warp per vertex of higher degree
+//     (four rows per load instruction), hub rows in chunks.  A lane runs exactly
 //     `rounds` gathers after admission and writes its last values into the
 //     query's result buffer.
 //
@@ -60,14 +61,25 @@ extern "C" int ipg_internal_fail(int code, const char* msg);
 namespace {
 
 constexpr int MP_K = 64;
-constexpr int PP_K = 16;
+constexpr int PP_K = 32;           // PPR lanes: a row of 32 FP32 quotients is one 128-byte line
+constexpr int PP_Q = PP_K / 4;     // float4 quads per row
+constexpr int PP_SLOTS = 32 / PP_Q;  // rows per warp load instruction
+static_assert(PP_K <= 32 && PP_Q <= 16 && PP_K % 16 == 0, "PPR lanes: a warp covers whole rows");
 constexpr int SRV_THREADS = 256;
 constexpr uint64_t MP_T0 = 8, MP_T1 = 4096;
+constexpr uint64_t PP_T0 = 64;                      // PPR: quads up to this degree, then warps
+constexpr uint64_t PP_NOALLOC_MAX_V = 67108864ull;  // ipg_degree_classes_noalloc's vertex limit
 constexpr uint32_t HUB_CHUNK = 1024;
 constexpr uint32_t SRV_INF = 0xffffffffu;
 constexpr unsigned FULL = 0xffffffffu;
 // Up to MP_SPARSE lanes of a vertex: a thread per edge, each relaxing all.
 constexpr int MP_SPARSE = 8;
+// A min-plus superstep pulls (symmetric graphs) when its frontier holds at
+// least E / MP_PULL_DIV edges and at least MP_PULL_LANES lanes are busy.  On
+// R-MAT graphs of scale 22 and 25 with 32 busy lanes, the dense supersteps
+// took 15-40 % less time pulled than pushed; with 5 lanes, 3-4 times more.
+constexpr uint64_t MP_PULL_DIV = 4;
+constexpr int MP_PULL_LANES = 16;
 // Resident CTAs per SM the min-plus kernels are compiled for (64 registers).
 #define MP_CTAS 4
 
@@ -90,6 +102,8 @@ struct MpStatus {
     uint32_t cnt[3];
     uint32_t chunks;
     uint32_t far_min[64];     // least deferred distance per lane
+    unsigned long long work;  // lane-edge relaxations examined (edges x lanes relaxing them)
+    unsigned long long esum[3];  // degree sums of the next frontier's classes
 };
 
 inline uint32_t warp_grid(uint64_t tasks)
@@ -181,14 +195,16 @@ struct MpArgs {
     const uint64_t* __restrict__ front;
     uint64_t* __restrict__ next;
     uint32_t* __restrict__ fbm;        // bit per vertex: in the next frontier
+    const uint32_t* __restrict__ fcur; // bit per vertex: in this superstep's frontier
     const uint32_t* __restrict__ thr;  // per lane: distances below it relax now
     MpStatus* __restrict__ st;
     uint64_t wmask;                    // lanes whose edges carry their weight (SSSP)
+    uint64_t busy;                     // lanes holding a query
 };
 
 // Per-thread flags of a superstep, reduced per CTA into the status.
 struct MpAcc {
-    unsigned long long any = 0, near = 0, far = 0;
+    unsigned long long any = 0, near = 0, far = 0, work = 0;
 };
 
 // Relaxes edge (v -> u, weight t) for the lanes ks[0..m) of v (distances
@@ -236,6 +252,7 @@ __device__ __forceinline__ void mp_edges_sparse(const MpArgs& a, uint64_t e0, ui
     for (uint64_t e = e0 + lane; e < e1; e += stride) {
         const uint32_t u = a.adj[e];
         const uint32_t t = a.wgt ? a.wgt[e] : 0u;
+        acc.work += (unsigned)m;
         const unsigned long long bits = mp_relax_edge<L>(a, u, t, m, ks, ds);
         if (bits) {
             mp_mark(a, u, bits);
@@ -290,7 +307,10 @@ __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e
     }
     const unsigned long long R = (unsigned long long)Mlo | ((unsigned long long)Mhi << 32);
     if (!R) return;
-    if (lane == 0) acc.near |= R;
+    if (lane == 0) {
+        acc.near |= R;
+        if (__popcll(R) > MP_SPARSE) acc.work += (unsigned long long)__popcll(R) * (e1 - e0);
+    }
     if (__popcll(R) <= MP_SPARSE) {
         int ks[MP_SPARSE];
         uint32_t ds[MP_SPARSE];
@@ -358,16 +378,18 @@ __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e
 // The CTA's flags and least deferred distances into the status.
 __device__ __forceinline__ void mp_block_flush(MpAcc acc, const MpArgs& a, uint32_t* s_fmin)
 {
-    __shared__ unsigned long long s[3][SRV_THREADS / 32];
+    __shared__ unsigned long long s[4][SRV_THREADS / 32];
     for (int o = 16; o > 0; o >>= 1) {
         acc.any |= __shfl_down_sync(FULL, acc.any, o);
         acc.near |= __shfl_down_sync(FULL, acc.near, o);
         acc.far |= __shfl_down_sync(FULL, acc.far, o);
+        acc.work += __shfl_down_sync(FULL, acc.work, o);
     }
     if ((threadIdx.x & 31) == 0) {
         s[0][threadIdx.x >> 5] = acc.any;
         s[1][threadIdx.x >> 5] = acc.near;
         s[2][threadIdx.x >> 5] = acc.far;
+        s[3][threadIdx.x >> 5] = acc.work;
     }
     __syncthreads();
     if (threadIdx.x < 3) {
@@ -375,6 +397,10 @@ __device__ __forceinline__ void mp_block_flush(MpAcc acc, const MpArgs& a, uint3
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) t |= s[threadIdx.x][w];
         unsigned long long* dst = threadIdx.x == 0 ? &a.st->any : (threadIdx.x == 1 ? &a.st->near : &a.st->far);
         if (t) atomicOr(dst, t);
+    } else if (threadIdx.x == 3) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s[3][w];
+        if (t) atomicAdd(&a.st->work, t);
     }
     if (threadIdx.x < MP_K && s_fmin[threadIdx.x] != SRV_INF) atomicMin(&a.st->far_min[threadIdx.x], s_fmin[threadIdx.x]);
 }
@@ -410,6 +436,7 @@ __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_thread(MpArgs a, co
                 continue;
             }
             acc.near |= bit;
+            acc.work += e1 - e0;
             const bool weighted = (a.wmask >> k) & 1ULL;
             for (uint64_t e = e0; e < e1; e++) {
                 const uint32_t u = a.adj[e];
@@ -470,6 +497,170 @@ __global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_hubs(MpArgs a, cons
     mp_block_flush(acc, a, s_fmin);
 }
 
+// Pull supersteps (direction-optimised relaxation, symmetric graphs: a
+// vertex's row lists its in-neighbours).  When the frontier covers a large
+// part of the graph, most edges are relaxed for many lanes at once and the
+// push kernels' atomicMin traffic dominates; pulling, the warp that owns a
+// vertex u gathers, over u's in-neighbours v in this superstep's frontier
+// (bitmap fcur), the candidates dist[v][k] + w of v's frontier lanes k below
+// their thresholds, and lowers dist[u][k] with a plain store: u has one owner,
+// so no atomics.  A neighbour's distance that its own owner lowers during the
+// same superstep is still a path length, and the lowered neighbour is in the
+// next frontier anyway, so reading either value reaches the same fixpoint.
+// Each vertex also classifies its own frontier lanes as the push kernels do:
+// below the threshold they are consumed (near), at or above it deferred into
+// the next frontier.
+
+// Least candidates over in-edges [e0, e1) of the warp's vertex: lane k in b0,
+// lane k + 32 in b1 (SRV_INF when none).  Frontier neighbours are found by a
+// ballot over 32 edges at a time and taken 4 at a time.  Every busy lane of a
+// frontier neighbour below its threshold is a candidate, whether or not the
+// lane itself is in the neighbour's frontier: a lane outside it was relaxed
+// at its current distance already, so its candidate lowers nothing, and not
+// reading the neighbour's frontier mask saves a dependent load per edge.
+// Work counts frontier in-edges.
+__device__ __forceinline__ void mp_pull_edges(const MpArgs& a, uint64_t e0, uint64_t e1, uint32_t thr0, uint32_t thr1,
+                                              bool w0, bool w1, uint32_t& b0, uint32_t& b1, MpAcc& acc)
+{
+    const int lane = threadIdx.x & 31;
+    const bool live0 = (a.busy >> lane) & 1ULL, live1 = (a.busy >> (lane + 32)) & 1ULL;
+    for (uint64_t e = e0; e < e1; e += 32) {
+        const uint64_t ee = e + lane;
+        const uint32_t vj = ee < e1 ? a.adj[ee] : 0u;
+        const bool fr = ee < e1 && ((a.fcur[vj >> 5] >> (vj & 31)) & 1u);
+        uint32_t fm = __ballot_sync(FULL, fr);
+        if (!fm) continue;
+        const uint32_t tj = (fr && a.wgt) ? a.wgt[ee] : 0u;
+        while (fm) {
+            int j[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                j[q] = fm ? __ffs(fm) - 1 : -1;
+                fm &= fm ? fm - 1 : 0u;
+            }
+            uint32_t v[4], t[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                v[q] = __shfl_sync(FULL, vj, j[q] & 31);
+                t[q] = __shfl_sync(FULL, tj, j[q] & 31);
+            }
+            uint32_t d0[4], d1[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                d0[q] = j[q] >= 0 && live0 ? a.dist[(uint64_t)v[q] * MP_K + lane] : SRV_INF;
+                d1[q] = j[q] >= 0 && live1 ? a.dist[(uint64_t)v[q] * MP_K + 32 + lane] : SRV_INF;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (d0[q] < thr0) b0 = min(b0, d0[q] + (w0 ? t[q] : 0u));
+                if (d1[q] < thr1) b1 = min(b1, d1[q] + (w1 ? t[q] : 0u));
+            }
+            if (lane == 0) acc.work += (unsigned long long)(j[0] >= 0) + (j[1] >= 0) + (j[2] >= 0) + (j[3] >= 0);
+        }
+    }
+}
+
+// Own frontier lanes of u (mask fu, distances du0/du1 read by the caller):
+// near lanes into acc.near, deferred ones into acc.far, the least deferred
+// distance per lane into s_fmin; returns the deferred lanes.
+__device__ __forceinline__ unsigned long long mp_pull_own(unsigned long long fu, uint32_t du0, uint32_t du1,
+                                                          uint32_t thr0, uint32_t thr1, MpAcc& acc, uint32_t* s_fmin)
+{
+    const int lane = threadIdx.x & 31;
+    const bool in0 = (fu >> lane) & 1ULL, in1 = (fu >> (lane + 32)) & 1ULL;
+    const bool far0 = in0 && du0 >= thr0, far1 = in1 && du1 >= thr1;
+    if (far0) atomicMin(&s_fmin[lane], du0);
+    if (far1) atomicMin(&s_fmin[lane + 32], du1);
+    const unsigned long long N = (unsigned long long)__ballot_sync(FULL, in0 && !far0) |
+                                 ((unsigned long long)__ballot_sync(FULL, in1 && !far1) << 32);
+    const unsigned long long D = (unsigned long long)__ballot_sync(FULL, far0) |
+                                 ((unsigned long long)__ballot_sync(FULL, far1) << 32);
+    if (lane == 0) {
+        acc.near |= N;
+        acc.far |= D;
+    }
+    return D;
+}
+
+// A warp per vertex of degree <= MP_T1 (the graph's class lists 0 and 1,
+// stored back to back).
+__global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_pull(MpArgs a, const uint32_t* __restrict__ list,
+                                                                   uint64_t n)
+{
+    __shared__ uint32_t s_fmin[MP_K];
+    mp_fmin_init(s_fmin);
+    MpAcc acc;
+    const int lane = threadIdx.x & 31;
+    const uint32_t thr0 = __ldg(&a.thr[lane]), thr1 = __ldg(&a.thr[lane + 32]);
+    const bool w0 = (a.wmask >> lane) & 1ULL, w1 = (a.wmask >> (lane + 32)) & 1ULL;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint32_t u = list[i];
+        uint32_t b0 = SRV_INF, b1 = SRV_INF;
+        mp_pull_edges(a, a.row[u], a.row[u + 1], thr0, thr1, w0, w1, b0, b1, acc);
+        const unsigned long long fu = ((a.fcur[u >> 5] >> (u & 31)) & 1u) ? a.front[u] : 0ULL;
+        if (!fu && !__any_sync(FULL, (b0 & b1) != SRV_INF)) continue;
+        const uint32_t du0 = a.dist[(uint64_t)u * MP_K + lane], du1 = a.dist[(uint64_t)u * MP_K + 32 + lane];
+        const unsigned long long D = fu ? mp_pull_own(fu, du0, du1, thr0, thr1, acc, s_fmin) : 0ULL;
+        const bool i0 = b0 < du0, i1 = b1 < du1;
+        if (i0) a.dist[(uint64_t)u * MP_K + lane] = b0;
+        if (i1) a.dist[(uint64_t)u * MP_K + 32 + lane] = b1;
+        const unsigned long long I = (unsigned long long)__ballot_sync(FULL, i0) |
+                                     ((unsigned long long)__ballot_sync(FULL, i1) << 32);
+        if (lane == 0 && (I | D)) {
+            acc.any |= I;
+            a.next[u] = I | D;  // u's only writer in a pull superstep
+            atomicOr(&a.fbm[u >> 5], 1u << (u & 31));
+        }
+    }
+    __syncthreads();
+    mp_block_flush(acc, a, s_fmin);
+}
+
+// A warp per HUB_CHUNK in-edges of a hub (degree > MP_T1): candidates lower
+// dist[u] by atomicMin (several chunks per hub); the hub's first chunk
+// classifies its own frontier lanes.
+__global__ void __launch_bounds__(SRV_THREADS, MP_CTAS) k_mp_pull_hubs(MpArgs a, const uint32_t* __restrict__ list,
+                                                                        uint32_t n, const uint32_t* __restrict__ prefix)
+{
+    __shared__ uint32_t s_fmin[MP_K];
+    mp_fmin_init(s_fmin);
+    MpAcc acc;
+    const int lane = threadIdx.x & 31;
+    const uint32_t thr0 = __ldg(&a.thr[lane]), thr1 = __ldg(&a.thr[lane + 32]);
+    const bool w0 = (a.wmask >> lane) & 1ULL, w1 = (a.wmask >> (lane + 32)) & 1ULL;
+    if (n) {
+        const uint32_t chunks = prefix[n];
+        const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+        for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
+            const uint32_t i = hub_of_chunk(prefix, n, (uint32_t)c);
+            const uint32_t u = list[i];
+            const uint64_t e0 = a.row[u] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
+            const uint64_t end = a.row[u + 1];
+            uint32_t b0 = SRV_INF, b1 = SRV_INF;
+            mp_pull_edges(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, thr0, thr1, w0, w1, b0, b1, acc);
+            unsigned long long D = 0;
+            if ((uint32_t)c == prefix[i]) {
+                const unsigned long long fu = ((a.fcur[u >> 5] >> (u & 31)) & 1u) ? a.front[u] : 0ULL;
+                if (fu)
+                    D = mp_pull_own(fu, a.dist[(uint64_t)u * MP_K + lane], a.dist[(uint64_t)u * MP_K + 32 + lane], thr0,
+                                    thr1, acc, s_fmin);
+            }
+            const bool i0 = b0 != SRV_INF && b0 < atomicMin(&a.dist[(uint64_t)u * MP_K + lane], b0);
+            const bool i1 = b1 != SRV_INF && b1 < atomicMin(&a.dist[(uint64_t)u * MP_K + 32 + lane], b1);
+            const unsigned long long I = (unsigned long long)__ballot_sync(FULL, i0) |
+                                         ((unsigned long long)__ballot_sync(FULL, i1) << 32);
+            if (lane == 0 && (I | D)) {
+                acc.any |= I;
+                atomicOr((unsigned long long*)&a.next[u], I | D);
+                atomicOr(&a.fbm[u >> 5], 1u << (u & 31));
+            }
+        }
+    }
+    __syncthreads();
+    mp_block_flush(acc, a, s_fmin);
+}
+
 // After a superstep: the consumed frontier masks back to zero.
 __global__ void k_mp_clear(uint64_t* __restrict__ front, const uint32_t* __restrict__ l0, const uint32_t* __restrict__ l1,
                            const uint32_t* __restrict__ l2, const uint32_t* __restrict__ cnt)
@@ -493,13 +684,14 @@ __global__ void k_mp_init_lane(uint32_t* __restrict__ dist, uint64_t* __restrict
 }
 
 // SSSP source s of lane k: distance 0 and into the current frontier lists.
-__global__ void k_mp_admit_source(uint32_t* __restrict__ dist, uint64_t* __restrict__ front,
+__global__ void k_mp_admit_source(uint32_t* __restrict__ dist, uint64_t* __restrict__ front, uint32_t* __restrict__ fcur,
                                   const uint64_t* __restrict__ row, uint64_t s, int k, uint32_t* __restrict__ l0,
                                   uint32_t* __restrict__ l1, uint32_t* __restrict__ l2, uint32_t* __restrict__ cnt)
 {
     dist[s * MP_K + k] = 0u;
     const unsigned long long old = front[s];
     front[s] = old | (1ULL << k);
+    fcur[s >> 5] |= 1u << (s & 31);
     if (!old) {
         const uint64_t d = row[s + 1] - row[s];
         const int cls = d <= MP_T0 ? 0 : (d <= MP_T1 ? 1 : 2);
@@ -736,34 +928,86 @@ __device__ __forceinline__ float pp_value(const PpLanes& L, int k, uint64_t v, f
     return __fadd_rn(L.seed[k] == (uint32_t)v ? 0.15f : 0.0f, __fmul_rn(0.85f, sum));
 }
 
-// A warp gathers [e0, e1): thread t takes edge slot t / 4 of every group of
-// 8 edges and lane quad t % 4, reading the neighbour's quad as one float4 and
-// summing its 4 lanes; then the 8 slots of each quad merge.  Threads 0..3 end
-// with the totals of lanes 4t..4t+3.  The order of a lane's terms depends on
-// the edge list only, not on which other lanes are active.
-__device__ __forceinline__ void pp_gather4(const PpArgs& a, uint64_t e0, uint64_t e1, bool quad_on, float* s, float* c)
+// Sum of up to four float4 terms, pairwise: (x0 + x1) + (x2 + x3), absent
+// terms 0.  All terms are non-negative quotients, so the group's rounding
+// error is at most 2 ulp of the group sum; the group then enters the
+// compensated sum as one term.  This cuts the compensated additions per
+// gathered row by four.
+__device__ __forceinline__ float4 pp_sum4(float4 x0, float4 x1, float4 x2, float4 x3)
 {
-    const int lane = threadIdx.x & 31, slot = lane >> 2, q = lane & 3;
+    return make_float4(__fadd_rn(__fadd_rn(x0.x, x1.x), __fadd_rn(x2.x, x3.x)),
+                       __fadd_rn(__fadd_rn(x0.y, x1.y), __fadd_rn(x2.y, x3.y)),
+                       __fadd_rn(__fadd_rn(x0.z, x1.z), __fadd_rn(x2.z, x3.z)),
+                       __fadd_rn(__fadd_rn(x0.w, x1.w), __fadd_rn(x2.w, x3.w)));
+}
+
+__device__ __forceinline__ void pp_add4(float* s, float* c, float4 t)
+{
+    pp_add(s[0], c[0], t.x);
+    pp_add(s[1], c[1], t.y);
+    pp_add(s[2], c[2], t.z);
+    pp_add(s[3], c[3], t.w);
+}
+
+// Quad q (lanes 4q..4q+3) of u's row: one 16-byte load.
+__device__ __forceinline__ float4 pp_row(const PpArgs& a, uint32_t u, int q)
+{
+    return reinterpret_cast<const float4*>(a.b_cur + (uint64_t)u * PP_K)[q];
+}
+
+// Threads q < PP_Q of a group finish lanes 4q..4q+3 of vertex v from their
+// compensated sums: x to the result buffer of a lane in its last gather,
+// else the quotient x / deg into the next row.
+__device__ __forceinline__ void pp_finish_quad(const PpArgs& a, const PpLanes& L, uint64_t v, uint64_t deg, int q,
+                                               const float* s, const float* c)
+{
+    float bn[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) s[i] = c[i] = 0.0f;
-    for (uint64_t e = e0; e < e1; e += 32) {
-        const uint32_t uj = (e + lane < e1) ? a.adj[e + lane] : 0u;
-        const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const int jj = r * 8 + slot;
-            const uint32_t u = __shfl_sync(FULL, uj, jj);
-            if (quad_on && jj < nj) {
-                const float4 x = reinterpret_cast<const float4*>(a.b_cur + (uint64_t)u * PP_K)[q];
-                pp_add(s[0], c[0], x.x);
-                pp_add(s[1], c[1], x.y);
-                pp_add(s[2], c[2], x.z);
-                pp_add(s[3], c[3], x.w);
-            }
+    for (int j = 0; j < 4; j++) {
+        const int k = 4 * q + j;
+        bn[j] = 0.0f;
+        if ((L.active >> k) & 1u) {
+            const float xn = pp_value(L, k, v, __fadd_rn(s[j], c[j]));
+            if (L.out[k]) L.out[k][v] = xn;
+            else if (deg) bn[j] = __fdiv_rn(xn, (float)deg);
         }
     }
+    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
+}
+
+// A warp gathers [e0, e1): thread t takes lane quad t % PP_Q and edge slot
+// t / PP_Q (PP_SLOTS slots), reading the neighbour's quad as one float4, so
+// each load instruction reads PP_SLOTS whole rows.  Every 4 rows of a thread
+// are summed pairwise and added compensated; the next 32 ids are loaded while
+// the current rows are in flight.  Then the slots of each quad merge (TwoSum),
+// and threads 0..PP_Q-1 hold the totals of their quads.  The order of a
+// lane's terms depends on the edge list only, not on which lanes are active.
+__device__ __forceinline__ void pp_gather_warp(const PpArgs& a, uint64_t e0, uint64_t e1, bool quad_on, float* s,
+                                               float* c)
+{
+    const int lane = threadIdx.x & 31, slot = lane / PP_Q, q = lane % PP_Q;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int off = 4; off < 32; off <<= 1)
+    for (int i = 0; i < 4; i++) s[i] = c[i] = 0.0f;
+    uint32_t uj = (e0 + lane < e1) ? a.adj[e0 + lane] : 0u;
+    for (uint64_t e = e0; e < e1; e += 32) {
+        const uint32_t un = (e + 32 + lane < e1) ? a.adj[e + 32 + lane] : 0u;
+        const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
+#pragma unroll
+        for (int h = 0; h < 32 / PP_SLOTS; h += 4) {
+            float4 x[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int jj = (h + r) * PP_SLOTS + slot;
+                const uint32_t u = __shfl_sync(FULL, uj, jj);
+                x[r] = (quad_on && jj < nj) ? pp_row(a, u, q) : z;
+            }
+            if (quad_on) pp_add4(s, c, pp_sum4(x[0], x[1], x[2], x[3]));
+        }
+        uj = un;
+    }
+#pragma unroll
+    for (int off = PP_Q; off < 32; off <<= 1)
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const float s2 = __shfl_xor_sync(FULL, s[i], off), c2 = __shfl_xor_sync(FULL, c[i], off);
@@ -771,103 +1015,65 @@ __device__ __forceinline__ void pp_gather4(const PpArgs& a, uint64_t e0, uint64_
         }
 }
 
-// Threads 0..3 finish lanes 4t..4t+3 of vertex v.
-__device__ __forceinline__ void pp_finish4(const PpArgs& a, const PpLanes& L, uint64_t v, uint64_t deg, const float* s,
-                                           const float* c)
+// PP_Q threads per low-degree vertex (degree <= PP_T0): thread q of the group
+// takes lane quad q of every in-neighbour's row, so a warp reads 32 / PP_Q
+// whole rows per load instruction and no partial sums need merging.  Four
+// threads of the group load four consecutive ids at a time and the group
+// shares them by shuffle; the four rows are summed pairwise and added
+// compensated, in edge order.
+__global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+                                                         uint64_t n)
 {
-    const int q = threadIdx.x & 31;
-    if (q >= 4) return;
-    float bn[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int k = 4 * q + i;
-        bn[i] = 0.0f;
-        if ((L.active >> k) & 1u) {
-            const float xn = pp_value(L, k, v, __fadd_rn(s[i], c[i]));
-            if (L.out[k]) L.out[k][v] = xn;
-            else if (deg) bn[i] = __fdiv_rn(xn, (float)deg);
-        }
-    }
-    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
-}
-
-// Threads 0..15 finish vertex v for their lane from (s, c).
-__device__ __forceinline__ void pp_finish(const PpArgs& a, const PpLanes& L, uint64_t v, uint64_t deg, float s, float c)
-{
-    const int k = threadIdx.x & 31;
-    if (k >= PP_K) return;
-    float bn = 0.0f;
-    if ((L.active >> k) & 1u) {
-        const float xn = pp_value(L, k, v, __fadd_rn(s, c));
-        if (L.out[k]) L.out[k][v] = xn;
-        else if (deg) bn = __fdiv_rn(xn, (float)deg);
-    }
-    a.b_next[v * PP_K + k] = bn;
-}
-
-// A thread per low-degree vertex (class 0): each in-neighbour's lane row
-// read as NQ float4 quads (lanes 4 NQ and up are idle, their quotients 0)
-// and summed per lane in edge order.
-template <int NQ>
-__global__ void __launch_bounds__(SRV_THREADS, 4) k_pp_thread(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
-                                                              uint64_t n)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, q = lane % PP_Q, gb = lane - q;
+    const unsigned gmask = ((1u << PP_Q) - 1u) << gb;
+    const bool quad_on = (L.active >> (4 * q)) & 0xFu;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint64_t groups = ((uint64_t)gridDim.x * blockDim.x) / PP_Q;
+    // the threads of a group share i, so they leave the loop together
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / PP_Q; i < n; i += groups) {
         const uint64_t v = list[i];
         const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
-        float s[4 * NQ], c[4 * NQ];
+        float s[4], c[4];
 #pragma unroll
-        for (int k = 0; k < 4 * NQ; k++) s[k] = c[k] = 0.0f;
-        for (uint64_t e = e0; e < e1; e++) {
-            const float4* r = reinterpret_cast<const float4*>(a.b_cur + (uint64_t)a.adj[e] * PP_K);
+        for (int k = 0; k < 4; k++) s[k] = c[k] = 0.0f;
+        for (uint64_t e = e0; e < e1; e += 4) {
+            const uint32_t uj = (q < 4 && e + q < e1) ? a.adj[e + q] : 0u;
+            const int ne = (int)((e1 - e) < 4 ? (e1 - e) : 4);
+            float4 x[4];
 #pragma unroll
-            for (int q = 0; q < NQ; q++) {
-                const float4 x = r[q];
-                pp_add(s[4 * q + 0], c[4 * q + 0], x.x);
-                pp_add(s[4 * q + 1], c[4 * q + 1], x.y);
-                pp_add(s[4 * q + 2], c[4 * q + 2], x.z);
-                pp_add(s[4 * q + 3], c[4 * q + 3], x.w);
+            for (int r = 0; r < 4; r++) {
+                const uint32_t u = __shfl_sync(gmask, uj, gb + r);
+                x[r] = (quad_on && r < ne) ? pp_row(a, u, q) : z;
             }
+            if (quad_on) pp_add4(s, c, pp_sum4(x[0], x[1], x[2], x[3]));
         }
-        const uint64_t deg = e1 - e0;
-        float bn[PP_K];
-#pragma unroll
-        for (int k = 0; k < PP_K; k++) {
-            bn[k] = 0.0f;
-            if (k < 4 * NQ && ((L.active >> k) & 1u)) {
-                const float xn = pp_value(L, k, v, __fadd_rn(s[k], c[k]));
-                if (L.out[k]) L.out[k][v] = xn;
-                else if (deg) bn[k] = __fdiv_rn(xn, (float)deg);
-            }
-        }
-        float4* w = reinterpret_cast<float4*>(a.b_next + v * PP_K);
-#pragma unroll
-        for (int q = 0; q < PP_K / 4; q++) w[q] = make_float4(bn[4 * q], bn[4 * q + 1], bn[4 * q + 2], bn[4 * q + 3]);
+        pp_finish_quad(a, L, v, e1 - e0, q, s, c);
     }
 }
 
-// A warp per vertex (class 1).
+// A warp per vertex of higher degree (up to MP_T1).
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                              uint64_t n)
 {
-    const bool quad_on = (L.active >> (4 * (threadIdx.x & 3))) & 0xFu;
+    const int lane = threadIdx.x & 31;
+    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFu;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
         const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
         float s[4], c[4];
-        pp_gather4(a, e0, e1, quad_on, s, c);
-        pp_finish4(a, L, v, e1 - e0, s, c);
+        pp_gather_warp(a, e0, e1, quad_on, s, c);
+        if (lane < PP_Q) pp_finish_quad(a, L, v, e1 - e0, lane, s, c);
     }
 }
 
-// Hubs (class 2): a warp per HUB_CHUNK edges, partial sums per chunk and lane...
+// Hubs: a warp per HUB_CHUNK edges, partial sums per chunk and lane...
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                                uint32_t n, const uint32_t* __restrict__ prefix)
 {
     if (!n) return;
     const int lane = threadIdx.x & 31;
-    const bool quad_on = (L.active >> (4 * (lane & 3))) & 0xFu;
+    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFu;
     const uint32_t chunks = prefix[n];
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
@@ -876,18 +1082,20 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes
         const uint64_t e0 = a.row[v] + (uint64_t)((uint32_t)c - prefix[i]) * HUB_CHUNK;
         const uint64_t end = a.row[v + 1];
         float s[4], cc[4];
-        pp_gather4(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, quad_on, s, cc);
-        if (lane < 4)
+        pp_gather_warp(a, e0, e0 + HUB_CHUNK < end ? e0 + HUB_CHUNK : end, quad_on, s, cc);
+        if (lane < PP_Q)
 #pragma unroll
             for (int j = 0; j < 4; j++) a.partial[c * PP_K + 4 * lane + j] = make_float2(s[j], cc[j]);
     }
 }
 
-// ...then a warp per hub merges its chunks' partials in chunk order.
+// ...then a warp per hub merges its chunks' partials in chunk order (a
+// thread per lane) and threads 0..PP_Q-1 finish the hub's quads.
 __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_finish(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                                uint32_t n, const uint32_t* __restrict__ prefix)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ float2 sh[SRV_THREADS / 32][PP_K];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
@@ -897,7 +1105,18 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_finish(PpArgs a, PpLanes
                 const float2 p = a.partial[(uint64_t)ch * PP_K + lane];
                 pp_merge(s, c, p.x, p.y);
             }
-        pp_finish(a, L, v, a.row[v + 1] - a.row[v], s, c);
+        if (lane < PP_K) sh[w][lane] = make_float2(s, c);
+        __syncwarp();
+        if (lane < PP_Q) {
+            float s4[4], c4[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                s4[j] = sh[w][4 * lane + j].x;
+                c4[j] = sh[w][4 * lane + j].y;
+            }
+            pp_finish_quad(a, L, v, a.row[v + 1] - a.row[v], lane, s4, c4);
+        }
+        __syncwarp();
     }
 }
 
@@ -956,8 +1175,9 @@ struct Group {
     uint32_t* dist = nullptr;
     uint64_t* front[2] = {nullptr, nullptr};
     int cur = 0;
-    uint32_t* fbm = nullptr;
+    uint32_t* fbm[2] = {nullptr, nullptr};  // frontier bitmaps: [cur] this superstep's, [cur ^ 1] the next
     uint32_t* list[3] = {nullptr, nullptr, nullptr};
+    uint64_t hesum = 0;                   // frontier edges of the next superstep (last status)
     uint32_t* cnt = nullptr;              // into stat_d
     uint32_t* prefix = nullptr;
     uint32_t* thr_d = nullptr;            // lane thresholds of the next superstep
@@ -973,6 +1193,12 @@ struct Group {
     // PPR
     float* b[2] = {nullptr, nullptr};
     float2* partial = nullptr;
+    // gather classes: quads for degree <= PP_T0, warps up to MP_T1 (hubs
+    // above, from the graph's classes); null when the graph is too large for
+    // ipg_degree_classes_noalloc, and then the graph's classes serve
+    uint32_t* pp_list = nullptr;
+    uint64_t* pp_tot = nullptr;
+    uint64_t pp_n[2] = {0, 0};
     int it[PP_K] = {0};
     uint32_t seed[PP_K] = {0};
     uint64_t supersteps = 0;
@@ -1006,11 +1232,14 @@ struct ipg_server {
     std::vector<uint64_t> completed;            // done since the last drain
     std::vector<double> busy_s;                 // per graph and group kind: superstep device time
     std::vector<uint64_t> steps, lanes;         // supersteps, lanes admitted
+    std::vector<uint64_t> work;                 // min-plus lane-edge relaxations examined
     std::multimap<uint64_t, void*> pool;        // released result buffers by size
     uint64_t next_id = 1;
     // near-far bucket width of SSSP lanes (IPG_SERVE_DELTA); on R-MAT graphs
     // with weights in [1, 255], 256..1024 measured best, 7 % faster than none
     uint32_t delta = 1024;
+    // dense min-plus supersteps on symmetric graphs pull (IPG_SERVE_PULL=0: never)
+    bool pull = true;
     std::mutex mu;
     ipg_server_stats stats{};
 };
@@ -1037,8 +1266,8 @@ void free_group(ipg_server* S, Group* G)
 uint64_t group_bytes(const Graph* G, int kind)
 {
     const uint64_t V = G->gv.V, E = G->gv.E;
-    if (kind == 0) return V * (MP_K * 4 + 16 + 12) + V / 8 + (E / (MP_T1 + 1) + 2) * 4 + 4096;
-    return V * (PP_K * 4 * 2) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8) + 4096;
+    if (kind == 0) return V * (MP_K * 4 + 16 + 12) + V / 4 + (E / (MP_T1 + 1) + 2) * 4 + 4096;
+    return V * (PP_K * 4 * 2 + 4) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8) + 4096;
 }
 
 // Frees idle groups (least recently used first), then cached result buffers,
@@ -1141,7 +1370,8 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
         if (r == IPG_OK) r = galloc(G, &G->dist, V * MP_K);
         if (r == IPG_OK) r = galloc(G, &G->front[0], V);
         if (r == IPG_OK) r = galloc(G, &G->front[1], V);
-        if (r == IPG_OK) r = galloc(G, &G->fbm, (V + 31) / 32 + 1);
+        if (r == IPG_OK) r = galloc(G, &G->fbm[0], (V + 31) / 32 + 1);
+        if (r == IPG_OK) r = galloc(G, &G->fbm[1], (V + 31) / 32 + 1);
         for (int k = 0; k < 3 && r == IPG_OK; k++) r = galloc(G, &G->list[k], V);
         if (r == IPG_OK) r = galloc(G, &G->stat_d, 1);
         if (r == IPG_OK) G->cnt = G->stat_d->cnt;
@@ -1155,7 +1385,8 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
             cudaMemsetAsync(G->dist, 0xff, V * MP_K * 4, G->st);  // every lane INF
             cudaMemsetAsync(G->front[0], 0, V * 8, G->st);
             cudaMemsetAsync(G->front[1], 0, V * 8, G->st);
-            cudaMemsetAsync(G->fbm, 0, ((V + 31) / 32 + 1) * 4, G->st);
+            cudaMemsetAsync(G->fbm[0], 0, ((V + 31) / 32 + 1) * 4, G->st);
+            cudaMemsetAsync(G->fbm[1], 0, ((V + 31) / 32 + 1) * 4, G->st);
             cudaMemsetAsync(G->stat_d, 0, sizeof(MpStatus), G->st);
             cudaMemsetAsync(G->prefix, 0, 8, G->st);
         }
@@ -1168,6 +1399,21 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
             // quotients of idle lanes are 0: an admitted lane sets its seed only
             cudaMemsetAsync(G->b[0], 0, V * PP_K * 4, G->st);
             cudaMemsetAsync(G->b[1], 0, V * PP_K * 4, G->st);
+        }
+        if (r == IPG_OK && V <= PP_NOALLOC_MAX_V) {
+            if (r == IPG_OK) r = galloc(G, &G->pp_list, V);
+            if (r == IPG_OK) r = galloc(G, &G->pp_tot, 6);
+            // the server's calls of ipg_degree_classes_noalloc are serialised
+            // by this synchronisation (its scratch is shared)
+            uint64_t tot[6] = {0, 0, 0, 0, 0, 0};
+            if (r == IPG_OK) r = ipg_degree_classes_noalloc(V, Gr->gv.d_row, PP_T0, MP_T1, G->pp_list, G->pp_tot, G->st);
+            if (r == IPG_OK && (cudaMemcpyAsync(tot, G->pp_tot, sizeof tot, cudaMemcpyDeviceToHost, G->st) != cudaSuccess ||
+                                cudaStreamSynchronize(G->st) != cudaSuccess))
+                r = ipg_internal_fail(IPG_ECUDA, "serve: PPR degree classes failed");
+            if (r == IPG_OK && tot[2] != Gr->bins.count[2])
+                r = ipg_internal_fail(IPG_EINVAL, "serve: PPR hub class differs from the graph's");
+            G->pp_n[0] = tot[0];
+            G->pp_n[1] = tot[1];
         }
     }
     if (r == IPG_OK && cudaGetLastError() != cudaSuccess) r = ipg_internal_fail(IPG_ECUDA, "serve: group setup failed");
@@ -1274,8 +1520,8 @@ void admit(ipg_server* S, Group* G, double now)
                 rebuild = true;
             } else {
                 // the lane is INF everywhere (cleared when its last query was extracted)
-                k_mp_admit_source<<<1, 1, 0, G->st>>>(G->dist, G->front[G->cur], G->G->gv.d_row, q.src, k,
-                                                       G->list[0], G->list[1], G->list[2], G->cnt);
+                k_mp_admit_source<<<1, 1, 0, G->st>>>(G->dist, G->front[G->cur], G->fbm[G->cur], G->G->gv.d_row,
+                                                       q.src, k, G->list[0], G->list[1], G->list[2], G->cnt);
                 G->wmask |= 1ULL << k;
                 G->thr_h[k] = S->delta;
                 G->appended++;
@@ -1291,15 +1537,17 @@ void admit(ipg_server* S, Group* G, double now)
         // a label-propagation CC lane puts every vertex into the frontier:
         // rebuild the lists and read their sizes back (grids are sized by them)
         k_mp_mark_all<<<resident_cap(k_mp_mark_all, thread_grid((V + 31) / 32)), SRV_THREADS, 0, G->st>>>(
-            G->front[G->cur], V, G->fbm);
+            G->front[G->cur], V, G->fbm[G->cur]);
         cudaMemsetAsync(G->cnt, 0, 12, G->st);
-        ipg_compact(G->fbm, V, G->G->gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
-                    G->st);
+        cudaMemsetAsync(G->stat_d->esum, 0, sizeof G->stat_d->esum, G->st);
+        ipg_compact(G->fbm[G->cur], V, G->G->gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt,
+                    (uint64_t*)G->stat_d->esum, 0, G->st);
         k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, G->G->gv.d_row, G->prefix, &G->stat_d->chunks);
         cudaMemcpyAsync(G->stat_h, G->stat_d, sizeof(MpStatus), cudaMemcpyDeviceToHost, G->st);
         cudaStreamSynchronize(G->st);
         for (int c = 0; c < 3; c++) G->hn[c] = G->stat_h->cnt[c];
         G->hchunks = G->stat_h->chunks;
+        G->hesum = G->stat_h->esum[0] + G->stat_h->esum[1] + G->stat_h->esum[2];
         G->appended = 0;
     }
 }
@@ -1316,10 +1564,12 @@ int launch_superstep(ipg_server* S, Group* G)
         a.dist = G->dist;
         a.front = G->front[G->cur];
         a.next = G->front[G->cur ^ 1];
-        a.fbm = G->fbm;
+        a.fbm = G->fbm[G->cur ^ 1];
+        a.fcur = G->fbm[G->cur];
         a.thr = G->thr_d;
         a.st = G->stat_d;
         a.wmask = G->wmask;
+        a.busy = G->busy;
         // grids from the list sizes of the last status plus the sources
         // appended since (each in some list; a hub one adds its chunks)
         const uint64_t add = G->appended;
@@ -1330,21 +1580,45 @@ int launch_superstep(ipg_server* S, Group* G)
         cudaMemcpyAsync(G->thr_d, G->thr_pin, sizeof G->thr_h, cudaMemcpyHostToDevice, G->st);
         cudaMemsetAsync(G->stat_d, 0, 3 * sizeof(unsigned long long), G->st);
         cudaMemsetAsync(G->stat_d->far_min, 0xff, sizeof G->stat_d->far_min, G->st);
-        if (add) k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, nullptr);
-        k_mp_thread<<<resident_cap(k_mp_thread, thread_grid(n0)), SRV_THREADS, 0, G->st>>>(a, G->list[0], G->cnt + 0);
-        k_mp_vertices<<<resident_cap(k_mp_vertices, warp_grid(n1)), SRV_THREADS, 0, G->st>>>(a, G->list[1],
-                                                                                          G->cnt + 1);
-        k_mp_hubs<<<resident_cap(k_mp_hubs, warp_grid(chunks)), SRV_THREADS, 0, G->st>>>(a, G->list[2], G->cnt + 2,
-                                                                                      G->prefix);
+        cudaMemsetAsync(&G->stat_d->work, 0, sizeof G->stat_d->work, G->st);
+        cudaMemsetAsync(G->stat_d->esum, 0, sizeof G->stat_d->esum, G->st);
+        // direction: pull when the frontier's edges are a large part of the
+        // graph and enough lanes are busy to share each row read
+        const Graph* Gr = G->G;
+        const bool pull = S->pull && gv.symmetric && Gr->classes && __builtin_popcountll(G->busy) >= MP_PULL_LANES &&
+                          G->hesum * MP_PULL_DIV >= gv.E;
+        if (pull) {
+            const ipg_bins& B = Gr->bins;
+            const uint64_t n01 = B.count[0] + B.count[1];
+            if (n01)
+                k_mp_pull<<<resident_cap(k_mp_pull, warp_grid(n01)), SRV_THREADS, 0, G->st>>>(a, B.d_list[0], n01);
+            if (B.count[2])
+                k_mp_pull_hubs<<<resident_cap(k_mp_pull_hubs, warp_grid(Gr->hub_chunks)), SRV_THREADS, 0, G->st>>>(
+                    a, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix);
+            S->stats.kernel_launches += (n01 ? 1 : 0) + (B.count[2] ? 1 : 0);
+        } else {
+            if (add) k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, nullptr);
+            k_mp_thread<<<resident_cap(k_mp_thread, thread_grid(n0)), SRV_THREADS, 0, G->st>>>(a, G->list[0],
+                                                                                            G->cnt + 0);
+            k_mp_vertices<<<resident_cap(k_mp_vertices, warp_grid(n1)), SRV_THREADS, 0, G->st>>>(a, G->list[1],
+                                                                                              G->cnt + 1);
+            k_mp_hubs<<<resident_cap(k_mp_hubs, warp_grid(chunks)), SRV_THREADS, 0, G->st>>>(a, G->list[2],
+                                                                                          G->cnt + 2, G->prefix);
+            S->stats.kernel_launches += 3 + (add ? 1 : 0);
+        }
+        S->stats.pull_supersteps += pull ? 1 : 0;
         k_mp_clear<<<resident_cap(k_mp_clear, thread_grid(G->hn[0] + G->hn[1] + G->hn[2] + add)), SRV_THREADS, 0,
                      G->st>>>(G->front[G->cur], G->list[0], G->list[1], G->list[2], G->cnt);
         cudaMemsetAsync(G->cnt, 0, 12, G->st);
-        ipg_compact(G->fbm, gv.V, gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt, nullptr, 1,
-                    G->st);
+        // the next bitmap is kept (it is the next superstep's frontier bitmap);
+        // this superstep's is cleared for reuse as the one after
+        ipg_compact(G->fbm[G->cur ^ 1], gv.V, gv.d_row, MP_T0, MP_T1, G->list[0], G->list[1], G->list[2], G->cnt,
+                    (uint64_t*)G->stat_d->esum, 0, G->st);
+        cudaMemsetAsync(G->fbm[G->cur], 0, ((gv.V + 31) / 32 + 1) * 4, G->st);
         k_chunk_prefix<<<1, 1024, 0, G->st>>>(G->list[2], G->cnt + 2, gv.d_row, G->prefix, &G->stat_d->chunks);
         cudaMemcpyAsync(G->stat_h, G->stat_d, sizeof(MpStatus), cudaMemcpyDeviceToHost, G->st);
         G->cur ^= 1;
-        S->stats.kernel_launches += 7 + (add ? 1 : 0);
+        S->stats.kernel_launches += 4;
     } else {
         const Graph* Gr = G->G;
         PpArgs a;
@@ -1362,24 +1636,14 @@ int launch_superstep(ipg_server* S, Group* G)
                 L.out[k] = (float*)S->queries[G->lane_q[k][0]].result;
         }
         const ipg_bins& B = Gr->bins;
-        // quads of lanes in use: lanes are taken lowest first
-        const int top = 32 - __builtin_clz((uint32_t)G->busy | 1u);
-        const int nq = (top + 3) / 4;
-        const uint64_t n0 = B.count[0];
-        if (n0) {
-            const uint32_t gt = thread_grid(n0);
-            if (nq <= 1)
-                k_pp_thread<1><<<resident_cap(k_pp_thread<1>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
-            else if (nq == 2)
-                k_pp_thread<2><<<resident_cap(k_pp_thread<2>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
-            else if (nq == 3)
-                k_pp_thread<3><<<resident_cap(k_pp_thread<3>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
-            else
-                k_pp_thread<4><<<resident_cap(k_pp_thread<4>, gt), SRV_THREADS, 0, G->st>>>(a, L, B.d_list[0], n0);
-        }
-        if (B.count[1])
-            k_pp_vertices<<<resident_cap(k_pp_vertices, warp_grid(B.count[1])), SRV_THREADS, 0, G->st>>>(
-                a, L, B.d_list[1], B.count[1]);
+        const uint32_t* l0 = G->pp_list ? G->pp_list : B.d_list[0];
+        const uint64_t n0 = G->pp_list ? G->pp_n[0] : B.count[0];
+        const uint32_t* l1 = G->pp_list ? G->pp_list + n0 : B.d_list[1];
+        const uint64_t n1 = G->pp_list ? G->pp_n[1] : B.count[1];
+        if (n0)
+            k_pp_rows<<<resident_cap(k_pp_rows, thread_grid(n0 * PP_Q)), SRV_THREADS, 0, G->st>>>(a, L, l0, n0);
+        if (n1)
+            k_pp_vertices<<<resident_cap(k_pp_vertices, warp_grid(n1)), SRV_THREADS, 0, G->st>>>(a, L, l1, n1);
         if (B.count[2]) {
             k_pp_hub_chunks<<<resident_cap(k_pp_hub_chunks, warp_grid(Gr->hub_chunks)), SRV_THREADS, 0, G->st>>>(
                 a, L, B.d_list[2], (uint32_t)B.count[2], Gr->hub_prefix);
@@ -1405,6 +1669,8 @@ void retire(ipg_server* S, Group* G, double now)
         const MpStatus& st = *G->stat_h;
         for (int c = 0; c < 3; c++) G->hn[c] = st.cnt[c];
         G->hchunks = st.chunks;
+        S->work[(size_t)G->G->gid * 2] += st.work;
+        G->hesum = st.esum[0] + st.esum[1] + st.esum[2];
         G->appended = 0;
         const uint64_t live = st.any | st.far;
         const uint64_t done = G->busy & ~live;
@@ -1461,6 +1727,8 @@ extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_s
     S->rounds = ppr_rounds;
     if (const char* d = getenv("IPG_SERVE_DELTA"))
         if (*d) S->delta = (uint32_t)std::max(1UL, strtoul(d, nullptr, 10));
+    if (const char* p = getenv("IPG_SERVE_PULL"))
+        if (*p) S->pull = strtol(p, nullptr, 10) != 0;
     *out = S;
     return IPG_OK;
 }
@@ -1493,6 +1761,13 @@ extern "C" int ipg_server_add_graph(ipg_server* S, ipg_graph* g, int* gid)
     if (G->gv.d_wgt && G->gv.weight_bytes != 4)
         return ipg_internal_fail(IPG_EINVAL, "ipg_server_add_graph: weights must be u32");
     std::lock_guard<std::mutex> lk(S->mu);
+    // degree classes and hub chunks (the PPR gathers, the union-find pass and
+    // the pull supersteps walk them) are built now, before queries arrive:
+    // building them synchronises the device
+    if ((r = graph_classes(G.get(), nullptr)) != IPG_OK) {
+        if (G->hub_prefix) ipg_dev_free(G->hub_prefix, (G->bins.count[2] + 5) * 4);
+        return r;
+    }
     *gid = (int)S->graphs.size();
     G->gid = *gid;
     S->graphs.push_back(std::move(G));
@@ -1500,6 +1775,7 @@ extern "C" int ipg_server_add_graph(ipg_server* S, ipg_graph* g, int* gid)
     S->busy_s.resize(S->graphs.size() * 2, 0.0);
     S->steps.resize(S->graphs.size() * 2, 0);
     S->lanes.resize(S->graphs.size() * 2, 0);
+    S->work.resize(S->graphs.size() * 2, 0);
     return IPG_OK;
 }
 
@@ -1658,7 +1934,7 @@ extern "C" int ipg_server_get_stats(ipg_server* S, ipg_server_stats* out)
 }
 
 extern "C" int ipg_server_group_stats(ipg_server* S, int gid, int group_kind, double* busy_s, uint64_t* supersteps,
-                                      uint64_t* lanes)
+                                      uint64_t* lanes, uint64_t* lane_edges)
 {
     if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_group_stats: null server");
     std::lock_guard<std::mutex> lk(S->mu);
@@ -1668,6 +1944,7 @@ extern "C" int ipg_server_group_stats(ipg_server* S, int gid, int group_kind, do
     if (busy_s) *busy_s = S->busy_s[slot];
     if (supersteps) *supersteps = S->steps[slot];
     if (lanes) *lanes = S->lanes[slot];
+    if (lane_edges) *lane_edges = S->work[slot];
     return IPG_OK;
 }
 

@@ -22,7 +22,8 @@ PENDING, RUNNING, FINISHING, DONE = 0, 1, 2, 3
 
 class _Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "lanes_admitted", "supersteps", "kernel_launches",
-                                                 "groups_created", "groups_freed", "bytes_in_use", "peak_bytes")]
+                                                 "groups_created", "groups_freed", "bytes_in_use", "peak_bytes",
+                                                 "pull_supersteps")]
 
 
 def _lib():
@@ -42,7 +43,7 @@ def _lib():
         L.ipg_server_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
         L.ipg_server_run_trace.argtypes = [vp, u64, vp, vp, vp, vp, i32, vp, vp, ctypes.POINTER(dbl)]
         L.ipg_server_group_stats.argtypes = [vp, i32, i32, ctypes.POINTER(dbl), ctypes.POINTER(u64),
-                                             ctypes.POINTER(u64)]
+                                             ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L._serve_typed = True
     return L
 
@@ -139,16 +140,17 @@ class Server:
         return {n: getattr(s, n) for n, _ in _Stats._fields_}
 
     def group_stats(self) -> list:
-        """[(gid, "minplus"|"ppr", busy seconds, supersteps, lanes)] of the
-        groups that ran (busy times of concurrent groups overlap)."""
+        """[(gid, "minplus"|"ppr", busy seconds, supersteps, lanes,
+        lane-edge relaxations)] of the groups that ran (busy times of
+        concurrent groups overlap; relaxations are counted for min-plus)."""
         out = []
         for gid in range(len(self.graphs)):
             for gk, name in ((0, "minplus"), (1, "ppr")):
-                b, s, n = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+                b, s, n, w = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
                 _check(_lib().ipg_server_group_stats(self._p, gid, gk, ctypes.byref(b), ctypes.byref(s),
-                                                     ctypes.byref(n)), where="ipg_server_group_stats")
+                                                     ctypes.byref(n), ctypes.byref(w)), where="ipg_server_group_stats")
                 if s.value:
-                    out.append((gid, name, b.value, s.value, n.value))
+                    out.append((gid, name, b.value, s.value, n.value, w.value))
         return out
 
     def run_trace(self, trace: Trace, keep_results=False):

@@ -203,6 +203,33 @@ def test_cc_union_find_with_hubs():
         d.free()
 
 
+def test_sssp_pull_supersteps_match_push_and_dijkstra():
+    """On a graph declared symmetric, dense min-plus supersteps pull (no
+    atomics); every distance equals Dijkstra's and the push-only run's."""
+    import ipregel_b200 as ip
+    from ipregel_b200 import serve as S
+    g = O.add_weights(O.gen_rmat(14, 16, seed=11, undirected=True), wmax=255, seed=11)
+    srcs = [int(s) for s in np.random.default_rng(3).choice(np.flatnonzero(np.diff(g.idx) > 0), 40, replace=False)]
+    results = {}
+    for symmetric in (True, False):
+        d = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, wgt=g.wgt)
+        d.set_symmetric(symmetric)
+        srv = S.Server()
+        try:
+            gid = srv.add_graph(d)
+            ids = [srv.submit(gid, S.SSSP, s) for s in srcs]
+            srv.drain()
+            results[symmetric] = [srv.result(q, S.SSSP, g.V) for q in ids]
+            pulls = srv.stats()["pull_supersteps"]
+            assert (pulls > 0) if symmetric else (pulls == 0)
+        finally:
+            srv.free()
+            d.free()
+    for s, a, b in zip(srcs, results[True], results[False]):
+        np.testing.assert_array_equal(a, O.dijkstra(g, s))
+        np.testing.assert_array_equal(a, b)
+
+
 def test_bad_requests_raise():
     import ipregel_b200 as ip
     from ipregel_b200 import serve as S
