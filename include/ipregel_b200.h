@@ -303,6 +303,12 @@ void ipg_server_free(ipg_server* srv);
 /* The graph stays owned by the caller and must outlive the server.  Builds
  * the graph's degree classes, which synchronises the device. */
 int ipg_server_add_graph(ipg_server* srv, ipg_graph* g, int* gid);
+/* Allocates and clears, now, the lane group that queries of `kind` on graph
+ * gid run in (no-op when it exists), so that
+ * their first arrivals find the device state resident; the group counts
+ * against the HBM budget (IPG_EBUDGET when it does not fit) and, when idle,
+ * may be evicted like any other.  Synchronous. */
+int ipg_server_reserve(ipg_server* srv, int gid, int kind);
 int ipg_server_submit(ipg_server* srv, int gid, int kind, uint64_t source, uint64_t* qid);
 /* One scheduling pass: completed supersteps retire lanes, pending queries
  * take free lanes, next supersteps are launched.  Non-blocking.

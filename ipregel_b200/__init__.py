@@ -47,6 +47,7 @@ RUNTIME_SYMBOLS = (
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
     "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats", "ipg_measure_gather",
+    "ipg_server_reserve",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.

@@ -1222,6 +1222,12 @@ int galloc(Group* G, T** p, uint64_t n)
 struct ipg_server {
     uint64_t budget = 0;
     uint64_t in_use = 0;
+    // result buffers come from a stream-ordered pool that keeps freed memory
+    // (release threshold unbounded): a query's result is allocated at
+    // admission and freed at release without a cudaMalloc / cudaFree, each of
+    // which costs about a millisecond and stalls the scheduling loop
+    cudaMemPool_t rpool = nullptr;
+    cudaStream_t rel_st = nullptr;  // stream of the frees (results released are complete)
     uint32_t rounds = 20;
     std::vector<std::unique_ptr<Graph>> graphs;
     std::vector<Group*> groups;
@@ -1233,7 +1239,6 @@ struct ipg_server {
     std::vector<double> busy_s;                 // per graph and group kind: superstep device time
     std::vector<uint64_t> steps, lanes;         // supersteps, lanes admitted
     std::vector<uint64_t> work;                 // min-plus lane-edge relaxations examined
-    std::multimap<uint64_t, void*> pool;        // released result buffers by size
     uint64_t next_id = 1;
     // near-far bucket width of SSSP lanes (IPG_SERVE_DELTA); on R-MAT graphs
     // with weights in [1, 255], 256..1024 measured best, 7 % faster than none
@@ -1281,13 +1286,6 @@ bool make_room(ipg_server* S, uint64_t need)
             if (!G->busy && !G->running && (!victim || G->last_used < victim->last_used)) victim = G;
         if (victim) {
             free_group(S, victim);
-            continue;
-        }
-        if (!S->pool.empty()) {
-            auto it = S->pool.begin();
-            ipg_dev_free(it->second, it->first);
-            S->in_use -= it->first;
-            S->pool.erase(it);
             continue;
         }
         return false;
@@ -1429,25 +1427,27 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
     return IPG_OK;
 }
 
-int take_result(ipg_server* S, Query& q, uint64_t bytes)
+int take_result(ipg_server* S, Query& q, uint64_t bytes, cudaStream_t st)
 {
-    auto it = S->pool.find(bytes);
-    if (it != S->pool.end()) {
-        q.result = it->second;
-        S->pool.erase(it);
-    } else {
-        if (!make_room(S, bytes)) return IPG_EBUDGET;
-        int r = ipg_dev_alloc(&q.result, bytes);
-        if (r != IPG_OK) return r;
-        S->in_use += bytes;
+    if (!make_room(S, bytes)) return IPG_EBUDGET;
+    if (cudaMallocFromPoolAsync(&q.result, bytes, S->rpool, st) != cudaSuccess) {
+        cudaGetLastError();
+        q.result = nullptr;
+        return IPG_ENOMEM;  // the query waits for memory
     }
+    S->in_use += bytes;
     q.result_bytes = bytes;
     return IPG_OK;
 }
 
-void release_result(ipg_server* S, Query& q)
+// st: a stream ordered after the allocation (the admitting group's stream,
+// or any stream once the query is done)
+void release_result(ipg_server* S, Query& q, cudaStream_t st = nullptr)
 {
-    if (q.result) S->pool.insert({q.result_bytes, q.result});
+    if (q.result) {
+        cudaFreeAsync(q.result, st ? st : S->rel_st);
+        S->in_use -= q.result_bytes;
+    }
     q.result = nullptr;
 }
 
@@ -1475,7 +1475,7 @@ void admit(ipg_server* S, Group* G, double now)
         const bool joins_cc = q.kind == IPG_QUERY_CC && G->cc_lane >= 0;
         if (!union_find && !joins_cc && (G->busy & full) == full) break;  // no lane free
         const uint64_t rbytes = V * 4;
-        if (take_result(S, q, rbytes) != IPG_OK) {
+        if (take_result(S, q, rbytes, G->st) != IPG_OK) {
             ++it;
             continue;
         }
@@ -1485,7 +1485,7 @@ void admit(ipg_server* S, Group* G, double now)
             // CC queries admitted together share one union-find pass
             if (!cc_first) {
                 if (graph_classes(G->G, G->st) != IPG_OK) {
-                    release_result(S, q);
+                    release_result(S, q, G->st);
                     q.state = IPG_QUERY_PENDING;
                     ++it;
                     continue;
@@ -1725,6 +1725,21 @@ extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_s
     if (!S) return ipg_internal_fail(IPG_ENOMEM, "ipg_server_create: out of host memory");
     S->budget = hbm_budget;
     S->rounds = ppr_rounds;
+    int dev = 0;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    cudaError_t e = cudaGetDevice(&dev);
+    props.location.id = dev;
+    if (e == cudaSuccess) e = cudaMemPoolCreate(&S->rpool, &props);
+    uint64_t keep = UINT64_MAX;
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(S->rpool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->rel_st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        if (S->rpool) cudaMemPoolDestroy(S->rpool);
+        delete S;
+        return ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+    }
     if (const char* d = getenv("IPG_SERVE_DELTA"))
         if (*d) S->delta = (uint32_t)std::max(1UL, strtoul(d, nullptr, 10));
     if (const char* p = getenv("IPG_SERVE_PULL"))
@@ -1742,9 +1757,11 @@ extern "C" void ipg_server_free(ipg_server* S)
             cudaEventSynchronize(kv.second.ready);
             cudaEventDestroy(kv.second.ready);
         }
-        if (kv.second.result) ipg_dev_free(kv.second.result, kv.second.result_bytes);
+        if (kv.second.result) cudaFreeAsync(kv.second.result, S->rel_st);
     }
-    for (auto& kv : S->pool) ipg_dev_free(kv.second, kv.first);
+    cudaStreamSynchronize(S->rel_st);
+    cudaStreamDestroy(S->rel_st);
+    cudaMemPoolDestroy(S->rpool);
     for (auto& g : S->graphs)
         if (g->hub_prefix) ipg_dev_free(g->hub_prefix, (g->bins.count[2] + 5) * 4);
     delete S;
@@ -1776,6 +1793,30 @@ extern "C" int ipg_server_add_graph(ipg_server* S, ipg_graph* g, int* gid)
     S->steps.resize(S->graphs.size() * 2, 0);
     S->lanes.resize(S->graphs.size() * 2, 0);
     S->work.resize(S->graphs.size() * 2, 0);
+    return IPG_OK;
+}
+
+extern "C" int ipg_server_reserve(ipg_server* S, int gid, int kind)
+{
+    if (!S) return ipg_internal_fail(IPG_EINVAL, "ipg_server_reserve: null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (gid < 0 || gid >= (int)S->graphs.size()) return ipg_internal_fail(IPG_EINVAL, "ipg_server_reserve: no such graph");
+    if (kind != IPG_QUERY_SSSP && kind != IPG_QUERY_PPR && kind != IPG_QUERY_CC)
+        return ipg_internal_fail(IPG_EINVAL, "ipg_server_reserve: unknown query kind");
+    Graph* Gr = S->graphs[gid].get();
+    // SSSP and CC queries run in the graph's min-plus group (union-find CC on
+    // its stream), PPR queries in its PPR group
+    const int gk = kind == IPG_QUERY_PPR ? 1 : 0;
+    if (gk ? Gr->pp : Gr->mp) return IPG_OK;
+    int r = create_group(S, Gr, gk);
+    if (r == IPG_ENOMEM) {
+        cudaMemPoolTrimTo(S->rpool, 0);
+        r = create_group(S, Gr, gk);
+    }
+    if (r == IPG_EBUDGET) return ipg_internal_fail(IPG_EBUDGET, "ipg_server_reserve: the group does not fit the budget");
+    if (r != IPG_OK) return r;
+    Group* G = gk ? Gr->pp : Gr->mp;
+    if (cudaStreamSynchronize(G->st) != cudaSuccess) return ipg_internal_fail(IPG_ECUDA, "ipg_server_reserve: failed");
     return IPG_OK;
 }
 
@@ -1839,6 +1880,11 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
         const int kind = (int)(i % 2);
         if (!(kind ? Gr->pp : Gr->mp)) {
             int r = create_group(S, Gr, kind);
+            if (r == IPG_ENOMEM) {
+                // memory the result pool keeps but does not use goes back first
+                cudaMemPoolTrimTo(S->rpool, 0);
+                r = create_group(S, Gr, kind);
+            }
             if (r != IPG_OK && r != IPG_EBUDGET && r != IPG_ENOMEM) return r;
         }
     }

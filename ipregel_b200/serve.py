@@ -35,6 +35,7 @@ def _lib():
         L.ipg_server_free.restype = None
         L.ipg_server_add_graph.argtypes = [vp, vp, ctypes.POINTER(i32)]
         L.ipg_server_submit.argtypes = [vp, i32, i32, u64, ctypes.POINTER(u64)]
+        L.ipg_server_reserve.argtypes = [vp, i32, i32]
         L.ipg_server_poll.argtypes = [vp, ctypes.POINTER(u64)]
         L.ipg_server_query.argtypes = [vp, u64, ctypes.POINTER(i32), ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
         L.ipg_server_result.argtypes = [vp, u64, vp, u64]
@@ -104,6 +105,11 @@ class Server:
         _check(_lib().ipg_server_add_graph(self._p, g.handle, ctypes.byref(gid)), where="ipg_server_add_graph")
         self.graphs.append(g)
         return gid.value
+
+    def reserve(self, gid, kind):
+        """Allocates the lane group for queries of `kind` on graph gid now
+        (ipg_server_reserve)."""
+        _check(_lib().ipg_server_reserve(self._p, int(gid), int(kind)), where="ipg_server_reserve")
 
     def submit(self, gid, kind, source=0) -> int:
         q = ctypes.c_uint64()

@@ -230,6 +230,41 @@ def test_sssp_pull_supersteps_match_push_and_dijkstra():
         np.testing.assert_array_equal(a, b)
 
 
+def test_reserved_groups_serve_and_respect_budget():
+    """Groups reserved before the queries arrive are the ones the queries run
+    in; a reservation that does not fit the budget raises."""
+    import ipregel_b200 as ip
+    from ipregel_b200 import serve as S
+    gs = _graphs()
+    dg = _device(gs)
+    srv = S.Server()
+    try:
+        gids = [srv.add_graph(d) for d in dg]
+        for gid in gids:
+            srv.reserve(gid, S.SSSP)
+            srv.reserve(gid, S.PPR)
+            srv.reserve(gid, S.SSSP)  # already there: no second group
+        st = srv.stats()
+        assert st["groups_created"] == 2 * len(gids) and st["bytes_in_use"] > 0
+        qs = [(gid, kind, 3) for gid in gids for kind in (S.SSSP, S.PPR)]
+        ids = [srv.submit(*q) for q in qs]
+        srv.drain()
+        for qid, (gid, kind, src) in zip(ids, qs):
+            _check(gs[gid], kind, src, srv.result(qid, kind, gs[gid].V))
+        assert srv.stats()["groups_created"] == 2 * len(gids)
+    finally:
+        srv.free()
+    small = S.Server(hbm_budget=1 << 20)
+    try:
+        gid = small.add_graph(dg[2])
+        with pytest.raises(ip.IPregelError, match="budget"):
+            small.reserve(gid, S.PPR)
+    finally:
+        small.free()
+        for d in dg:
+            d.free()
+
+
 def test_bad_requests_raise():
     import ipregel_b200 as ip
     from ipregel_b200 import serve as S
