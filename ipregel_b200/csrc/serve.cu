@@ -1275,8 +1275,8 @@ uint64_t group_bytes(const Graph* G, int kind)
     return V * (PP_K * 4 * 2 + 4) + (E / HUB_CHUNK + V / MP_T1 + 2) * (PP_K * 8) + 4096;
 }
 
-// Frees idle groups (least recently used first), then cached result buffers,
-// until `need` more bytes fit the budget.
+// Frees idle groups (least recently used first) until `need` more bytes fit
+// the budget.
 bool make_room(ipg_server* S, uint64_t need)
 {
     if (!S->budget) return true;
@@ -1427,16 +1427,26 @@ int create_group(ipg_server* S, Graph* Gr, int kind)
     return IPG_OK;
 }
 
-int take_result(ipg_server* S, Query& q, uint64_t bytes, cudaStream_t st)
+// A query's result buffer is counted against the budget when the query is
+// admitted (reserve_result) and allocated when it is first written
+// (alloc_result): at admission for union-find CC and PPR, at extraction for
+// min-plus lanes, whose distance column holds the result until then.
+int reserve_result(ipg_server* S, Query& q, uint64_t bytes)
 {
     if (!make_room(S, bytes)) return IPG_EBUDGET;
-    if (cudaMallocFromPoolAsync(&q.result, bytes, S->rpool, st) != cudaSuccess) {
-        cudaGetLastError();
-        q.result = nullptr;
-        return IPG_ENOMEM;  // the query waits for memory
-    }
     S->in_use += bytes;
     q.result_bytes = bytes;
+    return IPG_OK;
+}
+
+int alloc_result(ipg_server* S, Query& q, cudaStream_t st)
+{
+    if (q.result) return IPG_OK;
+    if (cudaMallocFromPoolAsync(&q.result, q.result_bytes, S->rpool, st) != cudaSuccess) {
+        cudaGetLastError();
+        q.result = nullptr;
+        return IPG_ENOMEM;  // the caller tries again later
+    }
     return IPG_OK;
 }
 
@@ -1444,10 +1454,9 @@ int take_result(ipg_server* S, Query& q, uint64_t bytes, cudaStream_t st)
 // or any stream once the query is done)
 void release_result(ipg_server* S, Query& q, cudaStream_t st = nullptr)
 {
-    if (q.result) {
-        cudaFreeAsync(q.result, st ? st : S->rel_st);
-        S->in_use -= q.result_bytes;
-    }
+    if (q.result) cudaFreeAsync(q.result, st ? st : S->rel_st);
+    S->in_use -= q.result_bytes;
+    q.result_bytes = 0;
     q.result = nullptr;
 }
 
@@ -1475,7 +1484,16 @@ void admit(ipg_server* S, Group* G, double now)
         const bool joins_cc = q.kind == IPG_QUERY_CC && G->cc_lane >= 0;
         if (!union_find && !joins_cc && (G->busy & full) == full) break;  // no lane free
         const uint64_t rbytes = V * 4;
-        if (take_result(S, q, rbytes, G->st) != IPG_OK) {
+        // a union-find CC result is written now and a PPR lane's by its last
+        // gather, so they allocate their buffers at admission; a min-plus
+        // lane's result is allocated when the lane is extracted (its column
+        // holds it until then), so running lanes hold no result memory
+        if (reserve_result(S, q, rbytes) != IPG_OK) {
+            ++it;
+            continue;
+        }
+        if ((union_find || G->kind == 1) && alloc_result(S, q, G->st) != IPG_OK) {
+            release_result(S, q, G->st);
             ++it;
             continue;
         }
@@ -1682,8 +1700,18 @@ void retire(ipg_server* S, Group* G, double now)
                 const uint64_t base = st.far_min[k] != SRV_INF ? st.far_min[k] : G->thr_h[k];
                 G->thr_h[k] = (uint32_t)std::min<uint64_t>(base + S->delta, SRV_INF);
             }
+        uint64_t extracted = 0;
         for (int k = 0; k < MP_K; k++) {
             if (!((done >> k) & 1)) continue;
+            // every query on the lane needs its buffer; a lane whose buffers
+            // do not fit yet stays busy (its frontier is empty, so its
+            // supersteps do nothing) and is tried again after the next one
+            bool ok = true;
+            for (uint64_t qid : G->lane_q[k]) {
+                Query& q = S->queries[qid];
+                if (alloc_result(S, q, G->st) != IPG_OK) ok = false;
+            }
+            if (!ok) continue;
             const void* first = nullptr;
             for (uint64_t qid : G->lane_q[k]) {
                 Query& q = S->queries[qid];
@@ -1698,8 +1726,9 @@ void retire(ipg_server* S, Group* G, double now)
             }
             G->lane_q[k].clear();
             if (G->cc_lane == k) G->cc_lane = -1;
+            extracted |= 1ULL << k;
         }
-        G->busy &= ~done;
+        G->busy &= ~extracted;
     } else {
         for (int k = 0; k < PP_K; k++) {
             if (!((G->busy >> k) & 1)) continue;
