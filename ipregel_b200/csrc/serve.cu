@@ -25,7 +25,9 @@
 //     128 bytes per vertex, one line) double-buffered; a pull gather over
 //     every row: 8 threads per low-degree vertex, each reading one float4
 //     quad of every in-neighbour's row, a warp per vertex of higher degree
-//     (four rows per load instruction), hub rows in chunks.  A lane runs exactly
+//     (four rows per load instruction), hub rows in chunks.  64 lanes (two
+//     lines per row) measured slower in the mixed serving workload: a
+//     superstep cost about twice as much, for half the supersteps.  A lane runs exactly
 //     `rounds` gathers after admission and writes its last values into the
 //     query's result buffer.
 //
@@ -64,7 +66,7 @@ constexpr int MP_K = 64;
 constexpr int PP_K = 32;           // PPR lanes: a row of 32 FP32 quotients is one 128-byte line
 constexpr int PP_Q = PP_K / 4;     // float4 quads per row
 constexpr int PP_SLOTS = 32 / PP_Q;  // rows per warp load instruction
-static_assert(PP_K <= 32 && PP_Q <= 16 && PP_K % 16 == 0, "PPR lanes: a warp covers whole rows");
+static_assert(PP_K <= 64 && PP_Q <= 16 && PP_K % 16 == 0, "PPR lanes: a warp covers whole rows");
 constexpr int SRV_THREADS = 256;
 constexpr uint64_t MP_T0 = 8, MP_T1 = 4096;
 constexpr uint64_t PP_T0 = 64;                      // PPR: quads up to this degree, then warps
@@ -889,7 +891,7 @@ __global__ void k_cc_compress(uint32_t* p, uint64_t V)
 struct PpLanes {
     float* out[PP_K];       // result buffer of a lane in its last gather, else null
     uint32_t seed[PP_K];
-    uint32_t active;        // lanes gathering this superstep
+    unsigned long long active;  // lanes gathering this superstep
 };
 
 struct PpArgs {
@@ -966,7 +968,7 @@ __device__ __forceinline__ void pp_finish_quad(const PpArgs& a, const PpLanes& L
     for (int j = 0; j < 4; j++) {
         const int k = 4 * q + j;
         bn[j] = 0.0f;
-        if ((L.active >> k) & 1u) {
+        if ((L.active >> k) & 1ULL) {
             const float xn = pp_value(L, k, v, __fadd_rn(s[j], c[j]));
             if (L.out[k]) L.out[k][v] = xn;
             else if (deg) bn[j] = __fdiv_rn(xn, (float)deg);
@@ -1026,7 +1028,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, co
 {
     const int lane = threadIdx.x & 31, q = lane % PP_Q, gb = lane - q;
     const unsigned gmask = ((1u << PP_Q) - 1u) << gb;
-    const bool quad_on = (L.active >> (4 * q)) & 0xFu;
+    const bool quad_on = (L.active >> (4 * q)) & 0xFULL;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint64_t groups = ((uint64_t)gridDim.x * blockDim.x) / PP_Q;
     // the threads of a group share i, so they leave the loop together
@@ -1056,7 +1058,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_vertices(PpArgs a, PpLanes L
                                                              uint64_t n)
 {
     const int lane = threadIdx.x & 31;
-    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFu;
+    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFULL;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
@@ -1073,7 +1075,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_chunks(PpArgs a, PpLanes
 {
     if (!n) return;
     const int lane = threadIdx.x & 31;
-    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFu;
+    const bool quad_on = (L.active >> (4 * (lane % PP_Q))) & 0xFULL;
     const uint32_t chunks = prefix[n];
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; c < chunks; c += warps) {
@@ -1099,13 +1101,14 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_hub_finish(PpArgs a, PpLanes
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint64_t v = list[i];
-        float s = 0.0f, c = 0.0f;
-        if (lane < PP_K)
+        for (int k = lane; k < PP_K; k += 32) {
+            float s = 0.0f, c = 0.0f;
             for (uint32_t ch = prefix[i]; ch < prefix[i + 1]; ch++) {
-                const float2 p = a.partial[(uint64_t)ch * PP_K + lane];
+                const float2 p = a.partial[(uint64_t)ch * PP_K + k];
                 pp_merge(s, c, p.x, p.y);
             }
-        if (lane < PP_K) sh[w][lane] = make_float2(s, c);
+            sh[w][k] = make_float2(s, c);
+        }
         __syncwarp();
         if (lane < PP_Q) {
             float s4[4], c4[4];
@@ -1484,15 +1487,15 @@ void admit(ipg_server* S, Group* G, double now)
         const bool joins_cc = q.kind == IPG_QUERY_CC && G->cc_lane >= 0;
         if (!union_find && !joins_cc && (G->busy & full) == full) break;  // no lane free
         const uint64_t rbytes = V * 4;
-        // a union-find CC result is written now and a PPR lane's by its last
-        // gather, so they allocate their buffers at admission; a min-plus
-        // lane's result is allocated when the lane is extracted (its column
-        // holds it until then), so running lanes hold no result memory
+        // a union-find CC result is written now, so it is allocated at
+        // admission; a PPR lane's is allocated before its last gather and a
+        // min-plus lane's when the lane is extracted (its column holds it
+        // until then), so running lanes hold no result memory
         if (reserve_result(S, q, rbytes) != IPG_OK) {
             ++it;
             continue;
         }
-        if ((union_find || G->kind == 1) && alloc_result(S, q, G->st) != IPG_OK) {
+        if (union_find && alloc_result(S, q, G->st) != IPG_OK) {
             release_result(S, q, G->st);
             ++it;
             continue;
@@ -1646,12 +1649,17 @@ int launch_superstep(ipg_server* S, Group* G)
         a.b_next = G->b[G->cur ^ 1];
         a.partial = G->partial;
         PpLanes L;
-        L.active = (uint32_t)G->busy;
+        L.active = G->busy;
         for (int k = 0; k < PP_K; k++) {
             L.seed[k] = G->seed[k];
             L.out[k] = nullptr;
-            if (((G->busy >> k) & 1) && G->it[k] + 1 == (int)S->rounds)
-                L.out[k] = (float*)S->queries[G->lane_q[k][0]].result;
+            if (((G->busy >> k) & 1) && G->it[k] + 1 == (int)S->rounds) {
+                // a lane's result buffer is allocated for its last gather; if
+                // the memory is not there yet the superstep waits
+                Query& q = S->queries[G->lane_q[k][0]];
+                if (alloc_result(S, q, G->st) != IPG_OK) return IPG_ENOMEM;
+                L.out[k] = (float*)q.result;
+            }
         }
         const ipg_bins& B = Gr->bins;
         const uint32_t* l0 = G->pp_list ? G->pp_list : B.d_list[0];
@@ -1934,7 +1942,7 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
         admit(S, G, now);
         if (G->busy) {
             int r = launch_superstep(S, G);
-            if (r != IPG_OK) return r;
+            if (r != IPG_OK && r != IPG_ENOMEM) return r;  // ENOMEM: launched at a later poll
         }
     }
     uint64_t n = S->n_pending + S->finishing.size();

@@ -127,6 +127,30 @@ def test_more_queries_than_lanes():
         d.free()
 
 
+def test_more_ppr_queries_than_lanes():
+    """70 PPR queries on one graph: every lane of the group in use at once,
+    lanes reused as queries finish; each within the FP32 tolerance of the
+    FP64 oracle and bitwise the same as alone."""
+    from ipregel_b200 import serve as S
+    g = O.add_weights(O.gen_rmat(11, 16, seed=8, undirected=True), wmax=255, seed=8)
+    (d,) = _device([g])
+    srv = S.Server(ppr_rounds=20)
+    try:
+        gid = srv.add_graph(d)
+        srcs = [int(s) for s in np.random.default_rng(4).integers(0, g.V, size=70)]
+        ids = [srv.submit(gid, S.PPR, s) for s in srcs]
+        srv.drain()
+        got = [srv.result(q, S.PPR, g.V) for q in ids]
+        for s, r in zip(srcs, got):
+            _check(g, S.PPR, s, r)
+        for s, r in list(zip(srcs, got))[::23]:
+            alone, _ = S.run_alone(srv, gid, S.PPR, s, g.V)
+            np.testing.assert_array_equal(alone.view(np.uint32), r.view(np.uint32))
+    finally:
+        srv.free()
+        d.free()
+
+
 def test_tight_hbm_budget_evicts_idle_groups():
     from ipregel_b200 import serve as S
     gs = _graphs()
