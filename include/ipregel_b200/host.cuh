@@ -59,6 +59,11 @@ struct ipx_host_state {
     ipg_graph_view gv;
     ipx_consts c;
     std::vector<std::pair<void*, uint64_t>> allocs;
+    /* device buffers of the previous attachment, kept through a re-attach:
+     * ipx_alloc takes one of exactly the size it needs before allocating,
+     * so re-attaching a graph of the same shape allocates and frees nothing
+     * (cudaFree synchronises the whole device) */
+    std::vector<std::pair<void*, uint64_t>> spare;
     uint32_t* blist[3] = {nullptr, nullptr, nullptr};  /* broadcaster classes */
     uint32_t* tlist[3] = {nullptr, nullptr, nullptr};  /* frontier / target classes */
     uint32_t* lcnt = nullptr;                          /* [0..2] broadcaster, [4..6] targets */
@@ -141,7 +146,14 @@ static int ipx_alloc(T** p, uint64_t n)
 {
     void* d = nullptr;
     uint64_t bytes = (n ? n : 1) * sizeof(T);
-    int r = ipg_dev_alloc(&d, bytes);
+    for (size_t i = 0; i < ipx_h.spare.size(); i++)
+        if (ipx_h.spare[i].second == bytes) {
+            d = ipx_h.spare[i].first;
+            ipx_h.spare[i] = ipx_h.spare.back();
+            ipx_h.spare.pop_back();
+            break;
+        }
+    int r = d ? IPG_OK : ipg_dev_alloc(&d, bytes);
     if (r != IPG_OK) {
         snprintf(ipx_h.err, sizeof ipx_h.err, "%s", ipg_last_error());
         return r;
@@ -151,9 +163,22 @@ static int ipx_alloc(T** p, uint64_t n)
     return IPG_OK;
 }
 
-static void ipx_release_state()
+static void ipx_free_spares()
 {
-    for (auto& a : ipx_h.allocs) ipg_dev_free(a.first, a.second);
+    for (auto& a : ipx_h.spare) ipg_dev_free(a.first, a.second);
+    ipx_h.spare.clear();
+}
+
+/* keep = true (a re-attach): the device buffers become spares for the next
+ * setup instead of being freed. */
+static void ipx_release_state(bool keep = false)
+{
+    if (keep) {
+        ipx_h.spare.insert(ipx_h.spare.end(), ipx_h.allocs.begin(), ipx_h.allocs.end());
+    } else {
+        for (auto& a : ipx_h.allocs) ipg_dev_free(a.first, a.second);
+        ipx_free_spares();
+    }
     ipx_h.allocs.clear();
     if (ipx_h.gexec) cudaGraphExecDestroy(ipx_h.gexec);
     ipx_h.gexec = nullptr;
@@ -368,7 +393,7 @@ static int ipx_setup_state()
 
 static int ipx_attach(ipg_graph* g, bool own)
 {
-    ipx_release_state();
+    ipx_release_state(true);
     ipx_h.err[0] = 0;
     ipx_h.g = g;
     ipx_h.own_graph = own;
@@ -387,6 +412,7 @@ static int ipx_attach(ipg_graph* g, bool own)
     ip_set_vertices_count(ipx_h.gv.V);
     ip_set_edges_count(ipx_h.gv.E);
     int r = ipx_setup_state();
+    ipx_free_spares(); /* the previous attachment's buffers this one did not take */
     if (r != IPG_OK) {
         ipx_h.own_graph = own;
         ipx_release_state();

@@ -47,7 +47,7 @@ RUNTIME_SYMBOLS = (
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
     "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats", "ipg_measure_gather",
-    "ipg_server_reserve",
+    "ipg_server_reserve", "ipg_graph_refill_host",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -99,6 +99,7 @@ def runtime():
         vp, u64, i32, dbl = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
         L.ipg_graph_from_host.argtypes = [u64, u64, vp, i32, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_from_device.argtypes = [u64, u64, vp, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
+        L.ipg_graph_refill_host.argtypes = [vp, vp, i32, vp, vp]
         L.ipg_graph_load.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, i32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_generate_rmat.argtypes = [ctypes.c_uint32, ctypes.c_uint32, dbl, dbl, dbl, u64, i32,
                                               ctypes.c_uint32, i32, ctypes.POINTER(vp)]
@@ -282,6 +283,23 @@ class Graph:
                                            ctypes.byref(h))
         _check(rc, where="ipg_graph_from_host")
         return cls(h.value)
+
+    def refill(self, idx, adj, wgt=None):
+        """New contents of the same size from host buffers, into this graph's
+        device buffers (ipg_graph_refill_host): nothing is allocated.  The
+        symmetric declaration and other derived data are dropped."""
+        V, E = int(self.view.V), int(self.view.E)
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        adj = np.ascontiguousarray(adj, dtype=np.uint32 if int(self.view.id_bytes) == 4 else np.uint64)
+        if idx.size != V or adj.size != E:
+            raise ValueError(f"refill: expected {V} row starts and {E} ids, got {idx.size} and {adj.size}")
+        if wgt is not None:
+            wgt = np.ascontiguousarray(wgt, dtype=np.uint32)
+        _check(runtime().ipg_graph_refill_host(self._h, idx.ctypes.data if V else None, 8,
+                                               adj.ctypes.data if E else None,
+                                               wgt.ctypes.data if (wgt is not None and E) else None),
+               where="ipg_graph_refill_host")
+        self.refresh()
 
     @classmethod
     def generate_rmat(cls, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, undirected=False, wmax=0,

@@ -552,6 +552,43 @@ extern "C" int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int 
     return finalize(g, need_in, out);
 }
 
+extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_bytes, const void* adj, const void* wgt)
+{
+    if (!g) return fail(IPG_EINVAL, "ipg_graph_refill_host: null graph");
+    if (!g->owns_out) return fail(IPG_EINVAL, "ipg_graph_refill_host: the graph wraps buffers it does not own");
+    const uint64_t V = g->v.V, E = g->v.E;
+    if ((V && !idx) || (E && !adj) || (E && g->v.weight_bytes && !wgt))
+        return fail(IPG_EINVAL, "ipg_graph_refill_host: null buffer");
+    // derived data of the old contents
+    for (auto& b : g->bins) {
+        ipg_dev_free(b.lists, b.bytes);
+        b = ipg_graph::BinCache();
+    }
+    g->v.symmetric = 0;
+    const bool own_in = g->in_row != nullptr;
+    if (own_in) {
+        g->v.device_bytes -= g->in_row_bytes + g->in_adj_bytes + g->in_wgt_bytes;
+        ipg_dev_free(g->in_row, g->in_row_bytes);
+        ipg_dev_free(g->in_adj, g->in_adj_bytes);
+        ipg_dev_free(g->in_wgt, g->in_wgt_bytes);
+        g->in_row = g->in_adj = g->in_wgt = nullptr;
+        g->in_row_bytes = g->in_adj_bytes = g->in_wgt_bytes = 0;
+        g->v.has_in = 0;
+        g->v.d_in_row = nullptr;
+        g->v.d_in_adj = nullptr;
+        g->v.d_in_wgt = nullptr;
+    }
+    IPG_TRY(upload_idx(g, idx, idx_bytes, true, 0));
+    if (E) {
+        IPG_CUDA(cudaMemcpy(g->adj, adj, E * (uint64_t)g->v.id_bytes, cudaMemcpyHostToDevice));
+        if (g->v.weight_bytes)
+            IPG_CUDA(cudaMemcpy(g->wgt, wgt, E * (uint64_t)g->v.weight_bytes, cudaMemcpyHostToDevice));
+    }
+    IPG_TRY(validate_graph(g, 0));
+    if (own_in) IPG_TRY(ipg_graph_build_in(g));
+    return finish_graph_stats(g, 0);
+}
+
 extern "C" int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_row, const void* d_adj, int id_bytes,
                                      const void* d_wgt, int weight_bytes, int directed, int need_in, ipg_graph** out)
 {

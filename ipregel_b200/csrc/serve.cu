@@ -94,6 +94,11 @@ double now_s()
 // Shared helpers
 // ---------------------------------------------------------------------------
 
+// Neighbour ids and weights a superstep reads once per edge: loaded
+// evict-first (ld.global.cs), so the gigabytes of edge stream leave the L2 to
+// the lane rows that edges read at random.
+__device__ __forceinline__ uint32_t ld_edge(const uint32_t* p) { return __ldcs(p); }
+
 // Status of a min-plus group after a superstep, copied to the host in one
 // transfer: lane flags, list sizes, hub chunks of list 2, least deferred
 // distance of each lane.
@@ -252,8 +257,8 @@ __device__ __forceinline__ void mp_edges_sparse(const MpArgs& a, uint64_t e0, ui
                                                 MpAcc& acc)
 {
     for (uint64_t e = e0 + lane; e < e1; e += stride) {
-        const uint32_t u = a.adj[e];
-        const uint32_t t = a.wgt ? a.wgt[e] : 0u;
+        const uint32_t u = ld_edge(&a.adj[e]);
+        const uint32_t t = a.wgt ? ld_edge(&a.wgt[e]) : 0u;
         acc.work += (unsigned)m;
         const unsigned long long bits = mp_relax_edge<L>(a, u, t, m, ks, ds);
         if (bits) {
@@ -331,8 +336,8 @@ __device__ __forceinline__ void mp_relax(const MpArgs& a, uint64_t v, uint64_t e
     const bool w0 = ((uint32_t)a.wmask >> lane) & 1u, w1 = ((uint32_t)(a.wmask >> 32) >> lane) & 1u;
     for (uint64_t e = e0; e < e1; e += 32) {
         const uint64_t ee = e + lane;
-        const uint32_t wj = ee < e1 ? a.adj[ee] : 0u;
-        const uint32_t tj = (ee < e1 && a.wgt) ? a.wgt[ee] : 0u;
+        const uint32_t wj = ee < e1 ? ld_edge(&a.adj[ee]) : 0u;
+        const uint32_t tj = (ee < e1 && a.wgt) ? ld_edge(&a.wgt[ee]) : 0u;
         const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
         for (int j0 = 0; j0 < nj; j0 += 4) {
             uint32_t u[4], t[4], c0[4], c1[4];
@@ -528,11 +533,11 @@ __device__ __forceinline__ void mp_pull_edges(const MpArgs& a, uint64_t e0, uint
     const bool live0 = (a.busy >> lane) & 1ULL, live1 = (a.busy >> (lane + 32)) & 1ULL;
     for (uint64_t e = e0; e < e1; e += 32) {
         const uint64_t ee = e + lane;
-        const uint32_t vj = ee < e1 ? a.adj[ee] : 0u;
+        const uint32_t vj = ee < e1 ? ld_edge(&a.adj[ee]) : 0u;
         const bool fr = ee < e1 && ((a.fcur[vj >> 5] >> (vj & 31)) & 1u);
         uint32_t fm = __ballot_sync(FULL, fr);
         if (!fm) continue;
-        const uint32_t tj = (fr && a.wgt) ? a.wgt[ee] : 0u;
+        const uint32_t tj = (fr && a.wgt) ? ld_edge(&a.wgt[ee]) : 0u;
         while (fm) {
             int j[4];
 #pragma unroll
@@ -974,7 +979,8 @@ __device__ __forceinline__ void pp_finish_quad(const PpArgs& a, const PpLanes& L
             else if (deg) bn[j] = __fdiv_rn(xn, (float)deg);
         }
     }
-    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
+    // evict-first: the writes would otherwise displace the rows this superstep reads at random
+    __stcs(reinterpret_cast<float4*>(a.b_next + v * PP_K) + q, make_float4(bn[0], bn[1], bn[2], bn[3]));
 }
 
 // A warp gathers [e0, e1): thread t takes lane quad t % PP_Q and edge slot
@@ -991,9 +997,9 @@ __device__ __forceinline__ void pp_gather_warp(const PpArgs& a, uint64_t e0, uin
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int i = 0; i < 4; i++) s[i] = c[i] = 0.0f;
-    uint32_t uj = (e0 + lane < e1) ? a.adj[e0 + lane] : 0u;
+    uint32_t uj = (e0 + lane < e1) ? ld_edge(&a.adj[e0 + lane]) : 0u;
     for (uint64_t e = e0; e < e1; e += 32) {
-        const uint32_t un = (e + 32 + lane < e1) ? a.adj[e + 32 + lane] : 0u;
+        const uint32_t un = (e + 32 + lane < e1) ? ld_edge(&a.adj[e + 32 + lane]) : 0u;
         const int nj = (int)((e1 - e) < 32 ? (e1 - e) : 32);
 #pragma unroll
         for (int h = 0; h < 32 / PP_SLOTS; h += 4) {
@@ -1039,7 +1045,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, co
 #pragma unroll
         for (int k = 0; k < 4; k++) s[k] = c[k] = 0.0f;
         for (uint64_t e = e0; e < e1; e += 4) {
-            const uint32_t uj = (q < 4 && e + q < e1) ? a.adj[e + q] : 0u;
+            const uint32_t uj = (q < 4 && e + q < e1) ? ld_edge(&a.adj[e + q]) : 0u;
             const int ne = (int)((e1 - e) < 4 ? (e1 - e) : 4);
             float4 x[4];
 #pragma unroll
