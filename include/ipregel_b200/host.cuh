@@ -182,15 +182,17 @@ static void ipx_release_state(bool keep = false)
     ipx_h.allocs.clear();
     if (ipx_h.gexec) cudaGraphExecDestroy(ipx_h.gexec);
     ipx_h.gexec = nullptr;
-    if (ipx_h.h_ctr) cudaFreeHost(ipx_h.h_ctr);
-    if (ipx_h.h_lcnt) cudaFreeHost(ipx_h.h_lcnt);
-    ipx_h.h_ctr = nullptr;
-    ipx_h.h_lcnt = nullptr;
-    if (ipx_h.ev0) cudaEventDestroy(ipx_h.ev0);
-    if (ipx_h.ev1) cudaEventDestroy(ipx_h.ev1);
-    if (ipx_h.st) cudaStreamDestroy(ipx_h.st);
-    ipx_h.ev0 = ipx_h.ev1 = nullptr;
-    ipx_h.st = nullptr;
+    if (!keep) { /* a re-attach keeps the stream, events and pinned words too */
+        if (ipx_h.h_ctr) cudaFreeHost(ipx_h.h_ctr);
+        if (ipx_h.h_lcnt) cudaFreeHost(ipx_h.h_lcnt);
+        ipx_h.h_ctr = nullptr;
+        ipx_h.h_lcnt = nullptr;
+        if (ipx_h.ev0) cudaEventDestroy(ipx_h.ev0);
+        if (ipx_h.ev1) cudaEventDestroy(ipx_h.ev1);
+        if (ipx_h.st) cudaStreamDestroy(ipx_h.st);
+        ipx_h.ev0 = ipx_h.ev1 = nullptr;
+        ipx_h.st = nullptr;
+    }
     if (ipx_h.g && ipx_h.own_graph) ipg_graph_free(ipx_h.g);
     ipx_h.g = nullptr;
     ipx_h.ready = false;
@@ -281,11 +283,12 @@ static int ipx_setup_state()
         return ipx_fail(IPG_EINVAL, "the application needs edge weights: load the graph with weighted = true");
     if (IPX_WEIGHT_BYTES && gv.weight_bytes != IPX_WEIGHT_BYTES)
         return ipx_fail(IPG_EINVAL, "graph weight width differs from IP_EDGE_WEIGHT_TYPE");
-    IPX_CU(cudaStreamCreateWithFlags(&ipx_h.st, cudaStreamNonBlocking));
-    IPX_CU(cudaEventCreate(&ipx_h.ev0));
-    IPX_CU(cudaEventCreate(&ipx_h.ev1));
-    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, IPX_NCTR * sizeof(unsigned long long), cudaHostAllocDefault));
-    IPX_CU(cudaHostAlloc((void**)&ipx_h.h_lcnt, 8 * sizeof(uint32_t), cudaHostAllocDefault));
+    if (!ipx_h.st) IPX_CU(cudaStreamCreateWithFlags(&ipx_h.st, cudaStreamNonBlocking));
+    if (!ipx_h.ev0) IPX_CU(cudaEventCreate(&ipx_h.ev0));
+    if (!ipx_h.ev1) IPX_CU(cudaEventCreate(&ipx_h.ev1));
+    if (!ipx_h.h_ctr)
+        IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, IPX_NCTR * sizeof(unsigned long long), cudaHostAllocDefault));
+    if (!ipx_h.h_lcnt) IPX_CU(cudaHostAlloc((void**)&ipx_h.h_lcnt, 8 * sizeof(uint32_t), cudaHostAllocDefault));
     IPX_OK(ipx_alloc(&c.value, V));
     IPX_OK(ipx_alloc(&c.ctr, IPX_NCTR));
     c.err = (uint32_t*)(c.ctr + IPX_CTR_ERR);

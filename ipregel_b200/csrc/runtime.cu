@@ -219,8 +219,19 @@ struct ipg_graph {
         uint64_t bytes = 0;
         ipg_bins bins;
     } bins[2];
+    // ipg_graph_refill_host's own stream, device words (check bits, degree
+    // maxima), pinned words and offset staging, made at its first call
+    cudaStream_t refill_st = nullptr;
+    void* refill_dev = nullptr;
+    uint64_t* refill_host = nullptr;
+    void* refill_stage = nullptr;
+    uint64_t refill_stage_bytes = 0;
     ~ipg_graph()
     {
+        ipg_dev_free(refill_dev, 64);
+        ipg_dev_free(refill_stage, refill_stage_bytes);
+        if (refill_host) cudaFreeHost(refill_host);
+        if (refill_st) cudaStreamDestroy(refill_st);
         if (owns_out) {
             ipg_dev_free(row, row_bytes);
             ipg_dev_free(adj, adj_bytes);
@@ -552,6 +563,10 @@ extern "C" int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int 
     return finalize(g, need_in, out);
 }
 
+// Everything on the graph's own non-blocking stream, synchronising only that
+// stream, with buffers made at the first call: a refill allocates nothing
+// and waits for no other work on the device, so it can run on one thread
+// while kernels of another graph run on another.
 extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_bytes, const void* adj, const void* wgt)
 {
     if (!g) return fail(IPG_EINVAL, "ipg_graph_refill_host: null graph");
@@ -559,6 +574,18 @@ extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_byte
     const uint64_t V = g->v.V, E = g->v.E;
     if ((V && !idx) || (E && !adj) || (E && g->v.weight_bytes && !wgt))
         return fail(IPG_EINVAL, "ipg_graph_refill_host: null buffer");
+    if (idx_bytes != 1 && idx_bytes != 2 && idx_bytes != 4 && idx_bytes != 8)
+        return fail(IPG_EINVAL, "unsupported offset width %d", idx_bytes);
+    if (!g->refill_st) IPG_CUDA(cudaStreamCreateWithFlags(&g->refill_st, cudaStreamNonBlocking));
+    if (!g->refill_dev) IPG_TRY(ipg_dev_alloc(&g->refill_dev, 64));
+    if (!g->refill_host) IPG_CUDA(cudaHostAlloc((void**)&g->refill_host, 64, cudaHostAllocDefault));
+    if (idx_bytes != 8 && g->refill_stage_bytes < V * (uint64_t)idx_bytes) {
+        ipg_dev_free(g->refill_stage, g->refill_stage_bytes);
+        g->refill_stage = nullptr;
+        g->refill_stage_bytes = 0;
+        IPG_TRY(ipg_dev_alloc(&g->refill_stage, V * (uint64_t)idx_bytes));
+        g->refill_stage_bytes = V * (uint64_t)idx_bytes;
+    }
     // derived data of the old contents
     for (auto& b : g->bins) {
         ipg_dev_free(b.lists, b.bytes);
@@ -578,15 +605,53 @@ extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_byte
         g->v.d_in_adj = nullptr;
         g->v.d_in_wgt = nullptr;
     }
-    IPG_TRY(upload_idx(g, idx, idx_bytes, true, 0));
-    if (E) {
-        IPG_CUDA(cudaMemcpy(g->adj, adj, E * (uint64_t)g->v.id_bytes, cudaMemcpyHostToDevice));
-        if (g->v.weight_bytes)
-            IPG_CUDA(cudaMemcpy(g->wgt, wgt, E * (uint64_t)g->v.weight_bytes, cudaMemcpyHostToDevice));
+    cudaStream_t st = g->refill_st;
+    uint64_t* row = (uint64_t*)g->row;
+    uint64_t* h = g->refill_host;  // [0] = E for row[V]; [1..3] read back
+    uint32_t* err = (uint32_t*)g->refill_dev;
+    unsigned long long* maxdeg = (unsigned long long*)((char*)g->refill_dev + 8);
+    h[0] = E;
+    if (V) {
+        if (idx_bytes == 8) {
+            IPG_CUDA(cudaMemcpyAsync(row, idx, V * 8, cudaMemcpyHostToDevice, st));
+        } else {
+            IPG_CUDA(cudaMemcpyAsync(g->refill_stage, idx, V * (uint64_t)idx_bytes, cudaMemcpyHostToDevice, st));
+            const void* src = g->refill_stage;
+            switch (idx_bytes) {
+            case 4: k_widen_idx<<<grid_for(V + 1, 256), 256, 0, st>>>((const uint32_t*)src, V, E, row); break;
+            case 2: k_widen_idx<<<grid_for(V + 1, 256), 256, 0, st>>>((const uint16_t*)src, V, E, row); break;
+            default: k_widen_idx<<<grid_for(V + 1, 256), 256, 0, st>>>((const uint8_t*)src, V, E, row); break;
+            }
+        }
     }
-    IPG_TRY(validate_graph(g, 0));
-    if (own_in) IPG_TRY(ipg_graph_build_in(g));
-    return finish_graph_stats(g, 0);
+    IPG_CUDA(cudaMemcpyAsync(row + V, &h[0], 8, cudaMemcpyHostToDevice, st));
+    if (E) {
+        IPG_CUDA(cudaMemcpyAsync(g->adj, adj, E * (uint64_t)g->v.id_bytes, cudaMemcpyHostToDevice, st));
+        if (g->v.weight_bytes)
+            IPG_CUDA(cudaMemcpyAsync(g->wgt, wgt, E * (uint64_t)g->v.weight_bytes, cudaMemcpyHostToDevice, st));
+    }
+    IPG_CUDA(cudaMemsetAsync(g->refill_dev, 0, 16, st));
+    if (V) {
+        k_check_row<<<grid_for(V, 256), 256, 0, st>>>(row, V, err);
+        k_max_degree<<<grid_for(V, 256), 256, 0, st>>>(row, V, maxdeg);
+    }
+    if (E) {
+        if (g->v.id_bytes == 4)
+            k_check_ids<<<grid_for(E, 256), 256, 0, st>>>((const uint32_t*)g->adj, E, V, err);
+        else
+            k_check_ids<<<grid_for(E, 256), 256, 0, st>>>((const uint64_t*)g->adj, E, V, err);
+    }
+    IPG_CUDA(cudaGetLastError());
+    IPG_CUDA(cudaMemcpyAsync(&h[1], g->refill_dev, 16, cudaMemcpyDeviceToHost, st));
+    IPG_CUDA(cudaStreamSynchronize(st));
+    const uint32_t bits = (uint32_t)h[1];
+    if (bits & 1) return fail(IPG_EIO, "malformed offsets: row starts must begin at 0, be non-decreasing and not exceed E");
+    if (bits & 2) return fail(IPG_EIO, "malformed adjacency: a neighbour id is >= the vertex count");
+    g->v.max_out_degree = h[2];
+    g->v.max_in_degree = h[2];
+    if (own_in) IPG_TRY(ipg_graph_build_in(g));  // allocates: directed graphs only
+    if (own_in) return finish_graph_stats(g, 0);
+    return IPG_OK;
 }
 
 extern "C" int ipg_graph_from_device(uint64_t V, uint64_t E, const uint64_t* d_row, const void* d_adj, int id_bytes,

@@ -122,3 +122,51 @@ def test_reattach_same_shape_and_other_shapes():
         eng.release()
         for gr in graphs.values():
             gr.free()
+
+
+def test_refill_on_a_thread_while_another_graph_runs():
+    """The pipelined pattern: graph X is refilled on a second host thread
+    (its own stream) while the engines run on graph Y; every step's results
+    equal the oracle's for that step's contents."""
+    import threading
+
+    import ipregel_b200 as ip
+    base = O.add_weights(O.gen_rmat(13, 16, seed=8, undirected=True), wmax=255, seed=2)
+    contents = [base] + [_relabel(base, seed=s) for s in (1, 2, 3, 4)]
+    gbuf = [ip.Graph.from_csr(base.V, base.E, base.idx, base.adj, wgt=base.wgt) for _ in range(2)]
+    cc = ip.Engine("cc", "spread")
+    sp = ip.Engine("sssp_weighted", "spread")
+    try:
+        for eng in (cc, sp):
+            eng.set_quiet(True)
+        sp.set_param("source", 0)
+        err = []
+
+        def refill(gr, src):
+            try:
+                gr.refill(src.idx, src.adj, src.wgt)
+            except Exception as ex:
+                err.append(ex)
+
+        th = threading.Thread(target=refill, args=(gbuf[0], contents[0]))
+        th.start()
+        for k, src in enumerate(contents):
+            th.join()
+            assert not err, err
+            if k + 1 < len(contents):
+                th = threading.Thread(target=refill, args=(gbuf[(k + 1) % 2], contents[k + 1]))
+                th.start()
+            gr = gbuf[k % 2]
+            gr.set_symmetric(True)
+            cc.attach(gr)
+            res = cc.run()
+            want, counts, _ = O.run(src, "cc", "spread")
+            _check(res, want, counts)
+            sp.attach(gr)
+            res = sp.run()
+            np.testing.assert_array_equal(res.values, O.dijkstra(src, 0))
+    finally:
+        cc.release()
+        sp.release()
+        for gr in gbuf:
+            gr.free()
