@@ -560,6 +560,17 @@ __device__ __forceinline__ T ipx_ld_stream(const T* p)
     return r;
 }
 
+/* Edge element read by a loop whose lanes take every lanes-th edge: evict-
+ * first only when a warp reads consecutive edges in one instruction (lanes
+ * >= 32).  A thread walking a short row alone (lanes = 1) comes back to the
+ * same line in its next steps, and an evict-first line is often gone by
+ * then (measured: more DRAM traffic and a slower thread class). */
+template <class T>
+__device__ __forceinline__ T ipx_ld_edge(const T* p, uint64_t lanes)
+{
+    return lanes >= 32 ? ipx_ld_stream(p) : *p;
+}
+
 /* Sets bit v of a shared bitmap; lanes that hit the same word combine first. */
 __device__ __forceinline__ void ipx_set_bit_agg(uint32_t* bm, uint64_t v)
 {
@@ -628,6 +639,7 @@ __device__ __forceinline__ T ipx_shfl_idx(T x, int src)
 struct ipx_push_visit {
     static constexpr bool kNeedsMessage = true;
     int p;
+    bool warp_wide; /* a warp or CTA walks each source's edges (weights loaded evict-first) */
     template <int U>
     __device__ __forceinline__ void batch(const uint64_t* e, const ipx_vid* w, const ipx_msg* m, const bool* ok) const
     {
@@ -638,7 +650,7 @@ struct ipx_push_visit {
             go[k] = false;
             if (ok[k]) {
 #if IPX_EDGE_MSG
-                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m[k], ipx_ld_stream(&ipx_c.wgt[e[k]]));
+                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m[k], warp_wide ? ipx_ld_stream(&ipx_c.wgt[e[k]]) : ipx_c.wgt[e[k]]);
 #else
                 mk[k] = m[k];
 #endif
@@ -687,7 +699,7 @@ __device__ __forceinline__ void ipx_edges_strided(const ipx_vid* __restrict__ ad
         for (int k = 0; k < IPX_UNROLL; k++) {
             ek[k] = e + k * lanes;
             ok[k] = ek[k] < e1;
-            w[k] = ok[k] ? ipx_ld_stream(&adj[ek[k]]) : (ipx_vid)0;
+            w[k] = ok[k] ? ipx_ld_edge(&adj[ek[k]], lanes) : (ipx_vid)0;
             mk[k] = m;
         }
         visit.template batch<IPX_UNROLL>(ek, w, mk, ok);
@@ -924,7 +936,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_push(const u
                                                           const uint32_t* __restrict__ prefix)
 {
     if (ipx_c.pull_ok && __ldcg(&ipx_c.ctr[IPX_CTR_MODE])) return; /* this superstep pulls */
-    ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{ipx_parity()});
+    ipx_over_sources<MODE>(list, *count, prefix, ipx_push_visit{ipx_parity(), MODE != 0});
 }
 
 /* Direction of the superstep's delivery: pull when the broadcasters' out-edges
@@ -988,7 +1000,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict_
         ipx_msg m[IPX_UNROLL];
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++)
-            u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_stream(&adj[e + k * lanes]) : 0;
+            u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_edge(&adj[e + k * lanes], lanes) : 0;
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) word[k] = (e + k * lanes < e1) ? __ldg(&hb[u[k] >> 5]) : 0u;
 #pragma unroll
@@ -1110,14 +1122,14 @@ __device__ __forceinline__ void ipx_pull_fold_edges(uint64_t e0, uint64_t e1, ui
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             const uint64_t ek = e + k * lanes;
-            u[k] = (ek < e1) ? (uint64_t)ipx_ld_stream(&adj[ek]) : 0;
+            u[k] = (ek < e1) ? (uint64_t)ipx_ld_edge(&adj[ek], lanes) : 0;
             word[k] = (ek < e1) ? __ldg(&bc[u[k] >> 5]) : 0u;
         }
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             if ((word[k] >> (u[k] & 31)) & 1u) {
 #if IPX_EDGE_MSG
-                ipx_msg m = IP_BROADCAST_EDGE_MESSAGE(__ldg(&ob[u[k]]), ipx_ld_stream(&ipx_c.in_wgt[e + k * lanes]));
+                ipx_msg m = IP_BROADCAST_EDGE_MESSAGE(__ldg(&ob[u[k]]), ipx_ld_edge(&ipx_c.in_wgt[e + k * lanes], lanes));
 #else
                 ipx_msg m = __ldg(&ob[u[k]]);
 #endif

@@ -979,8 +979,7 @@ __device__ __forceinline__ void pp_finish_quad(const PpArgs& a, const PpLanes& L
             else if (deg) bn[j] = __fdiv_rn(xn, (float)deg);
         }
     }
-    // evict-first: the writes would otherwise displace the rows this superstep reads at random
-    __stcs(reinterpret_cast<float4*>(a.b_next + v * PP_K) + q, make_float4(bn[0], bn[1], bn[2], bn[3]));
+    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
 }
 
 // A warp gathers [e0, e1): thread t takes lane quad t % PP_Q and edge slot
@@ -1045,7 +1044,7 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, co
 #pragma unroll
         for (int k = 0; k < 4; k++) s[k] = c[k] = 0.0f;
         for (uint64_t e = e0; e < e1; e += 4) {
-            const uint32_t uj = (q < 4 && e + q < e1) ? ld_edge(&a.adj[e + q]) : 0u;
+            const uint32_t uj = (q < 4 && e + q < e1) ? a.adj[e + q] : 0u;
             const int ne = (int)((e1 - e) < 4 ? (e1 - e) : 4);
             float4 x[4];
 #pragma unroll
