@@ -127,6 +127,23 @@ __device__ __forceinline__ T ipx_from_word(typename ipx_word<T>::type w)
     return x;
 }
 
+/* Bitwise equality: a compute kernel writes a vertex's value back only when
+ * ip_compute changed it (unchanged receivers are common in min-propagation
+ * supersteps; each skipped store is a dirty sector less). */
+template <class T>
+__device__ __forceinline__ bool ipx_same_bits(const T& a, const T& b)
+{
+    if constexpr (sizeof(T) <= 8) {
+        return ipx_to_word(a) == ipx_to_word(b);
+    } else {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&a);
+        const unsigned char* q = reinterpret_cast<const unsigned char*>(&b);
+        for (size_t k = 0; k < sizeof(T); k++)
+            if (p[k] != q[k]) return false;
+        return true;
+    }
+}
+
 template <class T>
 __device__ __forceinline__ T ipx_shfl_down(T x, int o)
 {
@@ -1232,11 +1249,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner()
                 x.has_message = h;
                 if (h) x.message = ipx_c.msg[v];
             }
-            x.value = ipx_c.value[v];
+            const ipx_val v0 = ipx_c.value[v];
+            x.value = v0;
             x.ipx_has_out = false;
             ipx_fill_topology(x, v);
             ip_compute(&x);
-            ipx_c.value[v] = x.value;
+            if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
             a = x.active;
             h = x.has_message;
             if (h) ipx_c.msg[v] = x.message;
@@ -1272,11 +1290,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32
         x.active = true;
         x.has_message = s != 0;
         if (s) x.message = ipx_mb::take(&ipx_c.mbox[pprev][v]);
-        x.value = ipx_c.value[v];
+        const ipx_val v0 = ipx_c.value[v];
+        x.value = v0;
         x.ipx_has_out = false;
         ipx_fill_topology(x, v);
         ip_compute(&x);
-        ipx_c.value[v] = x.value;
+        if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
         if (x.ipx_has_out) {
             ipx_c.outbox[v] = x.ipx_out;
             ipx_set_bit_agg(ipx_c.bcaster, v);
@@ -1303,11 +1322,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb()
             x.active = true;
             x.has_message = ipx_c.hasmsg_b[v];
             if (x.has_message) x.message = ipx_c.msg[v];
-            x.value = ipx_c.value[v];
+            const ipx_val v0 = ipx_c.value[v];
+            x.value = v0;
             x.ipx_has_out = false;
             ipx_fill_topology(x, v);
             ip_compute(&x);
-            ipx_c.value[v] = x.value;
+            if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
             if (!x.active) ipx_c.active_b[v] = 0;
             a = x.active;
             if (x.ipx_has_out) {
@@ -1342,11 +1362,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(const uint32_t*
         x.active = true;
         x.has_message = ipx_c.hasmsg_b[v];
         if (x.has_message) x.message = ipx_c.msg[v];
-        x.value = ipx_c.value[v];
+        const ipx_val v0 = ipx_c.value[v];
+        x.value = v0;
         x.ipx_has_out = false;
         ipx_fill_topology(x, v);
         ip_compute(&x);
-        ipx_c.value[v] = x.value;
+        if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
         if (x.ipx_has_out) {
             ipx_c.bval[v] = x.ipx_out;
             ipx_set_bit_agg(ipx_c.has_b, v);

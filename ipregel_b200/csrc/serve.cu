@@ -979,7 +979,9 @@ __device__ __forceinline__ void pp_finish_quad(const PpArgs& a, const PpLanes& L
             else if (deg) bn[j] = __fdiv_rn(xn, (float)deg);
         }
     }
-    reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
+    // a vertex without edges has quotient 0 in every lane, and both buffers
+    // start zeroed: its row is never written (a third of R-MAT's vertices)
+    if (deg) reinterpret_cast<float4*>(a.b_next + v * PP_K)[q] = make_float4(bn[0], bn[1], bn[2], bn[3]);
 }
 
 // A warp gathers [e0, e1): thread t takes lane quad t % PP_Q and edge slot
