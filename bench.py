@@ -417,6 +417,16 @@ def serving_row():
     runs.sort(key=lambda r: r[0]["qps"])
     summ, clk = runs[1]
     st = srv.stats()
+    # device time, supersteps and lanes per lane-group kind and graph scale
+    groups = {}
+    for gid, name, busy, steps, lanes, _ in srv.group_stats():
+        a = groups.setdefault(f"scale{scales[gid]}:{name}", {"busy_s": 0.0, "supersteps": 0, "lanes": 0})
+        a["busy_s"] = round(a["busy_s"] + busy, 3)
+        a["supersteps"] += steps
+        a["lanes"] += lanes
+    for k, a in groups.items():
+        if k.endswith(":ppr") and a["supersteps"]:
+            a["mean_busy_lanes"] = round(a["lanes"] * 20 / a["supersteps"], 1)  # each lane runs 20 gathers
     srv.free()
     m = 150
     tot, per = 0.0, {0: [], 1: [], 2: []}
@@ -453,6 +463,9 @@ def serving_row():
                             f"once per graph, device loop time only",
             "speedup_vs_plain": round(summ["qps"] / plain_qps, 2),
             "counters_cover": "the 64-query warm-up trace and the three runs",
+            "groups": groups,
+            "groups_note": "per graph scale (two graphs each) and group kind: summed superstep device time "
+                           "(concurrent groups overlap), supersteps, lanes admitted; PPR: mean busy lanes of 32",
             "lanes_admitted": st["lanes_admitted"], "supersteps": st["supersteps"],
             "kernel_launches": st["kernel_launches"], "pull_supersteps": st["pull_supersteps"],
             "peak_hbm_bytes": st["peak_bytes"], "hbm_free_before_trace": free_b, "clocks_during_trace": clk,
