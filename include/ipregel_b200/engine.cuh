@@ -911,13 +911,32 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
     if constexpr ((MODE == 0 || MODE == 1) && IPX_PUSH_EXPAND) {
         ipx_warp_expand(list, n, visit);
     } else if constexpr (MODE == 0) {
+        /* the next source's list entry, row bounds and message are loaded
+         * while this source's edges are visited */
         const ipx_vid* __restrict__ adj = ipx_c.adj;
         const uint64_t* __restrict__ row = ipx_c.row;
-        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+        const uint64_t stride = ipx_gstride();
+        uint64_t i = ipx_gtid(), r0 = 0, r1 = 0;
+        ipx_msg m = ipx_msg();
+        if (i < n) {
             const uint64_t u = list[i];
-            ipx_msg m = ipx_msg();
+            r0 = row[u];
+            r1 = row[u + 1];
             if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
-            ipx_edges_strided(adj, row[u], row[u + 1], 0, 1, m, visit);
+        }
+        for (; i < n; i += stride) {
+            uint64_t r0n = 0, r1n = 0;
+            ipx_msg mn = ipx_msg();
+            if (i + stride < n) {
+                const uint64_t un = list[i + stride];
+                r0n = row[un];
+                r1n = row[un + 1];
+                if constexpr (Visit::kNeedsMessage) mn = ipx_c.outbox[un];
+            }
+            ipx_edges_strided(adj, r0, r1, 0, 1, m, visit);
+            r0 = r0n;
+            r1 = r1n;
+            m = mn;
         }
     } else if constexpr (MODE == 1) {
         const ipx_vid* __restrict__ adj = ipx_c.adj;

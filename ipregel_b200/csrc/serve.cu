@@ -1030,7 +1030,7 @@ __device__ __forceinline__ void pp_gather_warp(const PpArgs& a, uint64_t e0, uin
 // threads of the group load four consecutive ids at a time and the group
 // shares them by shuffle; the four rows are summed pairwise and added
 // compensated, in edge order.
-__global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(SRV_THREADS, 4) k_pp_rows(PpArgs a, PpLanes L, const uint32_t* __restrict__ list,
                                                          uint64_t n)
 {
     const int lane = threadIdx.x & 31, q = lane % PP_Q, gb = lane - q;
@@ -1038,15 +1038,36 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, co
     const bool quad_on = (L.active >> (4 * q)) & 0xFULL;
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     const uint64_t groups = ((uint64_t)gridDim.x * blockDim.x) / PP_Q;
-    // the threads of a group share i, so they leave the loop together
-    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / PP_Q; i < n; i += groups) {
-        const uint64_t v = list[i];
-        const uint64_t e0 = a.row[v], e1 = a.row[v + 1];
+    // The next vertex's list entry, row bounds and first four ids are loaded
+    // while this vertex's rows are gathered, and the next four ids of a row
+    // while its current four rows are: the chain list -> offsets -> ids ->
+    // rows leaves the critical path except for its last link.  The threads
+    // of a group share i, so they leave the loop together.
+    uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / PP_Q;
+    uint64_t v = 0, e0 = 0, e1 = 0;
+    uint32_t u0 = 0;
+    if (i < n) {
+        v = list[i];
+        e0 = a.row[v];
+        e1 = a.row[v + 1];
+        u0 = (q < 4 && e0 + q < e1) ? a.adj[e0 + q] : 0u;
+    }
+    for (; i < n; i += groups) {
+        const uint64_t in = i + groups;
+        uint64_t vn = 0, e0n = 0, e1n = 0;
+        uint32_t u0n = 0;
+        if (in < n) {
+            vn = list[in];
+            e0n = a.row[vn];
+            e1n = a.row[vn + 1];
+            u0n = (q < 4 && e0n + q < e1n) ? a.adj[e0n + q] : 0u;
+        }
         float s[4], c[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) s[k] = c[k] = 0.0f;
+        uint32_t uj = u0;
         for (uint64_t e = e0; e < e1; e += 4) {
-            const uint32_t uj = (q < 4 && e + q < e1) ? a.adj[e + q] : 0u;
+            const uint32_t un = (q < 4 && e + 4 + q < e1) ? a.adj[e + 4 + q] : 0u;
             const int ne = (int)((e1 - e) < 4 ? (e1 - e) : 4);
             float4 x[4];
 #pragma unroll
@@ -1055,8 +1076,13 @@ __global__ void __launch_bounds__(SRV_THREADS) k_pp_rows(PpArgs a, PpLanes L, co
                 x[r] = (quad_on && r < ne) ? pp_row(a, u, q) : z;
             }
             if (quad_on) pp_add4(s, c, pp_sum4(x[0], x[1], x[2], x[3]));
+            uj = un;
         }
         pp_finish_quad(a, L, v, e1 - e0, q, s, c);
+        v = vn;
+        e0 = e0n;
+        e1 = e1n;
+        u0 = u0n;
     }
 }
 
