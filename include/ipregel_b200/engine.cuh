@@ -910,6 +910,16 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
 {
     if constexpr ((MODE == 0 || MODE == 1) && IPX_PUSH_EXPAND) {
         ipx_warp_expand(list, n, visit);
+    } else if constexpr (MODE == 0 && sizeof(ipx_vid) == 8) {
+        /* 64-bit ids: the loop below would spill registers */
+        const ipx_vid* __restrict__ adj = ipx_c.adj;
+        const uint64_t* __restrict__ row = ipx_c.row;
+        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
+            const uint64_t u = list[i];
+            ipx_msg m = ipx_msg();
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+            ipx_edges_strided(adj, row[u], row[u + 1], 0, 1, m, visit);
+        }
     } else if constexpr (MODE == 0) {
         /* the next source's list entry, row bounds and message are loaded
          * while this source's edges are visited */
@@ -1064,8 +1074,12 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
     const ipx_msg* __restrict__ bv = ipx_c.bval;
     unsigned long long react = 0;
     if constexpr (MODE == 0) {
-        for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
-            const uint64_t v = list[i];
+        /* the next vertex's list entry is loaded while this vertex's
+         * in-edges are folded (its row bounds too would spill registers) */
+        const uint64_t stride = ipx_gstride();
+        uint64_t i = ipx_gtid(), v = (i < n) ? list[i] : 0;
+        for (; i < n; i += stride) {
+            const uint64_t vn = (i + stride < n) ? list[i + stride] : 0;
             bool has = false;
             ipx_msg acc;
             ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], 0, 1, has, acc);
@@ -1079,6 +1093,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
                     }
                 }
             }
+            v = vn;
         }
     } else if constexpr (MODE == 1) {
         const int lane = threadIdx.x & 31;
