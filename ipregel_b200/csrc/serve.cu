@@ -1281,11 +1281,6 @@ struct ipg_server {
     uint32_t delta = 1024;
     // dense min-plus supersteps on symmetric graphs pull (IPG_SERVE_PULL=0: never)
     bool pull = true;
-    // an idle PPR group starts when this many queries wait for it
-    // (IPG_SERVE_PPR_FILL), when its oldest has waited ppr_wait seconds
-    // (IPG_SERVE_PPR_WAIT_MS), or when no other group is running
-    uint32_t ppr_fill = 24;
-    double ppr_wait = 0.5;
     std::mutex mu;
     ipg_server_stats stats{};
 };
@@ -1726,23 +1721,6 @@ int launch_superstep(ipg_server* S, Group* G)
     return IPG_OK;
 }
 
-// Whether an idle PPR group waits before starting a cohort.  A PPR superstep
-// gathers every edge of the graph whatever the number of busy lanes, so a
-// group started for the first query of a stream runs most of its supersteps
-// with lanes empty (13 - 18 busy of 32 on average, measured on the mixed R-MAT
-// trace).  While other groups keep the device busy, waiting costs no device
-// time; the lanes then fill at the start, and later queries still join at
-// every superstep of the running group.
-bool ppr_should_wait(ipg_server* S, Group* G, double now)
-{
-    const std::deque<uint64_t>& queue = S->pending[(size_t)G->G->gid * 2 + 1];
-    if (queue.empty() || queue.size() >= S->ppr_fill) return false;
-    if (now - S->queries[queue.front()].t_submit >= S->ppr_wait) return false;
-    for (const Group* o : S->groups)
-        if (o != G && o->running) return true;
-    return false;
-}
-
 // A completed superstep: retire finished lanes.
 void retire(ipg_server* S, Group* G, double now)
 {
@@ -1836,10 +1814,6 @@ extern "C" int ipg_server_create(uint64_t hbm_budget, uint32_t ppr_rounds, ipg_s
         if (*d) S->delta = (uint32_t)std::max(1UL, strtoul(d, nullptr, 10));
     if (const char* p = getenv("IPG_SERVE_PULL"))
         if (*p) S->pull = strtol(p, nullptr, 10) != 0;
-    if (const char* f = getenv("IPG_SERVE_PPR_FILL"))
-        if (*f) S->ppr_fill = (uint32_t)std::min(strtoul(f, nullptr, 10), (unsigned long)PP_K);
-    if (const char* w = getenv("IPG_SERVE_PPR_WAIT_MS"))
-        if (*w) S->ppr_wait = std::max(0.0, strtod(w, nullptr)) * 1e-3;
     *out = S;
     return IPG_OK;
 }
@@ -1998,7 +1972,6 @@ extern "C" int ipg_server_poll(ipg_server* S, uint64_t* outstanding)
             }
             retire(S, G, now);
         }
-        if (G->kind == 1 && !G->busy && ppr_should_wait(S, G, now)) continue;
         admit(S, G, now);
         if (G->busy) {
             int r = launch_superstep(S, G);
