@@ -161,7 +161,9 @@ __device__ __forceinline__ void pr_finish(const PrStep& a, uint64_t v, uint64_t 
 }
 
 // Lane-strided compensated sum of b_cur over adj[e0, e1), PR_UNROLL loads in
-// flight per lane.
+// flight per lane.  Ids are loaded evict-first where a warp reads consecutive
+// ids in one instruction (lanes >= 32); a thread walking a row alone comes
+// back to the same line in its next loads, so it keeps the line cached.
 template <bool COMP>
 __device__ __forceinline__ void pr_gather(const PrStep& a, uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
                                           float& s, float& c)
@@ -172,7 +174,7 @@ __device__ __forceinline__ void pr_gather(const PrStep& a, uint64_t e0, uint64_t
 #pragma unroll
         for (int k = 0; k < PR_UNROLL; k++) {
             const uint64_t ek = e + k * lanes;
-            u[k] = ek < e1 ? __ldcs(&a.in_adj[ek]) : 0u;
+            u[k] = ek < e1 ? (lanes >= 32 ? __ldcs(&a.in_adj[ek]) : a.in_adj[ek]) : 0u;
         }
 #pragma unroll
         for (int k = 0; k < PR_UNROLL; k++) q[k] = (e + k * lanes < e1) ? __ldg(&a.b_cur[u[k]]) : 0.0f;
@@ -218,12 +220,28 @@ __global__ void __launch_bounds__(PR_THREADS) k_pr_diag(const float* __restrict_
 template <bool COMP, bool LAST>
 __global__ void __launch_bounds__(PR_THREADS) k_pr_thread(PrStep a, const uint32_t* __restrict__ list, uint64_t n)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t v = list[i];
-        const uint64_t e0 = a.in_row[v], e1 = a.in_row[v + 1];
+    // the next vertex's list entry and row bounds are loaded while this
+    // vertex's in-edges are gathered
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, v = 0, e0 = 0, e1 = 0;
+    if (i < n) {
+        v = list[i];
+        e0 = a.in_row[v];
+        e1 = a.in_row[v + 1];
+    }
+    for (; i < n; i += stride) {
+        uint64_t vn = 0, e0n = 0, e1n = 0;
+        if (i + stride < n) {
+            vn = list[i + stride];
+            e0n = a.in_row[vn];
+            e1n = a.in_row[vn + 1];
+        }
         float s = 0.0f, c = 0.0f;
         pr_gather<COMP>(a, e0, e1, 0, 1, s, c);
         pr_finish<LAST>(a, v, pr_deg(a, v, e0, e1), __fadd_rn(s, c));
+        v = vn;
+        e0 = e0n;
+        e1 = e1n;
     }
 }
 
