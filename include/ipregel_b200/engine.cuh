@@ -901,10 +901,6 @@ __device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_
 /* Push delivery over degree-class lists of broadcasters.                   */
 /* MODE 0: a thread per broadcaster; 1: a warp; 2: a block.                 */
 /* ------------------------------------------------------------------------ */
-/* Source loops that load the next source while pushing the current one fit
- * the register budget (6 CTAs per SM) with 32-bit ids and a hardware combine. */
-constexpr bool ipx_prefetch_sources = sizeof(ipx_vid) == 4 && IP_COMBINE_KIND != IP_COMBINE_GENERIC;
-
 /* Runs a visitor over the out-edges of a degree-class list of sources:
  * MODE 0 and 1 by warp-cooperative expansion, MODE 2 (the hubs) a CTA per
  * IPX_HUB_CHUNK-edge chunk, chunks located through `prefix`. */
@@ -914,8 +910,8 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
 {
     if constexpr ((MODE == 0 || MODE == 1) && IPX_PUSH_EXPAND) {
         ipx_warp_expand(list, n, visit);
-    } else if constexpr (MODE == 0 && !ipx_prefetch_sources) {
-        /* 64-bit ids or a CAS-loop combine: the loop below would spill registers */
+    } else if constexpr (MODE == 0 && sizeof(ipx_vid) == 8) {
+        /* 64-bit ids: the loop below would spill registers */
         const ipx_vid* __restrict__ adj = ipx_c.adj;
         const uint64_t* __restrict__ row = ipx_c.row;
         for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
@@ -952,7 +948,7 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
             r1 = r1n;
             m = mn;
         }
-    } else if constexpr (MODE == 1 && !ipx_prefetch_sources) {
+    } else if constexpr (MODE == 1) {
         const ipx_vid* __restrict__ adj = ipx_c.adj;
         const uint64_t* __restrict__ row = ipx_c.row;
         const uint64_t lane = threadIdx.x & 31;
@@ -961,36 +957,6 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
             ipx_msg m = ipx_msg();
             if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
             ipx_edges_strided(adj, row[u], row[u + 1], lane, 32, m, visit);
-        }
-    } else if constexpr (MODE == 1) {
-        /* most sources of the warp class take one pass of the edge loop, so
-         * the next source's list entry, row bounds and message are loaded
-         * while this source's edges are pushed */
-        const ipx_vid* __restrict__ adj = ipx_c.adj;
-        const uint64_t* __restrict__ row = ipx_c.row;
-        const uint64_t lane = threadIdx.x & 31;
-        const uint64_t wstride = ipx_gstride() >> 5;
-        uint64_t i = ipx_gtid() >> 5, r0 = 0, r1 = 0;
-        ipx_msg m = ipx_msg();
-        if (i < n) {
-            const uint64_t u = list[i];
-            r0 = row[u];
-            r1 = row[u + 1];
-            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
-        }
-        for (; i < n; i += wstride) {
-            uint64_t r0n = 0, r1n = 0;
-            ipx_msg mn = ipx_msg();
-            if (i + wstride < n) {
-                const uint64_t un = list[i + wstride];
-                r0n = row[un];
-                r1n = row[un + 1];
-                if constexpr (Visit::kNeedsMessage) mn = ipx_c.outbox[un];
-            }
-            ipx_edges_strided(adj, r0, r1, lane, 32, m, visit);
-            r0 = r0n;
-            r1 = r1n;
-            m = mn;
         }
     } else {
         if (n == 0) return;
