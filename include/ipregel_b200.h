@@ -111,8 +111,11 @@ int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int idx_bytes,
  * degree classes, the symmetric declaration, and an in-CSR built for a
  * directed graph (rebuilt here).  Validation as at load; on a malformed
  * input the graph keeps the new contents and must not be run.  No engine may
- * be running on the graph; engines attached to it attach again before their
- * next run, and a request server must not hold it. */
+ * be running on the graph, nor another refill of it; engines attached to it
+ * attach again before their next run, and a request server must not hold it.
+ * The first call on a graph makes its stream and a few small buffers; later
+ * calls allocate nothing and synchronise only that stream, so one thread may
+ * refill a graph while kernels on another graph run. */
 int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_bytes,
                           const void* adj, const void* wgt);
 
