@@ -1317,8 +1317,13 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32
     const uint64_t s = ipx_step();
     const uint64_t n = s ? (uint64_t)*fcount : ipx_c.V;
     const int pprev = (int)((s + 1) & 1);
-    for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
-        const uint64_t v = s ? frontier[i] : i;
+    /* the next frontier entry is loaded while this vertex computes */
+    const uint64_t stride = ipx_gstride();
+    uint64_t i = ipx_gtid();
+    uint64_t vn = (i < n) ? (s ? frontier[i] : i) : 0;
+    for (; i < n; i += stride) {
+        const uint64_t v = vn;
+        vn = (i + stride < n) ? (s ? frontier[i + stride] : i + stride) : 0;
         struct ip_vertex_t x;
         x.id = (ipx_vid)v;
         x.active = true;
