@@ -48,9 +48,9 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--scale", type=int, default=24)
-    p.add_argument("--cpu-scale", type=int, default=22, help="scale of the bounded CPU sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the check of the results against the reference")
     p.add_argument("--no-extra", action="store_true",
                    help="skip the PageRank precision-split, batched and serving workloads")
     p.add_argument("--rows", default="",
@@ -212,29 +212,37 @@ def cpu_host_info():
     return os.cpu_count() or 1, model
 
 
-def run_reference_sample(graph_path, E, repeats):
-    """Times the reference's own OpenMP binaries (oracle/_ref) on graph files:
-    cc_spread_32 and sssp_spread_32 (the reference's SSSP counts hops; weights
-    have no reference implementation), all host threads, OMP_PROC_BIND=TRUE,
-    OMP_PLACES=cores, static schedule (submission.slurm:36-42).  Returns
-    (seconds for one CC + one SSSP run, best of `repeats` each, the reference's
-    own "Total time of supersteps")."""
+REF_ENV_NOTE = "OMP_PROC_BIND=TRUE, OMP_PLACES=cores, schedule static, chunk 0 (submission.slurm:36-42)"
+
+
+def reference_run(app, graph_path, threads, dump=True):
+    """One run of the reference's own OpenMP binary <app>_spread_32 (oracle/_ref)
+    on graph files, with all host threads and the environment of
+    submission.slurm:36-42.  Returns (the reference's own "Total time of
+    supersteps" in seconds, its dump text or None, its stdout).  The dump goes
+    to /dev/null when not needed (the dump is outside the timed supersteps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    threads, _ = cpu_host_info()
     env = {"OMP_NUM_THREADS": str(threads), "OMP_PROC_BIND": "TRUE", "OMP_PLACES": "cores"}
-    total = 0.0
-    for app in ("cc", "sssp"):
-        best = float("inf")
-        for _ in range(repeats):
-            _, out = O.run_ref(app, "spread", graph_path, threads=threads, schedule="static", chunk=0, env=env,
-                               timeout=1800)
-            best = min(best, O.parse_total_time(out))
-        total += best
-    return total, threads
+    if dump:
+        text, out = O.run_ref(app, "spread", graph_path, threads=threads, schedule="static", chunk=0, env=env,
+                              timeout=1800)
+    else:
+        _, out = O.run_ref(app, "spread", graph_path, threads=threads, schedule="static", chunk=0, env=env,
+                           timeout=1800, dump=False)
+        text = None
+    return O.parse_total_time(out), text, out
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU implementation of the path, on this arm's
+    workload: the scale-24 undirected R-MAT graph, generated by the oracle's
+    CPU generator (the same CSR as the device generator) and written once in
+    the reference loader's format.  Step k runs cc_spread_32 (k even) or
+    sssp_spread_32 (k odd), so that the K + W runs end within minutes; each
+    run's time is the reference's own "Total time of supersteps".  The
+    reference's SSSP counts hops: weighted SSSP has no reference
+    implementation.  Nothing of this repository's GPU runtime is loaded."""
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -242,32 +250,44 @@ def reference_arm(args, rank, world):
     if not O.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "reference binaries (oracle/_ref) were not built"}))
         return 0
-    import ipregel_b200 as ip
-    scale = args.cpu_scale
-    g = ip.Graph.generate_rmat(scale, 16, seed=1, undirected=True)
-    E = g.E
+    scale = args.scale
+    t_gen = time.time()
+    g = O.gen_rmat(scale, 16, seed=1, undirected=True)
+    t_gen = time.time() - t_gen
+    V, E = g.V, g.E
+    cores, model = cpu_host_info()
+    per = {"cc": [], "sssp": []}
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, f"rmat{scale}")
-        g.write(path)
-        g.free()
-        for _ in range(args.warmup):
-            run_reference_sample(path, E, 1)
+        O.write_graph(g, path)
+        del g
+        apps = ("cc", "sssp")
+        for k in range(args.warmup):
+            reference_run(apps[k % 2], path, cores, dump=False)
         secs = []
-        for _ in range(args.steps):
-            t, threads = run_reference_sample(path, E, 1)
+        for k in range(args.steps):
+            t, _, _ = reference_run(apps[k % 2], path, cores, dump=False)
+            per[apps[k % 2]].append(t)
             secs.append(t)
-    cores, model = cpu_host_info()
-    value = 2.0 * E * len(secs) / sum(secs) / 1e9
+    value = E * len(secs) / sum(secs) / 1e9
+    per_prog = {a: {"runs": len(v), "best_s": round(min(v), 4), "mean_s": round(sum(v) / len(v), 4),
+                    "gteps_best": round(E / min(v) / 1e9, 4)} for a, v in per.items() if v}
+    workload = (f"cc (spread) + sssp (spread, hop count: the reference has no weighted SSSP), undirected R-MAT "
+                f"scale {scale}, edge factor 16, a/b/c=0.57/0.19/0.19, seed 1")
+    sample = (f"reference cc_spread_32 and sssp_spread_32 (oracle/_ref, compiled from the reference sources) on the "
+              f"scale-{scale} graph (V={V}, E={E}, generated by the oracle's CPU generator in {t_gen:.0f} s, "
+              f"untimed), steps alternate the two programs, {cores} OpenMP threads, {REF_ENV_NOTE}, "
+              f"'Total time of supersteps', CPU {model}")
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "impl": "reference", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"cc_spread + sssp_spread, undirected R-MAT scale {scale} (bounded CPU sample of "
-                               f"the scale-{args.scale} workload), edge factor 16, seed 1",
-                   "edges_stored": E, "teps": "Graph500: stored edges per run / superstep time"},
+        "config": {"workload": workload, "vertices": V, "edges_stored": E,
+                   "teps": "Graph500: stored edges per run / superstep time",
+                   "step": "one reference run: cc_spread_32 on even steps, sssp_spread_32 on odd steps"},
+        "per_program": per_prog,
         "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
-                         "sample": f"reference cc_spread_32 + sssp_spread_32 (hop-count SSSP) on R-MAT scale {scale} "
-                                   f"undirected, OMP {cores} threads, 'Total time of supersteps', CPU {model}"},
+                         "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -472,6 +492,106 @@ def serving_row():
             "note": "arrivals exceed capacity: latency includes queueing"}
 
 
+def same_work_row(args, cc, g, E, world, barrier, max_over_ranks):
+    """CC (spread) + hop-count SSSP from 0 (spread: benchmarks/sssp.c's
+    program) on the headline graph, resident, through the captured loop: the
+    work the reference arm times, for a like-for-like ratio.  Returns (row,
+    hop distances of the last run, per-superstep counts)."""
+    import torch
+    import ipregel_b200 as ip
+    hop = ip.Engine("sssp", "spread")
+    hop.set_quiet(True)
+    hop.set_graph_loop(True)
+    hop.attach(g)
+    for _ in range(args.warmup):
+        cc.run_only()
+        hop.run_only()
+    barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    ms_cc = ms_hop = 0.0
+    for _ in range(args.steps):
+        cc.run_only()
+        ms_cc += cc.stats()[0] * 1e3
+        hop.run_only()
+        ms_hop += hop.stats()[0] * 1e3
+    t1.record()
+    barrier()
+    ms = max_over_ranks(t0.elapsed_time(t1))
+    res, counts, steps = hop.values(), hop.counts(), hop.stats()[2]
+    hop.release()
+    row = {"workload": "cc (spread) + sssp (spread, hop count from 0: benchmarks/sssp.c) on the headline graph, "
+                       "resident, captured loop",
+           "value": round(replica_gteps(world, E, 2 * args.steps, ms), 4), "unit": "GTEPS",
+           "ms_per_step": round(ms / args.steps, 3),
+           "gteps_per_program": {"cc": round(E * args.steps / (ms_cc * 1e-3) / 1e9, 4),
+                                 "sssp_hop": round(E * args.steps / (ms_hop * 1e-3) / 1e9, 4)},
+           "supersteps_sssp_hop": steps}
+    return row, res, counts
+
+
+def cpu_baseline_leg(g, E):
+    """The reference's own binaries (oracle/_ref cc_spread_32, sssp_spread_32)
+    once each on the headline graph itself (written in the reference loader's
+    format), all host threads: about 10-30 s of CPU work.  Returns (the
+    cpu_baseline object, {app: (dump text, stdout)}) -- the dumps also serve
+    the parity check."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    cores, model = cpu_host_info()
+    if not O.have_ref():
+        return {"value": None, "unit": "GTEPS", "cores": cores, "kind": "reference",
+                "sample": "reference binaries not built"}, {}
+    dumps, secs = {}, {}
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "graph")
+        g.write(path)
+        for app in ("cc", "sssp"):
+            t, text, out = reference_run(app, path, cores, dump=True)
+            secs[app] = t
+            dumps[app] = (text, out)
+    total = sum(secs.values())
+    cpu = {"value": round(2.0 * E / total / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+           "sample": f"reference cc_spread_32 + sssp_spread_32 (hop-count SSSP; weighted SSSP has no reference "
+                     f"implementation), one run each on the headline scale-24 graph (E={E}), {cores} OpenMP "
+                     f"threads, {REF_ENV_NOTE}, 'Total time of supersteps', CPU {model}",
+           "seconds": {k: round(v, 4) for k, v in secs.items()}}
+    return cpu, dumps
+
+
+def parity_check(V, E, idx, adj, wgt, res_cc, counts_cc, res_sp, res_hop, counts_hop, ref_dumps):
+    """Checks the timed runs' results: CC labels and hop-count SSSP distances
+    against the reference binaries' own dumps of the same graph (else the
+    oracle's restatement), per-superstep active counts against the
+    reference's log lines, weighted SSSP distances against the oracle's exact
+    Dijkstra.  Bit-exact comparisons."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    t = time.time()
+    g = O.CSR(V, E, idx, adj, wgt)
+    out = {}
+    for app, res, counts in (("cc", res_cc, counts_cc), ("sssp", res_hop, counts_hop)):
+        if res is None:
+            continue
+        if app in ref_dumps:
+            text, stdout = ref_dumps[app]
+            want = O.parse_dump_fast(text, V)
+            want_counts = O.parse_counts(stdout)
+            against = f"reference {app}_spread_32 dump"
+        else:
+            want, want_counts, _ = O.run(g, app, "spread")
+            want_counts = [int(c) for c in want_counts]
+            against = f"oracle {app} spread"
+        out[app] = {"values_equal": bool(np.array_equal(np.asarray(res, dtype=np.uint32), want)),
+                    "counts_equal": [int(c) for c in counts] == list(want_counts), "against": against}
+    d = O.dijkstra(g, 0)
+    out["sssp_weighted"] = {"values_equal": bool(np.array_equal(np.asarray(res_sp, dtype=np.uint32), d)),
+                            "against": "oracle Dijkstra (exact, integer)"}
+    ok = all(v["values_equal"] and v.get("counts_equal", True) for v in out.values())
+    return {"ok": ok, **out, "check_s": round(time.time() - t, 1)}
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_setup(args.gpus)
@@ -535,6 +655,10 @@ def main():
     clk = clocks.stop()
     ms = max_over_ranks(t0.elapsed_time(t1))
     launches = cc.launches() + sp.launches()
+    # the timed runs' own results, checked after the timing against the
+    # reference's binaries and the oracle (parity)
+    res_cc, res_sp = cc.values(), sp.values()
+    counts_cc = cc.counts()
 
     runs = 2 * args.steps
     value = replica_gteps(world, E, runs, ms)
@@ -588,11 +712,16 @@ def main():
         except Exception:
             pass
 
+    # ---- the same work as the reference arm: CC + hop-count SSSP ----
+    same_work, res_hop, counts_hop = same_work_row(args, cc, g, E, world, barrier, max_over_ranks)
+
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
-    cc_labels_components = reached = None
+    cc_labels_components = int(len(np.unique(res_cc)))
+    reached = int(np.count_nonzero(res_sp != 0xFFFFFFFF))
+    h_idx, h_adj, h_wgt = g.to_host()  # also the oracle's input for the parity checks
     if not args.no_e2e:
-        idx, adj, wgt = g.to_host()
+        idx, adj, wgt = h_idx, h_adj, h_wgt
         p_idx = ip.PinnedArray(V, np.uint64)
         p_adj = ip.PinnedArray(E, np.uint32)
         p_wgt = ip.PinnedArray(E, np.uint32)
@@ -667,37 +796,26 @@ def main():
                "sequential": {"value": round(replica_gteps(world, E, runs, ms_seq), 4),
                               "ms_per_step": round(ms_seq / args.steps, 3),
                               "path": "the same steps with no overlap: refill, then compute"}}
-        cc_labels_components = int(len(np.unique(out_cc.array)))
-        reached = int(np.count_nonzero(out_sp.array != 0xFFFFFFFF))
+        e2e["results_equal_resident"] = bool(np.array_equal(out_cc.array, res_cc) and
+                                             np.array_equal(out_sp.array, res_sp))
         for gr in gbuf:
             gr.free()
         for a in (p_idx, p_adj, p_wgt, out_cc, out_sp):
             a.free()
     cc.release()
     sp.release()
+
+    # ---- CPU baseline: the reference's binaries on the same graph ----
+    cpu, ref_dumps = None, {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, ref_dumps = cpu_baseline_leg(g, E)
     g.free()
 
-    # ---- CPU baseline: the reference's binaries on a bounded sample ----
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        cores, model = cpu_host_info()
-        if O.have_ref():
-            gs = ip.Graph.generate_rmat(args.cpu_scale, 16, seed=1, undirected=True)
-            Es = gs.E
-            with tempfile.TemporaryDirectory() as td:
-                path = os.path.join(td, f"rmat{args.cpu_scale}")
-                gs.write(path)
-                gs.free()
-                secs, threads = run_reference_sample(path, Es, 2)
-            cpu = {"value": round(2.0 * Es / secs / 1e9, 4), "unit": "GTEPS", "cores": threads, "kind": "reference",
-                   "sample": f"reference cc_spread_32 + sssp_spread_32 (hop-count SSSP; weighted SSSP has no "
-                             f"reference implementation) on undirected R-MAT scale {args.cpu_scale} "
-                             f"(E={Es}), best of 2, 'Total time of supersteps', CPU {model}"}
-        else:
-            cpu = {"value": None, "unit": "GTEPS", "cores": cores, "kind": "reference",
-                   "sample": "reference binaries not built"}
+    # ---- parity of the timed runs' results (outside every timed region) ----
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_check(V, E, h_idx, h_adj, h_wgt, res_cc, counts_cc, res_sp, res_hop, counts_hop, ref_dumps)
+    del h_idx, h_adj, h_wgt
 
     # ---- the other workloads (one GPU only; each frees what it held) ----
     extra = {}
@@ -727,6 +845,9 @@ def main():
                        "traversed_gteps": round(traversed_gteps, 4),
                        "supersteps_cc_sssp": list(supersteps[0]) if supersteps else None,
                        "cc_components": cc_labels_components, "sssp_reached": reached},
+            "parity": parity["ok"] if parity else None,
+            "parity_detail": parity,
+            "same_work_as_reference": same_work,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -112,12 +112,22 @@ int ipg_graph_from_host(uint64_t V, uint64_t E, const void* idx, int idx_bytes,
  * directed graph (rebuilt here).  Validation as at load; on a malformed
  * input the graph keeps the new contents and must not be run.  No engine may
  * be running on the graph, nor another refill of it; engines attached to it
- * attach again before their next run, and a request server must not hold it.
- * The first call on a graph makes its stream and a few small buffers; later
- * calls allocate nothing and synchronise only that stream, so one thread may
- * refill a graph while kernels on another graph run. */
+ * attach again before their next run (a run without it fails with
+ * IPG_EINVAL), and a request server must not hold it.  After a failed
+ * refill every attach and run on the graph fails with IPG_EINVAL until a
+ * refill succeeds.  The first call on a graph makes its stream and a few
+ * small buffers; later calls allocate nothing and synchronise only that
+ * stream, so one thread may refill a graph while kernels on another graph
+ * run.  Degree classes (single_broadcast versions) and a directed graph's
+ * in-CSR are derived data: the next attach of such a program rebuilds them,
+ * and that rebuild allocates and synchronises the device. */
 int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_bytes,
                           const void* adj, const void* wgt);
+
+/* The contents generation of a graph (0 at creation, +1 at every refill) and
+ * whether its contents passed validation (1) or a refill failed (0).  The
+ * engine records the generation at attach and checks both before each run. */
+int ipg_graph_contents(const ipg_graph* g, uint64_t* generation, int* valid);
 
 /* Wraps device buffers (row with V+1 entries) without copying; the caller
  * keeps them alive until ipg_graph_free. */
@@ -204,8 +214,10 @@ int ipg_graph_bins(ipg_graph* g, int use_in, uint64_t t0, uint64_t t1,
  * the device: the three class sizes, then their degree sums).  Scratch is a
  * static device array of 384 KiB that every GPU loading the library holds
  * until exit, so V is limited to 67,108,864 (IPG_EINVAL beyond).  The first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the array: calls that overlap
+ * call on a device looks up the array's device address and keeps it for the
+ * life of the process; make that first call before any stream capture.  A
+ * cudaDeviceReset invalidates the kept address (the module is loaded anew),
+ * so do not call this entry point on a device after resetting it.  All calls share the array: calls that overlap
  * on the GPU (different streams, or concurrent host threads) race and must be
  * serialised by the caller.  Asynchronous on `stream`. */
 int ipg_degree_classes_noalloc(uint64_t V, const uint64_t* d_row, uint64_t t0,

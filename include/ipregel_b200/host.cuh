@@ -57,6 +57,7 @@ struct ipx_host_state {
     ipg_graph* g = nullptr;
     bool own_graph = false;
     ipg_graph_view gv;
+    uint64_t graph_generation = 0; /* the graph's contents generation at attach */
     ipx_consts c;
     std::vector<std::pair<void*, uint64_t>> allocs;
     /* device buffers of the previous attachment, kept through a re-attach:
@@ -401,6 +402,13 @@ static int ipx_attach(ipg_graph* g, bool own)
     ipx_h.g = g;
     ipx_h.own_graph = own;
     IPX_OK(ipg_graph_view_get(g, &ipx_h.gv));
+    int valid = 1;
+    IPX_OK(ipg_graph_contents(g, &ipx_h.graph_generation, &valid));
+    if (!valid) {
+        ipx_h.g = nullptr;
+        ipx_h.own_graph = false;
+        return ipx_fail(IPG_EINVAL, "the graph's contents failed validation at its last refill");
+    }
     bool need_in = IPX_PULL
 #if defined(IP_NEEDS_IN_NEIGHBOUR_IDS) || defined(IP_NEEDS_IN_NEIGHBOUR_COUNT) || IPX_IN_WEIGHTS
                    || true
@@ -776,9 +784,23 @@ static int ipx_build_graph_loop()
 }
 
 /* Before a launch of a captured loop: superstep 0 on the device. */
+/* The attached graph still holds the contents the engine's derived state
+ * (degree classes, in-CSR pointers) was built from, and they are valid. */
+static int ipx_check_contents()
+{
+    uint64_t gen = 0;
+    int valid = 1;
+    IPX_OK(ipg_graph_contents(ipx_h.g, &gen, &valid));
+    if (!valid) return ipx_fail(IPG_EINVAL, "the graph's contents failed validation at its last refill");
+    if (gen != ipx_h.graph_generation)
+        return ipx_fail(IPG_EINVAL, "the graph was refilled after this engine attached it: attach it again");
+    return IPG_OK;
+}
+
 static int ipx_loop_prepare()
 {
     if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
+    IPX_OK(ipx_check_contents());
     if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
     ipx_h.dirty = true;
     size_t zero = 0;
@@ -849,6 +871,7 @@ static int ipx_run_graph_loop()
 static int ipx_run_impl()
 {
     if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "ip_run called before ip_init");
+    IPX_OK(ipx_check_contents());
     if (ipx_h.dirty) IPX_OK(ipx_reset_vertex_state());
     ipx_h.dirty = true;
     IPX_OK(ipx_h.graph_loop ? ipx_run_graph_loop() : ipx_run_host_loop());

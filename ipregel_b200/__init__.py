@@ -47,7 +47,7 @@ RUNTIME_SYMBOLS = (
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
     "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats", "ipg_measure_gather",
-    "ipg_server_reserve", "ipg_graph_refill_host",
+    "ipg_server_reserve", "ipg_graph_refill_host", "ipg_graph_contents",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -100,6 +100,7 @@ def runtime():
         L.ipg_graph_from_host.argtypes = [u64, u64, vp, i32, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_from_device.argtypes = [u64, u64, vp, vp, i32, vp, i32, i32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_refill_host.argtypes = [vp, vp, i32, vp, vp]
+        L.ipg_graph_contents.argtypes = [vp, ctypes.POINTER(u64), ctypes.POINTER(ctypes.c_int)]
         L.ipg_graph_load.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, i32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_generate_rmat.argtypes = [ctypes.c_uint32, ctypes.c_uint32, dbl, dbl, dbl, u64, i32,
                                               ctypes.c_uint32, i32, ctypes.POINTER(vp)]
@@ -245,6 +246,9 @@ class DeviceArray:
             pass
 
 
+_WEIGHT_DTYPES = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+
+
 class Graph:
     """A graph resident in HBM (the reference loader's CSR,
     src/iPregel_postamble.h:244-421, plus the in-CSR when needed)."""
@@ -293,13 +297,31 @@ class Graph:
         adj = np.ascontiguousarray(adj, dtype=np.uint32 if int(self.view.id_bytes) == 4 else np.uint64)
         if idx.size != V or adj.size != E:
             raise ValueError(f"refill: expected {V} row starts and {E} ids, got {idx.size} and {adj.size}")
-        if wgt is not None:
-            wgt = np.ascontiguousarray(wgt, dtype=np.uint32)
+        wb = int(self.view.weight_bytes)
+        if wb == 0:
+            if wgt is not None:
+                raise ValueError("refill: the graph is unweighted, but weights were given")
+        else:
+            if wgt is None:
+                if E:
+                    raise ValueError(f"refill: the graph is weighted ({wb}-byte weights): weights are required")
+            else:
+                wgt = np.ascontiguousarray(wgt, dtype=_WEIGHT_DTYPES[wb])
+                if wgt.size != E:
+                    raise ValueError(f"refill: expected {E} weights, got {wgt.size}")
         _check(runtime().ipg_graph_refill_host(self._h, idx.ctypes.data if V else None, 8,
                                                adj.ctypes.data if E else None,
                                                wgt.ctypes.data if (wgt is not None and E) else None),
                where="ipg_graph_refill_host")
         self.refresh()
+
+    def contents(self):
+        """(generation, valid): the contents generation (+1 at every refill)
+        and whether the last refill passed validation (ipg_graph_contents)."""
+        gen = ctypes.c_uint64()
+        ok = ctypes.c_int()
+        _check(runtime().ipg_graph_contents(self._h, ctypes.byref(gen), ctypes.byref(ok)), where="ipg_graph_contents")
+        return int(gen.value), bool(ok.value)
 
     @classmethod
     def generate_rmat(cls, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, undirected=False, wmax=0,
@@ -368,7 +390,7 @@ class Graph:
         V, E = self.V, self.E
         idx = np.zeros(max(V, 1), dtype=np.uint64)
         adj = np.zeros(max(E, 1), dtype=np.uint32 if self.view.id_bytes == 4 else np.uint64)
-        wgt = np.zeros(max(E, 1), dtype=np.uint32) if self.view.d_wgt else None
+        wgt = np.zeros(max(E, 1), dtype=_WEIGHT_DTYPES[int(self.view.weight_bytes)]) if self.view.d_wgt else None
         _check(runtime().ipg_graph_to_host(self._h, idx.ctypes.data, adj.ctypes.data,
                                            wgt.ctypes.data if wgt is not None else None), where="ipg_graph_to_host")
         return idx[:V], adj[:E], (wgt[:E] if wgt is not None else None)

@@ -226,6 +226,11 @@ struct ipg_graph {
     uint64_t* refill_host = nullptr;
     void* refill_stage = nullptr;
     uint64_t refill_stage_bytes = 0;
+    // contents generation (bumped by every refill) and whether the contents
+    // failed validation; engines record the generation at attach and refuse
+    // to run after it changed or while the contents are bad
+    uint64_t generation = 0;
+    bool bad = false;
     ~ipg_graph()
     {
         ipg_dev_free(refill_dev, 64);
@@ -586,6 +591,11 @@ extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_byte
         IPG_TRY(ipg_dev_alloc(&g->refill_stage, V * (uint64_t)idx_bytes));
         g->refill_stage_bytes = V * (uint64_t)idx_bytes;
     }
+    // From here on the old contents are being replaced: engines attached to
+    // them refuse to run (generation), and so does any engine while the new
+    // contents are not validated (bad).
+    g->generation++;
+    g->bad = true;
     // derived data of the old contents
     for (auto& b : g->bins) {
         ipg_dev_free(b.lists, b.bytes);
@@ -648,9 +658,22 @@ extern "C" int ipg_graph_refill_host(ipg_graph* g, const void* idx, int idx_byte
     if (bits & 1) return fail(IPG_EIO, "malformed offsets: row starts must begin at 0, be non-decreasing and not exceed E");
     if (bits & 2) return fail(IPG_EIO, "malformed adjacency: a neighbour id is >= the vertex count");
     g->v.max_out_degree = h[2];
-    g->v.max_in_degree = h[2];
-    if (own_in) IPG_TRY(ipg_graph_build_in(g));  // allocates: directed graphs only
-    if (own_in) return finish_graph_stats(g, 0);
+    // without an in-CSR the in-degrees are the out-degrees only for a graph
+    // whose rows are its in-lists; 0 = unknown, as the loader leaves it
+    g->v.max_in_degree = g->v.directed ? 0 : h[2];
+    if (own_in) {
+        IPG_TRY(ipg_graph_build_in(g));  // allocates: directed graphs only
+        IPG_TRY(finish_graph_stats(g, 0));
+    }
+    g->bad = false;
+    return IPG_OK;
+}
+
+extern "C" int ipg_graph_contents(const ipg_graph* g, uint64_t* generation, int* valid)
+{
+    if (!g) return fail(IPG_EINVAL, "ipg_graph_contents: null graph");
+    if (generation) *generation = g->generation;
+    if (valid) *valid = g->bad ? 0 : 1;
     return IPG_OK;
 }
 

@@ -242,15 +242,16 @@ def have_ref() -> bool:
 
 
 def run_ref(app: str, version: str, graph_path: str, *, threads=1, schedule="static", chunk=0,
-            id_bits=32, rounds=10, env=None, timeout=600):
+            id_bits=32, rounds=10, env=None, timeout=600, dump=True):
     """Runs a reference binary on graph files; returns (dump text, stdout).
+    dump=False sends the dump to /dev/null and returns "" for it.
 
     argv follows benchmarks/cc.c:75-81 (sssp.c adds a 6th argument, which it
     ignores: its source vertex is atoi(argv[4]) of the schedule string, i.e. 0,
     sssp.c:94-101)."""
     exe = ref_binary(app, version, id_bits, rounds)
     with tempfile.TemporaryDirectory() as td:
-        out = os.path.join(td, "out.txt")
+        out = os.path.join(td, "out.txt") if dump else os.devnull
         argv = [exe, graph_path, out, str(threads), schedule, str(chunk)]
         if app == "sssp":
             argv.append("0")
@@ -260,5 +261,21 @@ def run_ref(app: str, version: str, graph_path: str, *, threads=1, schedule="sta
         p = subprocess.run(argv, capture_output=True, text=True, env=e, timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError(f"{exe} failed ({p.returncode}): {p.stdout[-2000:]}")
+        if not dump:
+            return "", p.stdout
         with open(out) as f:
             return f.read(), p.stdout
+
+
+def parse_dump_fast(text: str, V: int, dtype=np.uint32):
+    """Values of an integer dump ("%u: %u" per line, cc.c:65-68 / sssp.c:81-84)
+    in vertex order, vectorised for dumps of millions of lines."""
+    nums = np.array(text.replace(":", " ").split(), dtype=np.uint64)
+    if nums.size != 2 * V:
+        raise ValueError(f"dump has {nums.size // 2} lines, expected {V}")
+    ids, vals = nums[0::2], nums[1::2]
+    out = np.zeros(V, dtype=dtype)
+    out[ids] = vals.astype(dtype)
+    if not np.array_equal(np.sort(ids), np.arange(V, dtype=np.uint64)):
+        raise ValueError("dump does not list every vertex once")
+    return out

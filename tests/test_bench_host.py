@@ -74,10 +74,68 @@ def test_clock_sampler_without_gpu_reports_unavailable():
 
 
 @pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built")
-def test_reference_sample_timing():
+def test_reference_run_and_dump_parsing():
     g = O.gen_rmat(12, 16, seed=1, undirected=True)
     with tempfile.TemporaryDirectory() as td:
         p = os.path.join(td, "g")
         O.write_graph(g, p)
-        secs, threads = bench.run_reference_sample(p, g.E, 1)
-    assert secs > 0 and threads >= 1
+        secs, text, out = bench.reference_run("cc", p, 2, dump=True)
+        secs2, text2, _ = bench.reference_run("sssp", p, 2, dump=False)
+    assert secs > 0 and secs2 > 0 and text2 is None
+    want, counts, _ = O.run(g, "cc", "spread")
+    assert (O.parse_dump_fast(text, g.V) == want).all()
+    assert O.parse_counts(out) == [int(c) for c in counts]
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built")
+def test_reference_arm_maps_no_repo_library():
+    """The reference arm times the reference's binaries on a graph from the
+    oracle's CPU generator: its process maps none of this repository's
+    CUDA libraries, and its JSON line names the workload it ran."""
+    import json
+    import subprocess
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--scale', '11', '--steps', '2', "
+            "'--warmup', '1']; sys.path.insert(0, %r); import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'mapped': [m for m in ('libipregel_b200', 'app_') if m in maps]}))" % ROOT)
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(x) for x in p.stdout.splitlines() if x.startswith("{")]
+    line, maps = lines[0], lines[1]
+    assert maps["mapped"] == []
+    assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 2
+    assert "scale 11" in line["config"]["workload"] and line["cpu_baseline"]["kind"] == "reference"
+    assert set(line["per_program"]) == {"cc", "sssp"}
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference binaries not built")
+def test_parity_check_against_reference_dumps():
+    """bench.parity_check passes results equal to the reference's and the
+    oracle's, and fails when one label, one hop distance, one weighted
+    distance or one count differs."""
+    import numpy as np
+    g = O.add_weights(O.gen_rmat(11, 16, seed=2, undirected=True), wmax=255, seed=3)
+    dumps = {}
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "g")
+        O.write_graph(g, p)
+        for app in ("cc", "sssp"):
+            _, text, out = bench.reference_run(app, p, 2, dump=True)
+            dumps[app] = (text, out)
+    cc, ccn, _ = O.run(g, "cc", "spread")
+    hop, hopn, _ = O.run(g, "sssp", "spread")
+    w = O.dijkstra(g, 0)
+    args = (g.V, g.E, g.idx, g.adj, g.wgt)
+    good = bench.parity_check(*args, cc, list(ccn), w, hop, list(hopn), dumps)
+    assert good["ok"] and good["cc"]["against"].startswith("reference")
+    assert bench.parity_check(*args, cc, list(ccn), w, hop, list(hopn), {})["ok"]  # oracle fallback
+    bad_cc = cc.copy()
+    bad_cc[5] += 1
+    assert not bench.parity_check(*args, bad_cc, list(ccn), w, hop, list(hopn), dumps)["ok"]
+    bad_hop = hop.copy()
+    bad_hop[-1] ^= 1
+    assert not bench.parity_check(*args, cc, list(ccn), w, bad_hop, list(hopn), dumps)["ok"]
+    bad_w = w.copy()
+    bad_w[np.argmax(w != 0xFFFFFFFF)] += 1
+    assert not bench.parity_check(*args, cc, list(ccn), bad_w, hop, list(hopn), dumps)["ok"]
+    assert not bench.parity_check(*args, cc, list(ccn)[:-1], w, hop, list(hopn), dumps)["ok"]

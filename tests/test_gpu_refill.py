@@ -170,3 +170,52 @@ def test_refill_on_a_thread_while_another_graph_runs():
         sp.release()
         for gr in gbuf:
             gr.free()
+
+
+def test_run_refuses_stale_attach_and_bad_contents():
+    """An engine attached before a refill refuses to run until it attaches
+    again (its degree classes and in-list pointers belong to the old
+    contents); after a failed refill every attach and run refuses until a
+    refill succeeds."""
+    import ipregel_b200 as ip
+    a = O.gen_rmat(11, 16, seed=12, undirected=False)
+    b = _relabel(a, seed=5)
+    g = ip.Graph.from_csr(a.V, a.E, a.idx, a.adj, directed=True, need_in=True)
+    pr = ip.Engine("pagerank", "single_broadcast")
+    cc = ip.Engine("cc", "spread")
+    try:
+        for eng in (pr, cc):
+            eng.set_quiet(True)
+            eng.attach(g)
+        gen0, ok = g.contents()
+        assert ok
+        g.refill(b.idx, b.adj)
+        gen1, ok = g.contents()
+        assert ok and gen1 == gen0 + 1
+        for eng in (pr, cc):
+            with pytest.raises(ip.IPregelError, match="attach it again"):
+                eng.run_only()
+        pr.attach(g)
+        res = pr.run()
+        want, counts, _ = O.run(b, "pagerank", "single_broadcast", directed=True)
+        _check(res, want, counts, fp=True)
+
+        bad = b.adj.copy()
+        bad[7] = b.V
+        with pytest.raises(ip.IPregelError, match="neighbour id"):
+            g.refill(b.idx, bad)
+        assert g.contents() == (gen1 + 1, False)
+        with pytest.raises(ip.IPregelError, match="failed validation"):
+            pr.run_only()
+        with pytest.raises(ip.IPregelError, match="failed validation"):
+            cc.attach(g)
+        g.refill(a.idx, a.adj)
+        assert g.contents() == (gen1 + 2, True)
+        cc.attach(g)
+        res = cc.run()
+        want, counts, _ = O.run(a, "cc", "spread", directed=True)
+        _check(res, want, counts)
+    finally:
+        pr.release()
+        cc.release()
+        g.free()
