@@ -51,6 +51,8 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true", help="skip the check of the results against the reference")
+    p.add_argument("--write-traffic", nargs=2, metavar=("NCU_CSV", "BENCH_LINE"),
+                   help="write profiles/traffic.json from an ncu launch list and the bench line of the same command")
     p.add_argument("--no-extra", action="store_true",
                    help="skip the PageRank precision-split, batched and serving workloads")
     p.add_argument("--rows", default="",
@@ -294,7 +296,7 @@ def reference_arm(args, rank, world):
     return 0
 
 
-def pagerank_row(peak):
+def pagerank_row(peak, check_oracle=True):
     """PageRank precision split on directed R-MAT scale 25, 30 rounds: FP32
     compensated pull (ipg_pr_run_f32) against the FP64 engine (pagerank,
     single broadcast), per-vertex error of FP32 against FP64 on the GPU."""
@@ -330,12 +332,35 @@ def pagerank_row(peak):
     for _ in range(2):
         eng.run_only()
         ms64.append(eng.stats()[0] * 1e3)
+    eng_counts = eng.counts()
     ptr = ctypes.c_void_p()
     eng._check(eng.lib.ipg_app_values_device(ctypes.byref(ptr)), "ipg_app_values_device")
     err = ip.error_f32_f64(x, ip.DeviceArray.wrap(ptr.value, V, np.float64))
+    v64 = eng.values()
+    v32 = x.to_host()
     eng.set_graph_loop(False)
     eng.set_param("rounds", 10)
     eng.release()
+    # both against the FP64 CPU oracle (pagerank single_broadcast, the same
+    # 30 rounds on the same CSR), outside the timed runs
+    vs_oracle = None
+    if check_oracle:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        t_chk = time.time()
+        idx, adj, _ = g.to_host()
+        want, counts, _ = O.run(O.CSR(V, E, idx, adj), "pagerank", "single_broadcast", rounds=rounds)
+        del idx, adj
+        a64 = np.abs(v64 - want)
+        a32 = np.abs(v32.astype(np.float64) - want)
+        nz = want != 0
+        vs_oracle = {"fp64_engine_max_abs": float(a64.max()), "fp64_within_1e-12": bool(a64.max() <= 1e-12),
+                     "fp64_counts_equal": [int(c) for c in counts] == eng_counts,
+                     "fp32_max_abs": float(a32.max()),
+                     "fp32_max_rel": float((a32[nz] / want[nz]).max()) if nz.any() else 0.0,
+                     "fp32_mean_abs": float(a32.mean()),
+                     "oracle": "FP64 CPU restatement of pagerank.c's single_broadcast run (oracle/), "
+                               f"{time.time() - t_chk:.0f} s"}
     byts = 8 * E + 24 * V
     achieved = byts / (ms32 / rounds * 1e-3) / 1e9
     launches = launches_per_run_f32(pr.info(), rounds)
@@ -356,6 +381,7 @@ def pagerank_row(peak):
                                     "frac": round(edge_rate / ceil["rows_per_s"], 4) if ceil["rows_per_s"] else None}},
            "fp64_engine": {"ms": round(min(ms64), 3), "gteps": round(E * rounds / (min(ms64) * 1e-3) / 1e9, 2)},
            "fp32_vs_fp64": {k: (float(f"{v:.4g}") if isinstance(v, float) else v) for k, v in err.items()},
+           "vs_fp64_cpu_oracle": vs_oracle,
            "fp64_diagnostics_last": {"mass": float(diag[-1, 0]), "dangling": float(diag[-1, 1]),
                                      "residual_l1": float(diag[-1, 2])}}
     x.free()
@@ -436,6 +462,12 @@ def serving_row():
         runs.append((S.summarize(lat, mk, tr.kind), clk))
     runs.sort(key=lambda r: r[0]["qps"])
     summ, clk = runs[1]
+    # below capacity: arrivals at about half the served rate, so that the
+    # percentiles are service latencies rather than queueing
+    low_rate = 150.0
+    tr_low = S.poisson_trace(600, low_rate, sizes, seed=2)
+    _, lat_low, mk_low = srv.run_trace(tr_low)
+    low = S.summarize(lat_low, mk_low, tr_low.kind)
     st = srv.stats()
     # device time, supersteps and lanes per lane-group kind and graph scale
     groups = {}
@@ -482,14 +514,19 @@ def serving_row():
                             f"(sssp_weighted/spread, ppr/single_broadcast FP64, cc/spread), graph attached "
                             f"once per graph, device loop time only",
             "speedup_vs_plain": round(summ["qps"] / plain_qps, 2),
-            "counters_cover": "the 64-query warm-up trace and the three runs",
+            "counters_cover": "the 64-query warm-up trace, the three runs and the unsaturated trace",
             "groups": groups,
             "groups_note": "per graph scale (two graphs each) and group kind: summed superstep device time "
                            "(concurrent groups overlap), supersteps, lanes admitted; PPR: mean busy lanes of 32",
             "lanes_admitted": st["lanes_admitted"], "supersteps": st["supersteps"],
             "kernel_launches": st["kernel_launches"], "pull_supersteps": st["pull_supersteps"],
             "peak_hbm_bytes": st["peak_bytes"], "hbm_free_before_trace": free_b, "clocks_during_trace": clk,
-            "note": "arrivals exceed capacity: latency includes queueing"}
+            "note": "arrivals exceed capacity: latency includes queueing",
+            "unsaturated": {"workload": f"600 queries of the same mix, Poisson {low_rate:.0f}/s (below the served "
+                                        f"rate), seed 2", "served_qps": round(low["qps"], 1),
+                            "p50_ms": round(low["p50_ms"], 2), "p99_ms": round(low["p99_ms"], 2),
+                            "per_kind_ms": {k: round(v, 2) for k, v in low.items()
+                                            if k.endswith("_ms") and "_" in k[:-3]}}}
 
 
 def same_work_row(args, cc, g, E, world, barrier, max_over_ranks):
@@ -592,8 +629,107 @@ def parity_check(V, E, idx, adj, wgt, res_cc, counts_cc, res_sp, res_hop, counts
     return {"ok": ok, **out, "check_s": round(time.time() - t, 1)}
 
 
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
+# The kernel sources a DRAM capture describes: the engine headers and the
+# runtime's kernels.  A capture of other sources says nothing about these.
+KERNEL_SOURCES = ("include/ipregel_b200/engine.cuh", "include/ipregel_b200/host.cuh",
+                  "include/ipregel_b200/api.cuh", "ipregel_b200/csrc/runtime.cu")
+
+
+def kernel_sources_sha16():
+    import hashlib
+    h = hashlib.sha256()
+    for rel in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def stored_traffic(name, bytes_per_launch):
+    """roofline.traffic from profiles/traffic.json: the DRAM bytes per
+    algorithmic byte that one ncu capture measured for this kernel, times
+    this launch's algorithmic bytes -- only when that capture ran the same
+    kernel sources as this build (else null, with the reason)."""
+    try:
+        d = json.load(open(TRAFFIC_PATH))
+    except Exception:
+        return {"traffic": None, "traffic_source": "no DRAM capture stored (profiles/traffic.json)"}
+    if d.get("_kernel_sources_sha16") != kernel_sources_sha16():
+        return {"traffic": None,
+                "traffic_source": "the stored DRAM capture (profiles/traffic.json) ran other kernel sources "
+                                  "than this build"}
+    tr = d.get(name)
+    if not tr:
+        return {"traffic": None, "traffic_source": f"no DRAM capture of {name} stored"}
+    return {"traffic": round(tr["dram_bytes_per_algorithmic_byte"] * bytes_per_launch),
+            "traffic_source": "scaled, not measured by this run: DRAM/algorithmic bytes of this kernel in an ncu "
+                              "capture of the same kernel sources (" + tr["source"] + "), times this launch's "
+                              "algorithmic bytes"}
+
+
+NCU_KERNEL_NAMES = (("ipx_k_push<0>", "push_thread"), ("ipx_k_push<1>", "push_warp"), ("ipx_k_push<2>", "push_block"),
+                    ("ipx_k_compute_spread", "compute"))
+
+
+def write_traffic(csv_path, line_path, out_path=TRAFFIC_PATH):
+    """profiles/traffic.json from an ncu launch list (--metrics
+    gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --csv)
+    of `bench.py --steps 1 --warmup 1 --no-e2e --no-cpu-baseline --no-extra
+    --no-parity` and the JSON line of the same command run without ncu (its
+    `kernels` give the algorithmic bytes).  The profiled step runs CC, then
+    SSSP, each superstep opening with ipx_k_begin_superstep; k_compact
+    launches alternate broadcasters / next frontier within a superstep."""
+    import csv
+    line = json.loads(open(line_path).read().strip().splitlines()[-1])
+    steps_cc = line["kernels"]["cc:compute"]["launches"]
+    rows = [r for r in csv.DictReader(l for l in open(csv_path) if not l.startswith("=="))]
+    launches = {}
+    for r in rows:
+        launches.setdefault(r["ID"], {"name": r["Kernel Name"]})[r["Metric Name"]] = float(r["Metric Value"].replace(",", ""))
+    order = [launches[k] for k in sorted(launches, key=int)]
+    # the profiled step: the last 2 runs' host-loop launches, from the first
+    # begin_superstep of its CC run
+    begins = [i for i, x in enumerate(order) if x["name"].startswith("ipx_k_begin_superstep")]
+    steps_sp = line["kernels"]["sssp:compute"]["launches"]
+    begins = begins[-(steps_cc + steps_sp):]
+    dram, seen = {}, {}
+    for j, b in enumerate(begins):
+        prog = "cc" if j < steps_cc else "sssp"
+        end = begins[j + 1] if j + 1 < len(begins) else len(order)
+        compacts = 0
+        for x in order[b:end]:
+            nm = x["name"]
+            key = None
+            for pref, short in NCU_KERNEL_NAMES:
+                if nm.startswith(pref):
+                    key = short
+            if nm.startswith("k_compact"):
+                key = "compact_broadcasters" if compacts == 0 else "compact_targets"
+                compacts += 1
+            if key is None:
+                continue
+            k = f"{prog}:{key}"
+            dram[k] = dram.get(k, 0.0) + x.get("dram__bytes_read.sum", 0.0) + x.get("dram__bytes_write.sum", 0.0)
+            seen[k] = seen.get(k, 0) + 1
+    out = {"_kernel_sources_sha16": kernel_sources_sha16()}
+    for k, b in sorted(dram.items(), key=lambda kv: -kv[1]):
+        alg = line["kernels"].get(k, {}).get("bytes")
+        if not alg:
+            continue
+        out[k] = {"dram_bytes_per_algorithmic_byte": round(b / alg, 4), "launches": seen[k], "dram_bytes": int(b),
+                  "algorithmic_bytes": int(alg),
+                  "source": f"ncu 1-pass dram__bytes_read.sum + dram__bytes_write.sum over one profiled CC + SSSP "
+                            f"step, R-MAT scale {line['config'].get('scale', 24)}"}
+    with open(out_path, "w") as f:
+        json.dump(out, f, indent=1)
+    return out
+
+
 def main():
     args = parse_args()
+    if args.write_traffic:
+        print(json.dumps(write_traffic(*args.write_traffic), indent=1))
+        return 0
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -702,15 +838,7 @@ def main():
                        "(the 4-byte mailbox), ipg_measure_gather",
             "rows_per_s": round(ceil["rows_per_s"] / 1e9, 2), "kernel_edges_per_s": round(rate / 1e9, 2),
             "unit": "G/s", "frac": round(rate / ceil["rows_per_s"], 4) if ceil["rows_per_s"] else None}
-    traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(traffic_path):
-        try:
-            tr = json.load(open(traffic_path)).get(top_name)
-            if tr:
-                roofline["traffic"] = round(tr["dram_bytes_per_algorithmic_byte"] * bytes_per_launch)
-                roofline["traffic_source"] = tr["source"]
-        except Exception:
-            pass
+    roofline.update(stored_traffic(top_name, bytes_per_launch))
 
     # ---- the same work as the reference arm: CC + hop-count SSSP ----
     same_work, res_hop, counts_hop = same_work_row(args, cc, g, E, world, barrier, max_over_ranks)
@@ -820,7 +948,8 @@ def main():
     # ---- the other workloads (one GPU only; each frees what it held) ----
     extra = {}
     if world == 1 and not args.no_extra:
-        rows = (("pagerank_precision_split", lambda: pagerank_row(peak)), ("batched_many_graph", batch_row),
+        rows = (("pagerank_precision_split", lambda: pagerank_row(peak, not args.no_parity)),
+                ("batched_many_graph", batch_row),
                 ("serving", serving_row))
         wanted = set(args.rows.split(",")) if args.rows else None
         for name, fn in rows:
@@ -838,7 +967,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": f"cc (spread) + weighted sssp from 0 (spread, atomicMin), undirected R-MAT "
                                    f"scale {scale}, edge factor 16, a/b/c=0.57/0.19/0.19, seed 1, weights U[1,255]",
-                       "vertices": V, "edges_stored": E, "parallelism": f"replicas x{world}",
+                       "scale": scale, "vertices": V, "edges_stored": E, "parallelism": f"replicas x{world}",
                        "superstep_loop": "captured CUDA graph with a device-evaluated while condition",
                        "teps": "Graph500: stored edges x runs / time",
                        "l2": "inputs (3.8 GB) larger than L2; no flush",
@@ -853,7 +982,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
-            "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+            "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3), "bytes": round(v["bytes"]),
                             "gbs": round(v["bytes"] / (v["ms"] * 1e-3) / 1e9, 1) if v["ms"] else None}
                         for k, v in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])},
         }

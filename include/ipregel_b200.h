@@ -246,16 +246,6 @@ int ipg_bitmap_popc_or(const uint32_t* d_a, const uint32_t* d_b, uint64_t nwords
 /* SM count of the current device (cached). */
 int ipg_sm_count(void);
 
-/* The random-gather ceiling -- no counterpart in the reference.  Times n
- * reads of `row_bytes`-byte rows (4; or 64, 128, 256 read as 16-byte quads
- * by 4, 8, 16 consecutive threads) at pseudo-random positions of a table of `table_bytes`, each
- * position taken from a coalesced u32 index stream: the access pattern of
- * the push prechecks and of the pull gathers, with nothing else.  Returns
- * rows read per second and (index + row) bytes per second in GB/s, averaged
- * over `reps` launches after one warm-up launch.  Allocates n * 4 +
- * table_bytes of device memory for the call; synchronous. */
-int ipg_measure_gather(uint64_t table_bytes, uint32_t row_bytes, uint64_t n, int reps, double* rows_per_s,
-                       double* gbs);
 
 /* ------------------------------------------------------------------------
  * PageRank precision split -- no counterpart in the reference, whose

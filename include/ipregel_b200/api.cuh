@@ -113,8 +113,13 @@ struct ip_vertex_t;
 struct ip_vertex_t* ip_all_vertices = NULL;
 int ip_thread_count;
 
-/* Device mirrors read by ip_compute through the same accessor names. */
+/* Device mirrors read by ip_compute through the same accessor names.
+ * ipd_superstep is the superstep the engine's kernels are in;
+ * ipd_compute_superstep the one whose compute phase runs, which ip_compute
+ * sees: the same, except in the single_broadcast version, whose fused kernel
+ * gathers superstep s's broadcasts and runs the compute phase of s+1. */
 __device__ size_t ipd_superstep;
+__device__ size_t ipd_compute_superstep;
 __device__ size_t ipd_vertices_count;
 __device__ size_t ipd_edges_count;
 
@@ -161,7 +166,7 @@ extern "C" {
 __host__ __device__ size_t ip_get_superstep()
 {
 #ifdef __CUDA_ARCH__
-    return __ldg((const unsigned long long*)&ipd_superstep);
+    return __ldg((const unsigned long long*)&ipd_compute_superstep);
 #else
     return ip_superstep;
 #endif

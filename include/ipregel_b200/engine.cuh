@@ -18,8 +18,9 @@
  *   received[2]                    push: bitmap of mailboxes that got mail
  *   outbox[V] + broadcaster bitmap push: ip_broadcast records here; delivery
  *                                  is a separate edge-parallel kernel
- *   bval[V] + has_bcast bitmap     pull: the externalised broadcast slot of
- *                                  combiner_single_broadcast_preamble.h:42-50
+ *   bslot[V]                       pull: the externalised broadcast slot of
+ *                                  combiner_single_broadcast_preamble.h:42-50,
+ *                                  {message, superstep stamp} in 8 or 16 bytes
  * Messages become visible only at the next superstep in every version
  * (combiner_postamble.h:168-183), so recording broadcasts in an outbox and
  * delivering them after the compute kernel gives the reference's results;
@@ -88,6 +89,7 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 #define IPX_ERR_SEND_IN_BROADCAST 1u
 #define IPX_ERR_COMBINE_HINT 2u
 #define IPX_ERR_SUPERSTEP_LIMIT 4u
+#define IPX_ERR_COPY_TIMEOUT 8u
 #define IPX_HIST 65536
 
 /* Default degree-class thresholds for the thread / warp / block kernels
@@ -465,6 +467,49 @@ typedef ipx_mailbox<IP_COMBINE_KIND, (int)sizeof(ipx_msg)> ipx_mb;
 typedef typename ipx_mb::slot ipx_slot;
 
 /* ------------------------------------------------------------------------ */
+/* Pull broadcast slot.  The reference keeps {has_broadcast, message} per    */
+/* vertex (combiner_single_broadcast_preamble.h:42-50) and clears the flags  */
+/* every superstep.  Here a slot holds the message's bits and the superstep  */
+/* in which it was broadcast: it counts in superstep s iff its stamp is s,   */
+/* so no slot is ever cleared, and a gathered edge costs one 8-byte (message */
+/* up to 4 bytes) or 16-byte (up to 8 bytes) load -- one L2 request -- where */
+/* a flag bitmap costs a dependent bitmap-word load before the value.        */
+/* ------------------------------------------------------------------------ */
+typedef typename std::conditional<(sizeof(ipx_msg) <= 4), uint2, uint4>::type ipx_bslot;
+/* Stamp of a slot that holds no broadcast (all bytes 0xff after a reset);
+ * supersteps stay below it (ipx_max_supersteps). */
+#define IPX_NO_STAMP 0xffffffffu
+
+__device__ __forceinline__ void ipx_bslot_store(uint2* p, unsigned long long w, uint32_t stamp)
+{
+    *p = make_uint2((uint32_t)w, stamp);
+}
+__device__ __forceinline__ void ipx_bslot_store(uint4* p, unsigned long long w, uint32_t stamp)
+{
+    *p = make_uint4((uint32_t)w, (uint32_t)(w >> 32), stamp, 0u);
+}
+__device__ __forceinline__ unsigned long long ipx_bslot_bits(const uint2& w) { return w.x; }
+__device__ __forceinline__ unsigned long long ipx_bslot_bits(const uint4& w)
+{
+    return ((unsigned long long)w.y << 32) | w.x;
+}
+__device__ __forceinline__ uint32_t ipx_bslot_stamp(const uint2& w) { return w.y; }
+__device__ __forceinline__ uint32_t ipx_bslot_stamp(const uint4& w) { return w.z; }
+
+__device__ __forceinline__ void ipx_bslot_put(ipx_bslot* p, const ipx_msg& m, uint32_t stamp)
+{
+    ipx_bslot_store(p, (unsigned long long)ipx_to_word(m), stamp);
+}
+
+/* The message of a loaded slot; true when it was broadcast in superstep
+ * `stamp`. */
+__device__ __forceinline__ bool ipx_bslot_take(const ipx_bslot& w, uint32_t stamp, ipx_msg& m)
+{
+    m = ipx_from_word<ipx_msg>((typename ipx_word<ipx_msg>::type)ipx_bslot_bits(w));
+    return ipx_bslot_stamp(w) == stamp;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Device-resident engine state, read through the constant bank.            */
 /* ------------------------------------------------------------------------ */
 struct ipx_consts {
@@ -488,9 +533,10 @@ struct ipx_consts {
     uint32_t* recv[2];
     ipx_msg* outbox;
     uint32_t* bcaster;
-    /* pull broadcast slots */
-    ipx_msg* bval;
-    uint32_t* has_b;
+    /* pull broadcast slots: single_broadcast alternates bslot[s & 1] (its
+     * fused kernel reads superstep s's slots while writing s+1's);
+     * spread+single_broadcast uses bslot[0] */
+    ipx_bslot* bslot[2];
     uint32_t* bt;
     /* counters: [0..3] active counts ring, [4] edges, [5] error word */
     unsigned long long* ctr;
@@ -502,6 +548,10 @@ struct ipx_consts {
      * active count, edges traversed, direction, unused */
     uint32_t* lcnt;
     unsigned long long* hist;
+    /* single_broadcast hub chunks: per chunk the partial fold ({message,
+     * has} in a slot, has in the stamp word), per hub the chunks arrived */
+    ipx_bslot* hub_part;
+    uint32_t* hub_arrived;
 };
 
 __constant__ ipx_consts ipx_c;
@@ -680,6 +730,38 @@ struct ipx_push_visit {
             if (go[k] && ipx_mb::commit(&ipx_c.mbox[p][t], mk[k])) atomicOr(&ipx_c.recv[p][t >> 5], 1u << (t & 31));
         }
     }
+    /* Four consecutive edges e0 .. e0+3 (e0 a multiple of 4) whose ids one
+     * 128-bit load gave; 4-byte weights come the same way. */
+    __device__ __forceinline__ void batch_v4(uint64_t e0, const uint4& id, const ipx_msg& m) const
+    {
+        const uint32_t w[4] = {id.x, id.y, id.z, id.w};
+        ipx_msg mk[4];
+#if IPX_EDGE_MSG
+        if constexpr (sizeof(ipx_wgt) == 4) {
+            const uint4 ww = __ldcs(reinterpret_cast<const uint4*>(ipx_c.wgt + e0));
+            const uint32_t wk[4] = {ww.x, ww.y, ww.z, ww.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                ipx_wgt x;
+                memcpy(&x, &wk[k], 4);
+                mk[k] = IP_BROADCAST_EDGE_MESSAGE(m, x);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) mk[k] = IP_BROADCAST_EDGE_MESSAGE(m, ipx_ld_stream(&ipx_c.wgt[e0 + k]));
+        }
+#else
+        (void)e0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) mk[k] = m;
+#endif
+        bool go[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) go[k] = ipx_mb::precheck(&ipx_c.mbox[p][w[k]], mk[k]);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (go[k] && ipx_mb::commit(&ipx_c.mbox[p][w[k]], mk[k])) atomicOr(&ipx_c.recv[p][w[k] >> 5], 1u << (w[k] & 31));
+    }
 };
 
 /* Target-marking visitor (spread+single_broadcast). */
@@ -699,14 +781,69 @@ struct ipx_mark_visit {
             if (!(cur[k] & bit)) atomicOr(&ipx_c.bt[(uint64_t)w[k] >> 5], bit);
         }
     }
+    __device__ __forceinline__ void batch_v4(uint64_t e0, const uint4& id, const ipx_msg& m) const
+    {
+        const uint64_t e[4] = {e0, e0 + 1, e0 + 2, e0 + 3};
+        const ipx_vid w[4] = {(ipx_vid)id.x, (ipx_vid)id.y, (ipx_vid)id.z, (ipx_vid)id.w};
+        const ipx_msg mk[4] = {m, m, m, m};
+        const bool ok[4] = {true, true, true, true};
+        batch<4>(e, w, mk, ok);
+    }
 };
 
+/* Edges [e0, e1) of one source visited by a warp or block (lanes >= 32)
+ * with 32-bit ids: the ids of four consecutive edges per lane come from one
+ * 128-bit load (the weights too, when the visitor needs 4-byte weights),
+ * the up to 3 edges before the first 16-byte boundary and after the last one
+ * take a lane each. */
+template <class Visit>
+__device__ __forceinline__ void ipx_edges_v4(const uint32_t* __restrict__ adj, uint64_t e0, uint64_t e1,
+                                             uint64_t lane, uint64_t lanes, ipx_msg m, const Visit& visit)
+{
+    uint64_t a = (e0 + 3) & ~3ULL;
+    if (a > e1) a = e1;
+    const uint64_t b = a + ((e1 - a) & ~3ULL);
+    {
+        const uint64_t nh = a - e0, nt = e1 - b;
+        uint64_t e = e1;
+        if (lane < nh) e = e0 + lane;
+        else if (lane < nh + nt) e = b + (lane - nh);
+        const uint64_t ek[1] = {e};
+        const bool ok[1] = {e < e1};
+        const ipx_vid w[1] = {ok[0] ? (ipx_vid)ipx_ld_stream(&adj[e]) : (ipx_vid)0};
+        const ipx_msg mk[1] = {m};
+        visit.template batch<1>(ek, w, mk, ok);
+    }
+    const uint4* __restrict__ q = reinterpret_cast<const uint4*>(adj + a);
+    const uint64_t groups = (b - a) >> 2;
+    for (uint64_t g = lane; g < groups; g += lanes) visit.batch_v4(a + 4 * g, __ldcs(q + g), m);
+}
+
+/* The 128-bit path needs 16-byte aligned id and weight arrays (always so for
+ * arrays the runtime allocates; a caller's array may not be). */
+__device__ __forceinline__ bool ipx_v4_ok(const void* adj)
+{
+    if constexpr (sizeof(ipx_vid) != 4) return false;
+    if ((reinterpret_cast<uintptr_t>(adj) & 15) != 0) return false;
+#if IPX_EDGE_MSG
+    if ((reinterpret_cast<uintptr_t>(ipx_c.wgt) & 15) != 0) return false;
+#endif
+    return true;
+}
+
 /* Visits edges [e0, e1) of one source lane-strided, IPX_UNROLL edges a lane
- * at a time, loading the ids of a batch before visiting any of it. */
+ * at a time, loading the ids of a batch before visiting any of it (warps and
+ * blocks over 32-bit ids: ipx_edges_v4). */
 template <class Visit>
 __device__ __forceinline__ void ipx_edges_strided(const ipx_vid* __restrict__ adj, uint64_t e0, uint64_t e1,
                                                   uint64_t lane, uint64_t lanes, ipx_msg m, const Visit& visit)
 {
+    if constexpr (sizeof(ipx_vid) == 4) {
+        if (lanes >= 32 && ipx_v4_ok(adj)) {
+            ipx_edges_v4(reinterpret_cast<const uint32_t*>(adj), e0, e1, lane, lanes, m, visit);
+            return;
+        }
+    }
     for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
         uint64_t ek[IPX_UNROLL];
         ipx_vid w[IPX_UNROLL];
@@ -1032,31 +1169,82 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
 
 /* Folds the broadcasts of the in-neighbours at edges e0 + lane, e0 + lane +
  * lanes, ... below e1, in that order.  IPX_UNROLL edges a step: their ids,
- * then their broadcast bits, then the values of the set bits are each loaded
- * for all IPX_UNROLL edges before the next level, so a lane has IPX_UNROLL
- * independent loads in flight instead of one three-load chain per edge. */
-__device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict__ adj, const uint32_t* __restrict__ hb,
-                                                      const ipx_msg* __restrict__ bv, uint64_t e0, uint64_t e1,
-                                                      uint64_t lane, uint64_t lanes, bool& has, ipx_msg& acc)
+ * then their broadcast slots are each loaded for all IPX_UNROLL edges before
+ * any is folded, so a lane has IPX_UNROLL independent slot loads in flight.
+ * A warp or block (lanes >= 32) with 32-bit ids reads the ids 128 bits at a
+ * time instead: four consecutive in-edges per lane and load instruction
+ * (ipx_gather_fold_edges_v4). */
+__device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restrict__ adj,
+                                                         const ipx_bslot* __restrict__ bs, uint32_t stamp,
+                                                         uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
+                                                         bool& has, ipx_msg& acc)
 {
+    /* [e0, a): up to 3 edges before the first 16-byte boundary; [a, b): whole
+     * groups of four; [b, e1): up to 3 edges after.  The 6 or fewer edges of
+     * both ends take one lane each (lanes >= 32). */
+    uint64_t a = (e0 + 3) & ~3ULL;
+    if (a > e1) a = e1;
+    const uint64_t b = a + ((e1 - a) & ~3ULL);
+    {
+        const uint64_t nh = a - e0, nt = e1 - b;
+        uint64_t e = e1;
+        if (lane < nh) e = e0 + lane;
+        else if (lane < nh + nt) e = b + (lane - nh);
+        if (e < e1) {
+            const ipx_bslot w = __ldg(&bs[adj[e]]);
+            ipx_msg m;
+            if (ipx_bslot_take(w, stamp, m)) ipx_fold(has, acc, true, m);
+        }
+    }
+    const uint4* __restrict__ q = reinterpret_cast<const uint4*>(adj + a);
+    const uint64_t groups = (b - a) >> 2;
+    for (uint64_t g = lane; g < groups; g += lanes) {
+        const uint4 id = __ldcs(q + g);
+        ipx_bslot w[4];
+        w[0] = __ldg(&bs[id.x]);
+        w[1] = __ldg(&bs[id.y]);
+        w[2] = __ldg(&bs[id.z]);
+        w[3] = __ldg(&bs[id.w]);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            ipx_msg m;
+            if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+        }
+    }
+}
+
+__device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict__ adj,
+                                                      const ipx_bslot* __restrict__ bs, uint32_t stamp, uint64_t e0,
+                                                      uint64_t e1, uint64_t lane, uint64_t lanes, bool& has,
+                                                      ipx_msg& acc)
+{
+    if constexpr (sizeof(ipx_vid) == 4) {
+        /* the vector path needs a 16-byte aligned id array (always so for
+         * arrays the runtime allocates; a caller's array may not be) */
+        if (lanes >= 32 && (reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
+            ipx_gather_fold_edges_v4(reinterpret_cast<const uint32_t*>(adj), bs, stamp, e0, e1, lane, lanes, has, acc);
+            return;
+        }
+    }
     for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
         uint64_t u[IPX_UNROLL];
-        uint32_t word[IPX_UNROLL];
-        bool on[IPX_UNROLL];
-        ipx_msg m[IPX_UNROLL];
+        ipx_bslot w[IPX_UNROLL];
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++)
             u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_edge(&adj[e + k * lanes], lanes) : 0;
 #pragma unroll
-        for (int k = 0; k < IPX_UNROLL; k++) word[k] = (e + k * lanes < e1) ? __ldg(&hb[u[k] >> 5]) : 0u;
-#pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
-            on[k] = (word[k] >> (u[k] & 31)) & 1u;
-            if (on[k]) m[k] = __ldg(&bv[u[k]]);
+            if (e + k * lanes < e1) {
+                w[k] = __ldg(&bs[u[k]]);
+            } else {
+                memset(&w[k], 0xff, sizeof w[k]); /* no broadcast */
+            }
         }
 #pragma unroll
-        for (int k = 0; k < IPX_UNROLL; k++)
-            if (on[k]) ipx_fold(has, acc, true, m[k]);
+        for (int k = 0; k < IPX_UNROLL; k++) {
+            ipx_msg m;
+            if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+        }
     }
 }
 
@@ -1070,8 +1258,8 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
     const uint64_t n = count_dev ? (uint64_t)*count_dev : count_host;
     const ipx_vid* __restrict__ adj = ipx_c.in_adj;
     const uint64_t* __restrict__ row = ipx_c.in_row;
-    const uint32_t* __restrict__ hb = ipx_c.has_b;
-    const ipx_msg* __restrict__ bv = ipx_c.bval;
+    const ipx_bslot* __restrict__ bs = ipx_c.bslot[0];
+    const uint32_t stamp = (uint32_t)ipx_step();
     unsigned long long react = 0;
     if constexpr (MODE == 0) {
         /* the next vertex's list entry is loaded while this vertex's
@@ -1082,7 +1270,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t vn = (i + stride < n) ? list[i + stride] : 0;
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], 0, 1, has, acc);
+            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], 0, 1, has, acc);
             ipx_c.hasmsg_b[v] = has;
             if (has) {
                 ipx_c.msg[v] = acc;
@@ -1101,7 +1289,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t v = list[i];
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], lane, 32, has, acc);
+            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], lane, 32, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 ipx_c.hasmsg_b[v] = has;
@@ -1124,7 +1312,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_gather(const
             const uint64_t v = list[i];
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, hb, bv, row[v], row[v + 1], threadIdx.x, blockDim.x, has, acc);
+            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], threadIdx.x, blockDim.x, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 s_has[warp] = has;
@@ -1342,46 +1530,376 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32
     }
 }
 
-/* Single broadcast (pull) compute phase: combiner_single_broadcast_postamble.h:
- * 185-201.  Each warp rewrites whole has_broadcast words, which also clears
- * last superstep's flags. */
-__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb()
+/* Single broadcast (pull), superstep 0's compute phase
+ * (combiner_single_broadcast_postamble.h:185-201): every vertex is active and
+ * has no message.  A broadcast writes the vertex's slot in buffer 0 stamped
+ * 0.  Later supersteps' compute phases run inside ipx_k_gather_compute; this
+ * kernel returns at once after superstep 0, so the same launch sequence
+ * serves every superstep of a captured loop.  The count of superstep 0 is
+ * made by the gather that follows. */
+__global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb0()
 {
-    const int ctr_slot = (int)(ipx_step() & 3);
+    if (ipx_step() != 0) return;
     const uint64_t V = ipx_c.V;
-    const uint64_t Vp = (V + 31) & ~31ULL;
-    const int lane = threadIdx.x & 31;
-    unsigned long long cnt = 0;
-    for (uint64_t v = ipx_gtid(); v < Vp; v += ipx_gstride()) {
-        bool a = (v < V) && ipx_c.active_b[v];
-        bool out = false;
-        if (a) {
-            struct ip_vertex_t x;
-            x.id = (ipx_vid)v;
-            x.active = true;
-            x.has_message = ipx_c.hasmsg_b[v];
-            if (x.has_message) x.message = ipx_c.msg[v];
-            const ipx_val v0 = ipx_c.value[v];
-            x.value = v0;
-            x.ipx_has_out = false;
-            ipx_fill_topology(x, v);
-            ip_compute(&x);
-            if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
-            if (!x.active) ipx_c.active_b[v] = 0;
-            a = x.active;
-            if (x.ipx_has_out) {
-                ipx_c.bval[v] = x.ipx_out;
-                out = true;
+    ipx_bslot* __restrict__ out = ipx_c.bslot[0];
+    for (uint64_t v = ipx_gtid(); v < V; v += ipx_gstride()) {
+        if (!ipx_c.active_b[v]) continue;
+        struct ip_vertex_t x;
+        x.id = (ipx_vid)v;
+        x.active = true;
+        x.has_message = false;
+        const ipx_val v0 = ipx_c.value[v];
+        x.value = v0;
+        x.ipx_has_out = false;
+        ipx_fill_topology(x, v);
+        ip_compute(&x);
+        if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
+        if (!x.active) ipx_c.active_b[v] = 0;
+        if (x.ipx_has_out) ipx_bslot_put(&out[v], x.ipx_out, 0u);
+    }
+}
+
+/* After vertex v's gather of superstep s: whether v is active (it was after
+ * compute(s), or a message reactivates it, :65-71), and if so its compute
+ * phase of superstep s+1 (:185-201) with the gathered message; a broadcast
+ * goes to `out` stamped s+1.  Returns the activity that superstep s counts. */
+__device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const ipx_msg& acc, ipx_bslot* out,
+                                                    uint32_t next_stamp)
+{
+    const bool a0 = ipx_c.active_b[v] != 0;
+    if (!a0 && !has) return false;
+    struct ip_vertex_t x;
+    x.id = (ipx_vid)v;
+    x.active = true;
+    x.has_message = has;
+    if (has) x.message = acc;
+    const ipx_val v0 = ipx_c.value[v];
+    x.value = v0;
+    x.ipx_has_out = false;
+    ipx_fill_topology(x, v);
+    ip_compute(&x);
+    if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
+    if (x.active != a0) ipx_c.active_b[v] = x.active ? 1 : 0;
+    if (x.ipx_has_out) ipx_bslot_put(&out[v], x.ipx_out, next_stamp);
+    return true;
+}
+
+/* ---- bulk copies into shared memory (cp.async.bulk, completed on an
+ * mbarrier; one CTA, no cluster, no multicast) ---- */
+__device__ __forceinline__ uint32_t ipx_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void ipx_mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ipx_smem(bar)) : "memory");
+}
+
+/* The issuing thread's arrival on `bar`, expecting `bytes` from a bulk copy
+ * (0: a plain arrival, which completes the phase). */
+__device__ __forceinline__ void ipx_mbar_arrive_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ipx_smem(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ipx_bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     ipx_smem(dst)),
+                 "l"(src), "r"(bytes), "r"(ipx_smem(bar))
+                 : "memory");
+}
+
+/* Waits for phase `parity` of `bar` to complete, at most `limit` polls. */
+__device__ __forceinline__ bool ipx_mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t k = 0; k < limit; k++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(ipx_smem(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+/* Polls before a wait for a chunk's ids is given up (each try_wait may
+ * suspend the thread for a while): an 8 KB copy lands in microseconds, so
+ * this is reached only if the copy never completes. */
+#define IPX_COPY_WAIT_LIMIT (1u << 22)
+
+/* A hub chunk as thread 0 located it: the vertex, its hub index, the chunk's
+ * edge range [e0, e1) and the 16-byte aligned range [a0, b) copied into
+ * shared memory (b <= a0: nothing copied). */
+struct ipx_hub_chunk {
+    uint64_t v, e0, e1, a0, b;
+    uint64_t i;
+    uint32_t c, c0, nch, pad;
+};
+
+__device__ __forceinline__ void ipx_locate_chunk(const uint32_t* __restrict__ list, uint64_t n,
+                                                 const uint32_t* __restrict__ prefix, const uint64_t* __restrict__ row,
+                                                 uint32_t c, ipx_hub_chunk& h)
+{
+    h.c = c;
+    h.i = ipx_hub_of_chunk(prefix, n, c);
+    h.v = list[h.i];
+    h.c0 = prefix[h.i];
+    h.nch = prefix[h.i + 1] - h.c0;
+    h.e0 = row[h.v] + (uint64_t)(c - h.c0) * IPX_HUB_CHUNK;
+    const uint64_t end = row[h.v + 1];
+    h.e1 = (h.e0 + IPX_HUB_CHUNK < end) ? h.e0 + IPX_HUB_CHUNK : end;
+    h.a0 = h.e0 & ~3ULL;
+    h.b = h.e1 & ~3ULL;
+}
+
+/* The CTA's fold of one hub chunk is done (thread 0 holds it): store it;
+ * the CTA whose chunk arrives last folds the hub's partials in chunk order
+ * and runs the vertex's compute phase of the next superstep.  Returns the
+ * count the caller adds (thread 0 only). */
+__device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_chunk& h, bool has, ipx_msg acc,
+                                                                 ipx_bslot* out, uint32_t next_stamp)
+{
+    bool last = h.nch == 1;
+    if (!last) {
+        ipx_bslot_put(&ipx_c.hub_part[h.c], acc, has ? 1u : 0u);
+        __threadfence();
+        last = atomicAdd(&ipx_c.hub_arrived[h.i], 1u) == h.nch - 1;
+        if (last) {
+            __threadfence();
+            has = false;
+            for (uint32_t k = 0; k < h.nch; k++) {
+                const ipx_bslot p = __ldcg(&ipx_c.hub_part[h.c0 + k]);
+                ipx_msg m;
+                if (ipx_bslot_take(p, 1u, m)) ipx_fold(has, acc, true, m);
             }
-        }
-        const uint32_t ob = __ballot_sync(IPX_FULL, out);
-        const uint32_t ab = __ballot_sync(IPX_FULL, a);
-        if (lane == 0) {
-            ipx_c.has_b[v >> 5] = ob;
-            cnt += __popc(ab);
+            ipx_c.hub_arrived[h.i] = 0; /* every chunk of the hub has arrived */
         }
     }
-    ipx_block_count(cnt, &ipx_c.ctr[ctr_slot]);
+    return last ? (unsigned long long)ipx_sb_compute_next(h.v, has, acc, out, next_stamp) : 0ULL;
+}
+
+#ifndef IPX_HUB_SMEM
+#define IPX_HUB_SMEM 1
+#endif
+
+/* The hub class of ipx_k_gather_compute with ids staged in shared memory:
+ * two id buffers, each filled by one bulk copy per chunk and completed on
+ * its own mbarrier.  Thread 0 locates chunk k+1 and starts its copy before
+ * the CTA waits for chunk k's.  Each iteration thread 0 arrives once on the
+ * barrier of the chunk it issues (with the copy's byte count, or alone when
+ * the chunk has no whole 16-byte group), so buffer j's barrier completes its
+ * u-th phase at its u-th use.  Edges outside the copied range are read from
+ * global memory.  A wait that gives up (never expected) sets
+ * IPX_ERR_COPY_TIMEOUT, and the CTA reads ids from global memory for the
+ * rest of the launch; results stay exact. */
+__device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
+    const uint32_t* __restrict__ adj, const uint64_t* __restrict__ row, const uint32_t* __restrict__ list, uint64_t n,
+    const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_bslot* __restrict__ bs, uint32_t stamp,
+    ipx_bslot* __restrict__ out)
+{
+    __shared__ __align__(16) uint32_t s_ids[2][IPX_HUB_CHUNK + 4];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ ipx_hub_chunk s_h[2];
+    __shared__ bool s_has[IPX_THREADS / 32];
+    __shared__ ipx_msg s_acc[IPX_THREADS / 32];
+    __shared__ int s_fail;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nthr = blockDim.x;
+    unsigned long long cnt = 0;
+    bool pending[2] = {false, false}; /* thread 0: a copy issued and not yet waited for */
+    if (threadIdx.x == 0) {
+        ipx_mbar_init(&s_bar[0]);
+        ipx_mbar_init(&s_bar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    __syncthreads();
+    auto issue = [&](uint32_t c, int buf) {
+        ipx_hub_chunk& h = s_h[buf];
+        ipx_locate_chunk(list, n, prefix, row, c, h);
+        if (h.b > h.a0 && !s_fail) {
+            const uint32_t bytes = (uint32_t)((h.b - h.a0) * 4);
+            ipx_mbar_arrive_tx(&s_bar[buf], bytes);
+            ipx_bulk_load(s_ids[buf], adj + h.a0, bytes, &s_bar[buf]);
+            pending[buf] = true;
+        } else {
+            h.b = h.a0; /* nothing copied: every id from global memory */
+            ipx_mbar_arrive_tx(&s_bar[buf], 0u);
+        }
+    };
+    if (threadIdx.x == 0 && blockIdx.x < chunks) issue(blockIdx.x, 0);
+    uint32_t it = 0;
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x, it++) {
+        const int buf = (int)(it & 1);
+        __syncthreads(); /* s_h[buf] is written; everyone is done with buffer buf ^ 1 */
+        if (threadIdx.x == 0 && c + gridDim.x < chunks) issue(c + gridDim.x, buf ^ 1);
+        bool staged = ipx_mbar_wait(&s_bar[buf], (it >> 1) & 1u, IPX_COPY_WAIT_LIMIT);
+        if (!staged) {
+            atomicOr(ipx_c.err, IPX_ERR_COPY_TIMEOUT);
+            s_fail = 1;
+        } else if (threadIdx.x == 0) {
+            pending[buf] = false;
+        }
+        const ipx_hub_chunk h = s_h[buf];
+        staged = staged && !s_fail;
+        const uint64_t sb = staged ? h.b : h.e0; /* ids of [e0, sb) from shared memory */
+        bool has = false;
+        ipx_msg acc;
+        for (uint64_t e = h.e0 + threadIdx.x; e < h.e1; e += IPX_UNROLL * (uint64_t)nthr) {
+            uint32_t u[IPX_UNROLL];
+            ipx_bslot w[IPX_UNROLL];
+#pragma unroll
+            for (int k = 0; k < IPX_UNROLL; k++) {
+                const uint64_t ek = e + (uint64_t)k * nthr;
+                u[k] = (ek < sb) ? s_ids[buf][ek - h.a0] : (ek < h.e1 ? __ldcs(&adj[ek]) : 0u);
+            }
+#pragma unroll
+            for (int k = 0; k < IPX_UNROLL; k++) {
+                if (e + (uint64_t)k * nthr < h.e1) {
+                    w[k] = __ldg(&bs[u[k]]);
+                } else {
+                    memset(&w[k], 0xff, sizeof w[k]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IPX_UNROLL; k++) {
+                ipx_msg m;
+                if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+            }
+        }
+        ipx_warp_fold(has, acc);
+        if (lane == 0) {
+            s_has[warp] = has;
+            s_acc[warp] = acc;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            has = false;
+            for (int w = 0; w < (int)(nthr >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+            cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1);
+        }
+    }
+    /* a copy given up on may still be in flight: wait for it (bounded)
+     * before the CTA's shared memory is released */
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2; b++)
+            if (pending[b]) {
+                /* the phase in progress is the copy's: one of the two
+                 * parities is the completed phase before it and returns at
+                 * once, the other waits for the copy */
+                ipx_mbar_wait(&s_bar[b], 0u, IPX_COPY_WAIT_LIMIT);
+                ipx_mbar_wait(&s_bar[b], 1u, IPX_COPY_WAIT_LIMIT);
+            }
+    }
+    __syncthreads();
+    return cnt;
+}
+
+/* Single broadcast (pull), one superstep s >= 0 after its compute phase:
+ * ip_fetch_broadcast_messages (combiner_single_broadcast_postamble.h:57-89)
+ * for the vertices of one in-degree class, then, vertex by vertex, the
+ * compute phase of superstep s+1.  The gather reads buffer s & 1 (slots
+ * stamped s) and the compute writes buffer (s+1) & 1, which no gather of
+ * superstep s reads, so the two phases need no grid-wide barrier between
+ * them and the message goes from the fold to ip_compute in registers.
+ * Count of superstep s: the vertices active after the gather.  When it is
+ * 0 no vertex was active or received a message, so no compute phase of
+ * superstep s+1 ran, and the loop ends (:164).  MODE 0: a thread per vertex,
+ * folding in adjacency order as the reference does; 1: a warp; 2: a block
+ * (lane-strided runs folded in order, then a tree, per chunk of a hub's
+ * row; chunks folded in order: only the order of the ip_combine calls
+ * differs). */
+/* Resident CTAs per SM the fused pull kernel is compiled for: it carries
+ * ip_compute besides the gather, which needs more registers than the other
+ * edge kernels. */
+#ifndef IPX_GATHER_CTAS
+#define IPX_GATHER_CTAS 5
+#endif
+
+template <int MODE>
+__global__ void __launch_bounds__(IPX_THREADS, IPX_GATHER_CTAS) ipx_k_gather_compute(const uint32_t* __restrict__ list,
+                                                                                  uint64_t n,
+                                                                                  const uint32_t* __restrict__ prefix)
+{
+    const uint64_t s = ipx_step();
+    const uint32_t stamp = (uint32_t)s;
+    const ipx_vid* __restrict__ adj = ipx_c.in_adj;
+    const uint64_t* __restrict__ row = ipx_c.in_row;
+    const ipx_bslot* __restrict__ bs = ipx_c.bslot[s & 1];
+    ipx_bslot* __restrict__ out = ipx_c.bslot[(s + 1) & 1];
+    unsigned long long cnt = 0;
+    if constexpr (MODE == 0) {
+        /* the next vertex's list entry is loaded while this vertex's
+         * in-edges are folded */
+        const uint64_t stride = ipx_gstride();
+        uint64_t i = ipx_gtid(), v = (i < n) ? list[i] : 0;
+        for (; i < n; i += stride) {
+            const uint64_t vn = (i + stride < n) ? list[i + stride] : 0;
+            bool has = false;
+            ipx_msg acc;
+            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], 0, 1, has, acc);
+            cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
+            v = vn;
+        }
+    } else if constexpr (MODE == 1) {
+        const int lane = threadIdx.x & 31;
+        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], lane, 32, has, acc);
+            ipx_warp_fold(has, acc);
+            if (lane == 0) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
+        }
+    } else {
+        /* hubs in chunks of IPX_HUB_CHUNK in-edges, spread over all CTAs
+         * (one hub's row would otherwise keep one CTA busy long after the
+         * others finished): each chunk's fold is stored, and the CTA whose
+         * chunk arrives last folds the partials in chunk order, then runs
+         * the compute phase (ipx_hub_chunk_done).  No CTA waits for another.
+         * With 32-bit ids the chunk's ids are staged through shared memory:
+         * while the CTA gathers one chunk, a bulk copy brings the ids of its
+         * next chunk, so the slot loads are issued from shared memory
+         * instead of behind a global id load each. */
+        if (n == 0) return;
+        const uint32_t chunks = prefix[n];
+        if constexpr (sizeof(ipx_vid) == 4 && IPX_HUB_SMEM) {
+            if ((reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
+                cnt += ipx_gather_hubs_staged(reinterpret_cast<const uint32_t*>(adj), row, list, n, prefix, chunks,
+                                              bs, stamp, out);
+                ipx_block_count(cnt, &ipx_c.ctr[s & 3]);
+                return;
+            }
+        }
+        __shared__ bool s_has[IPX_THREADS / 32];
+        __shared__ ipx_msg s_acc[IPX_THREADS / 32];
+        __shared__ ipx_hub_chunk s_h;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            if (threadIdx.x == 0) ipx_locate_chunk(list, n, prefix, row, c, s_h);
+            __syncthreads();
+            const ipx_hub_chunk h = s_h;
+            bool has = false;
+            ipx_msg acc;
+            ipx_gather_fold_edges(adj, bs, stamp, h.e0, h.e1, threadIdx.x, blockDim.x, has, acc);
+            ipx_warp_fold(has, acc);
+            if (lane == 0) {
+                s_has[warp] = has;
+                s_acc[warp] = acc;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                has = false;
+                for (int w = 0; w < (int)(blockDim.x >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
+                cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1);
+            }
+            __syncthreads();
+        }
+    }
+    ipx_block_count(cnt, &ipx_c.ctr[s & 3]);
 }
 
 /* Spread + single broadcast compute phase: combiner_spread_single_broadcast_
@@ -1408,8 +1926,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(const uint32_t*
         ip_compute(&x);
         if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
         if (x.ipx_has_out) {
-            ipx_c.bval[v] = x.ipx_out;
-            ipx_set_bit_agg(ipx_c.has_b, v);
+            ipx_bslot_put(&ipx_c.bslot[0][v], x.ipx_out, (uint32_t)s);
             ipx_set_bit_agg(ipx_c.bcaster, v);
         }
     }
@@ -1451,6 +1968,11 @@ __global__ void ipx_k_begin_superstep()
     const uint64_t s = ipx_step();
     ipx_c.ctr[s & 3] = 0ULL;
     for (int k = 8; k < 14; k++) ipx_c.ctr[k] = 0ULL;
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    /* the fused kernels of superstep s run the compute phase of s + 1
+     * (superstep 0's own compute phase, ipx_k_compute_sb0, ran before) */
+    ipd_compute_superstep = s + 1;
+#endif
 }
 
 /* Combiner: active count of the superstep = |active or received|
@@ -1507,6 +2029,7 @@ __global__ void ipx_k_advance(cudaGraphConditionalHandle loop, unsigned long lon
         go = false;
     }
     ipd_superstep = s + 1;
+    ipd_compute_superstep = s + 1;
     cudaGraphSetConditional(loop, go ? 1u : 0u);
 }
 

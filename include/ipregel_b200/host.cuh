@@ -223,7 +223,8 @@ static uint64_t ipx_push_t0() { return IPX_PUSH_EXPAND ? ipx_h.tune.t1 : ipx_h.t
 static int ipx_reset_vertex_state()
 {
     const ipx_consts& c = ipx_h.c;
-    const uint64_t V = c.V, W = c.W;
+    const uint64_t V = c.V;
+    [[maybe_unused]] const uint64_t W = c.W;
     cudaStream_t st = ipx_h.st;
     if (V) {
         ipx_k_init_values<<<ipx_grid(), IPX_THREADS, 0, st>>>(0, V - 1);
@@ -240,11 +241,13 @@ static int ipx_reset_vertex_state()
     IPX_CU(cudaMemsetAsync(c.recv[1], 0, W * 4 + 4, st));
     IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
-    IPX_CU(cudaMemsetAsync(c.hasmsg_b, 0, V + 1, st));
-    IPX_CU(cudaMemsetAsync(c.has_b, 0, W * 4 + 4, st));
+    /* every stamp IPX_NO_STAMP: no slot counts in any superstep */
+    IPX_CU(cudaMemsetAsync(c.bslot[0], 0xff, (V ? V : 1) * sizeof(ipx_bslot), st));
+    IPX_CU(cudaMemsetAsync(c.bslot[1], 0xff, (V ? V : 1) * sizeof(ipx_bslot), st));
+    IPX_CU(cudaMemsetAsync(c.hub_arrived, 0, (ipx_h.gbins.count[2] + 1) * sizeof(uint32_t), st));
 #else
     IPX_CU(cudaMemsetAsync(c.hasmsg_b, 0, V + 1, st));
-    IPX_CU(cudaMemsetAsync(c.has_b, 0, W * 4 + 4, st));
+    IPX_CU(cudaMemsetAsync(c.bslot[0], 0xff, (V ? V : 1) * sizeof(ipx_bslot), st));
     IPX_CU(cudaMemsetAsync(c.bt, 0, W * 4 + 4, st));
     IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
 #endif
@@ -345,15 +348,33 @@ static int ipx_setup_state()
         IPX_CU(cudaDeviceSynchronize());
     }
 #endif
-#if IPX_PULL
+#if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
     IPX_OK(ipx_alloc(&c.hasmsg_b, V + 1));
     IPX_OK(ipx_alloc(&c.msg, V));
-    IPX_OK(ipx_alloc(&c.bval, V));
-    IPX_OK(ipx_alloc(&c.has_b, W + 1));
+    IPX_OK(ipx_alloc(&c.bslot[0], V));
 #endif
 #if IPX_VERSION == IPX_SINGLE_BROADCAST
+    IPX_OK(ipx_alloc(&c.bslot[0], V));
+    IPX_OK(ipx_alloc(&c.bslot[1], V));
     IPX_OK(ipx_alloc(&c.active_b, V + 1));
     IPX_OK(ipg_graph_bins(ipx_h.g, 1, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
+    {
+        /* chunks of the hub class: prefix, partial folds, arrival counters */
+        const ipg_bins& b = ipx_h.gbins;
+        const uint64_t n2 = b.count[2];
+        const uint64_t max_chunks = b.edges[2] / IPX_HUB_CHUNK + n2 + 1;
+        IPX_OK(ipx_alloc(&ipx_h.pull_prefix, n2 + 2));
+        IPX_OK(ipx_alloc(&c.hub_part, max_chunks));
+        IPX_OK(ipx_alloc(&c.hub_arrived, n2 + 1));
+        IPX_CU(cudaMemset(c.hub_arrived, 0, (n2 + 1) * sizeof(uint32_t)));
+        uint32_t* dcount = nullptr;
+        IPX_OK(ipx_alloc(&dcount, 1));
+        const uint32_t n2u = (uint32_t)n2;
+        IPX_CU(cudaMemcpy(dcount, &n2u, 4, cudaMemcpyHostToDevice));
+        ipx_k_hub_prefix<<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
+        IPX_CU(cudaGetLastError());
+        IPX_CU(cudaDeviceSynchronize());
+    }
 #endif
 #if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
     IPX_OK(ipx_alloc(&c.bt, W + 1));
@@ -384,8 +405,8 @@ static int ipx_setup_state()
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_spread, tb, per_sm);
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_push<1>, tb, per_sm);
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
-        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb, tb, per_sm);
-        ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, true>, tb, per_sm);
+        ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb0, tb, per_sm);
+        ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather_compute<1>, tb, per_sm);
 #else
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb, tb, per_sm);
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, false>, tb, per_sm);
@@ -436,6 +457,7 @@ static int ipx_set_superstep(uint64_t s)
 {
     size_t v = s;
     IPX_CU(cudaMemcpyToSymbolAsync(ipd_superstep, &v, sizeof v, 0, cudaMemcpyHostToDevice, ipx_h.st));
+    IPX_CU(cudaMemcpyToSymbolAsync(ipd_compute_superstep, &v, sizeof v, 0, cudaMemcpyHostToDevice, ipx_h.st));
     return IPG_OK;
 }
 
@@ -557,10 +579,16 @@ static void ipx_account_bytes(uint64_t s, uint64_t frontier)
     B[IPX_K_COMPACT_T] += V / 8.0 + l[4] * 4.0;
 #endif
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
+    /* superstep 0's compute: activity, value read and write, broadcast;
+     * the fused kernels: per vertex its list entry, in-row bounds, activity
+     * and value read + write, out-row bounds and a broadcast (the compute
+     * phase of the next superstep); per in-edge its id and the gathered
+     * message */
     const ipg_bins& b = ipx_h.gbins;
-    B[IPX_K_COMPUTE] += V * 1.0 / 8.0 + frontier * (2 * vb + mb + 2);
+    (void)frontier;
+    if (s == 0) B[IPX_K_COMPUTE] += V * (1.0 + 2 * vb + 16.0 + mb);
     for (int k = 0; k < 3; k++)
-        B[IPX_K_GATHER0 + k] += b.count[k] * (4.0 + 8.0 + 2.0 + mb) + b.edges[k] * (ib + mb + 0.125);
+        B[IPX_K_GATHER0 + k] += b.count[k] * (4.0 + 16.0 + 1.0 + 2 * vb + mb) + b.edges[k] * (ib + mb);
     for (int k = 0; k < 3; k++) N[IPX_K_GATHER0 + k] += b.edges[k];
 #else
     const double nb = (double)l[0] + l[1] + l[2];
@@ -588,6 +616,8 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count, uint64_t frontier)
         return ipx_fail(IPG_EDEVICE,
                         "The function send_message should not be used in the SINGLE_BROADCAST version; only "
                         "broadcast() should be called, and once per superstep maximum.");
+    if (err & IPX_ERR_COPY_TIMEOUT)
+        return ipx_fail(IPG_EDEVICE, "a bulk copy into shared memory did not complete in time (results kept exact)");
     if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
     *count = ipx_h.h_ctr[s & 3];
@@ -643,6 +673,11 @@ static int ipx_enqueue_superstep()
     const uint64_t V = c.V;
     (void)V;
     (void)ge;
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+    /* superstep 0's compute phase (returns at once later), before
+     * ipx_k_begin_superstep moves ip_get_superstep() to the next superstep */
+    IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb0<<<g, ipx_h.tb, 0, st>>>());
+#endif
     IPX_LAUNCH(IPX_K_CTRL, ipx_k_begin_superstep<<<1, 1, 0, st>>>());
 #if IPX_VERSION == IPX_COMBINER
     IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_combiner<<<g, ipx_h.tb, 0, st>>>());
@@ -659,14 +694,17 @@ static int ipx_enqueue_superstep()
                                                    ipx_h.lcnt + 4, nullptr, 1, st)));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
     {
-        IPX_LAUNCH(IPX_K_COMPUTE, ipx_k_compute_sb<<<g, ipx_h.tb, 0, st>>>());
+        /* gather of this superstep fused with the next one's compute phase */
         const ipg_bins& b = ipx_h.gbins;
         if (b.count[0])
-            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[0], nullptr, b.count[0]));
+            IPX_LAUNCH(IPX_K_GATHER0,
+                       ipx_k_gather_compute<0><<<ge, ipx_h.tb, 0, st>>>(b.d_list[0], b.count[0], nullptr));
         if (b.count[1])
-            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[1], nullptr, b.count[1]));
+            IPX_LAUNCH(IPX_K_GATHER1,
+                       ipx_k_gather_compute<1><<<ge, ipx_h.tb, 0, st>>>(b.d_list[1], b.count[1], nullptr));
         if (b.count[2])
-            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, true><<<ge, ipx_h.tb, 0, st>>>(b.d_list[2], nullptr, b.count[2]));
+            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather_compute<2><<<ge, ipx_h.tb, 0, st>>>(b.d_list[2], b.count[2],
+                                                                                          ipx_h.pull_prefix));
     }
 #else
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
@@ -685,7 +723,6 @@ static int ipx_enqueue_superstep()
     IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather<0, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[0], ipx_h.lcnt + 4, 0));
     IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather<1, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[1], ipx_h.lcnt + 5, 0));
     IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather<2, false><<<ge, ipx_h.tb, 0, st>>>(ipx_h.tlist[2], ipx_h.lcnt + 6, 0));
-    IPX_CU(cudaMemsetAsync(c.has_b, 0, c.W * 4 + 4, st));
 #endif
     IPX_CU(cudaGetLastError());
     return IPG_OK;
@@ -696,7 +733,9 @@ static uint64_t ipx_max_supersteps()
     /* The reference loops until quiescence; a bound (IPG_MAX_SUPERSTEPS,
      * default 10^6) turns a program that never halts into an error. */
     const char* lim = getenv("IPG_MAX_SUPERSTEPS");
-    return (lim && *lim) ? strtoull(lim, nullptr, 10) : 1000000ULL;
+    const uint64_t n = (lim && *lim) ? strtoull(lim, nullptr, 10) : 1000000ULL;
+    /* pull versions stamp broadcast slots with the superstep's low 32 bits */
+    return (IPX_PULL && n > (uint64_t)IPX_NO_STAMP - 1) ? (uint64_t)IPX_NO_STAMP - 1 : n;
 }
 
 /* Host-driven loop: one synchronisation per superstep, which gives the
@@ -805,6 +844,7 @@ static int ipx_loop_prepare()
     ipx_h.dirty = true;
     size_t zero = 0;
     IPX_CU(cudaMemcpyToSymbol(ipd_superstep, &zero, sizeof zero));
+    IPX_CU(cudaMemcpyToSymbol(ipd_compute_superstep, &zero, sizeof zero));
     return IPG_OK;
 }
 
@@ -846,6 +886,8 @@ static int ipx_loop_collect(double seconds)
                         "The function send_message should not be used in the SINGLE_BROADCAST version; only "
                         "broadcast() should be called, and once per superstep maximum.");
     if (err & IPX_ERR_SUPERSTEP_LIMIT) return ipx_fail(IPG_EDEVICE, "superstep limit (IPG_MAX_SUPERSTEPS) reached");
+    if (err & IPX_ERR_COPY_TIMEOUT)
+        return ipx_fail(IPG_EDEVICE, "a bulk copy into shared memory did not complete in time (results kept exact)");
     if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
     return IPG_OK;
 }

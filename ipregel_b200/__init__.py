@@ -46,7 +46,7 @@ RUNTIME_SYMBOLS = (
     "ipg_error_f32_f64", "ipg_graph_concat", "ipg_fused_create", "ipg_fused_graph", "ipg_fused_launch",
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
-    "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats", "ipg_measure_gather",
+    "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats",
     "ipg_server_reserve", "ipg_graph_refill_host", "ipg_graph_contents",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
@@ -136,7 +136,6 @@ def runtime():
         L.ipg_pr_run_f32.argtypes = [vp, ctypes.c_uint32, dbl, i32, vp, vp, vp]
         L.ipg_error_f32_f64.argtypes = [vp, vp, u64, ctypes.POINTER(dbl), ctypes.POINTER(dbl),
                                         ctypes.POINTER(dbl), ctypes.POINTER(u64), vp]
-        L.ipg_measure_gather.argtypes = [u64, ctypes.c_uint32, u64, i32, ctypes.POINTER(dbl), ctypes.POINTER(dbl)]
         _rt = L
     return _rt
 
@@ -735,12 +734,36 @@ class PageRankF32:
             pass
 
 
+PROBE_PATH = os.path.join(LIB_DIR, "libipregel_b200_probe.so")
+PROBE_SYMBOLS = ("ipg_measure_gather", "ipg_probe_last_error")
+_probe = None
+
+
+def probe():
+    """Loads the benchmark's measurement library (libipregel_b200_probe.so),
+    which is not part of the runtime."""
+    global _probe
+    if _probe is None:
+        runtime()
+        if not os.path.exists(PROBE_PATH):
+            raise IPregelError(f"{PROBE_PATH} is missing: build it with `make -C {HERE}`")
+        L = ctypes.CDLL(PROBE_PATH)
+        L.ipg_measure_gather.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.ipg_probe_last_error.restype = ctypes.c_char_p
+        _probe = L
+    return _probe
+
+
 def measure_gather(table_bytes: int, row_bytes: int = 4, n: int = 1 << 28, reps: int = 5) -> dict:
-    """The random-gather ceiling (ipg_measure_gather): rows/s and GB/s of n
-    scattered reads of row_bytes-byte rows from a table of table_bytes."""
+    """The random-gather ceiling (ipg_measure_gather, measurement library):
+    rows/s and GB/s of n scattered reads of row_bytes-byte rows from a table
+    of table_bytes."""
     rows, gbs = ctypes.c_double(), ctypes.c_double()
-    _check(runtime().ipg_measure_gather(table_bytes, row_bytes, n, reps, ctypes.byref(rows), ctypes.byref(gbs)),
-           where="ipg_measure_gather")
+    P = probe()
+    rc = P.ipg_measure_gather(table_bytes, row_bytes, n, reps, ctypes.byref(rows), ctypes.byref(gbs))
+    if rc != 0:
+        raise IPregelError(f"ipg_measure_gather failed ({rc}): {P.ipg_probe_last_error().decode()}")
     return {"table_bytes": table_bytes, "row_bytes": row_bytes, "rows_per_s": rows.value, "gbs": gbs.value}
 
 

@@ -11,12 +11,24 @@
 // element at a pseudo-random position -- so that the kernels' edge rates can
 // be read against the rate the memory system sustains for the same pattern.
 #include "ipregel_b200.h"
+#include "ipregel_b200_probe.h"
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
 
-extern "C" int ipg_internal_fail(int code, const char* msg);
+// The probe library's own last error (it links nothing of the runtime but
+// its header's status codes).
+static thread_local char pb_err[256];
+
+static int pb_fail(int code, const char* msg)
+{
+    snprintf(pb_err, sizeof pb_err, "%s", msg);
+    return code;
+}
+
+extern "C" const char* ipg_probe_last_error(void) { return pb_err; }
 
 #define PB_THREADS 256
 #define PB_UNROLL 8
@@ -24,7 +36,7 @@ extern "C" int ipg_internal_fail(int code, const char* msg);
 #define PB_CU(call)                                                                     \
     do {                                                                                \
         cudaError_t e_ = (call);                                                        \
-        if (e_ != cudaSuccess) return ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e_)); \
+        if (e_ != cudaSuccess) return pb_fail(IPG_ECUDA, cudaGetErrorString(e_)); \
     } while (0)
 
 // A 32-bit mixing function (the finaliser of MurmurHash3, Appleby 2011):
@@ -100,11 +112,11 @@ __global__ void __launch_bounds__(PB_THREADS) k_pb_gather_rows(const uint32_t* _
 extern "C" int ipg_measure_gather(uint64_t table_bytes, uint32_t row_bytes, uint64_t n, int reps,
                                   double* rows_per_s, double* gbs)
 {
-    if (!rows_per_s || !gbs) return ipg_internal_fail(IPG_EINVAL, "ipg_measure_gather: null output");
+    if (!rows_per_s || !gbs) return pb_fail(IPG_EINVAL, "ipg_measure_gather: null output");
     if (row_bytes != 4 && row_bytes != 64 && row_bytes != 128 && row_bytes != 256)
-        return ipg_internal_fail(IPG_EINVAL, "ipg_measure_gather: row_bytes must be 4, 64, 128 or 256");
+        return pb_fail(IPG_EINVAL, "ipg_measure_gather: row_bytes must be 4, 64, 128 or 256");
     if (table_bytes < row_bytes || table_bytes / row_bytes > 0xffffffffull || n == 0 || n > (1ull << 31) || reps < 1)
-        return ipg_internal_fail(IPG_EINVAL, "ipg_measure_gather: table of 1 .. 2^32 rows, 1 <= n <= 2^31, reps >= 1");
+        return pb_fail(IPG_EINVAL, "ipg_measure_gather: table of 1 .. 2^32 rows, 1 <= n <= 2^31, reps >= 1");
     const uint64_t rows = table_bytes / row_bytes;
     int dev = 0, sms = 0, per_sm = 0;
     PB_CU(cudaGetDevice(&dev));
@@ -118,7 +130,7 @@ extern "C" int ipg_measure_gather(uint64_t table_bytes, uint32_t row_bytes, uint
     int rc = IPG_OK;
     float ms = 0.f;
     auto check = [&](cudaError_t e) {
-        if (e != cudaSuccess && rc == IPG_OK) rc = ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+        if (e != cudaSuccess && rc == IPG_OK) rc = pb_fail(IPG_ECUDA, cudaGetErrorString(e));
         return rc == IPG_OK;
     };
     if (check(cudaMalloc(&idx, n * 4)) && check(cudaMalloc(&table, rows * row_bytes)) && check(cudaMalloc(&sink, 4)) &&

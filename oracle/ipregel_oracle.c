@@ -464,6 +464,29 @@ static void og_fetch(og_ctx* c, uint64_t v, uint64_t* count, int reactivate)
         if (c->has_b[c->in_adj[i]]) og_combine(c, &c->message[v], c->bval[c->in_adj[i]]);
 }
 
+/* og_fetch with reactivation, for concurrent calls on distinct vertices:
+ * the edges it reads are returned instead of added to c->edges, and the
+ * reactivations are counted into the caller's *count. */
+static uint64_t og_fetch_sb(og_ctx* c, uint64_t v, uint64_t* count)
+{
+    uint64_t i = c->in_row[v], end = c->in_row[v + 1];
+    const uint64_t edges = end - i;
+    while (i < end && !c->has_b[c->in_adj[i]]) i++;
+    if (i >= end) {
+        c->has_message[v] = 0;
+        return edges;
+    }
+    if (!c->active[v]) {
+        (*count)++;
+        c->active[v] = 1;
+    }
+    c->has_message[v] = 1;
+    c->message[v] = c->bval[c->in_adj[i]];
+    for (i++; i < end; i++)
+        if (c->has_b[c->in_adj[i]]) og_combine(c, &c->message[v], c->bval[c->in_adj[i]]);
+    return edges;
+}
+
 static int og_record(og_ctx* c, uint64_t count, uint64_t* counts_out, uint64_t max_counts)
 {
     if (counts_out && c->s < max_counts) counts_out[c->s] = count;
@@ -571,19 +594,30 @@ int og_run(const og_graph* g, const og_params* p, void* values_out,
         break;
     }
     case OG_SINGLE_BROADCAST: {  /* src/combiner_single_broadcast_postamble.h:91-259 */
+        /* Both phases are loops over independent vertices, as the
+         * reference's `omp for` loops are (:185-201, :213-220): a vertex's
+         * compute writes only its own value, flags and broadcast slot, and a
+         * vertex's fetch folds its in-list sequentially into its own
+         * message, so running them on several threads gives the same bits. */
         for (uint64_t v = 0; v < V; v++) c.active[v] = 1;
         count = V;
         while (count != 0) {
-            count = 0;
+            uint64_t cnt = 0, edges = 0;
+            int fatal = 0;
+            #pragma omp parallel for schedule(dynamic, 4096) reduction(+:cnt) reduction(|:fatal)
             for (uint64_t v = 0; v < V; v++) {
                 c.has_b[v] = 0;
                 if (c.active[v]) {
                     og_compute(&c, v);
-                    if (c.fatal) { rc = c.fatal; goto done; }
-                    if (c.active[v]) count++;
+                    if (c.fatal) fatal = 1;
+                    if (c.active[v]) cnt++;
                 }
             }
-            for (uint64_t v = 0; v < V; v++) og_fetch(&c, v, &count, 1);
+            if (fatal) { rc = c.fatal; goto done; }
+            #pragma omp parallel for schedule(dynamic, 4096) reduction(+:cnt, edges)
+            for (uint64_t v = 0; v < V; v++) edges += og_fetch_sb(&c, v, &cnt);
+            c.edges += edges;
+            count = cnt;
             if ((rc = og_record(&c, count, counts_out, max_counts))) goto done;
         }
         break;

@@ -139,3 +139,57 @@ def test_parity_check_against_reference_dumps():
     bad_w[np.argmax(w != 0xFFFFFFFF)] += 1
     assert not bench.parity_check(*args, cc, list(ccn), bad_w, hop, list(hopn), dumps)["ok"]
     assert not bench.parity_check(*args, cc, list(ccn)[:-1], w, hop, list(hopn), dumps)["ok"]
+
+
+def test_traffic_capture_of_other_sources_is_not_used(tmp_path, monkeypatch):
+    import json
+    p = tmp_path / "traffic.json"
+    monkeypatch.setattr(bench, "TRAFFIC_PATH", str(p))
+    assert bench.stored_traffic("sssp:push_warp", 1000)["traffic"] is None
+    entry = {"dram_bytes_per_algorithmic_byte": 0.5, "source": "capture"}
+    p.write_text(json.dumps({"_kernel_sources_sha16": "0" * 16, "sssp:push_warp": entry}))
+    r = bench.stored_traffic("sssp:push_warp", 1000)
+    assert r["traffic"] is None and "other kernel sources" in r["traffic_source"]
+    p.write_text(json.dumps({"_kernel_sources_sha16": bench.kernel_sources_sha16(), "sssp:push_warp": entry}))
+    r = bench.stored_traffic("sssp:push_warp", 1000)
+    assert r["traffic"] == 500 and r["traffic_source"].startswith("scaled, not measured")
+
+
+def test_write_traffic_from_launch_list(tmp_path):
+    """Launches are assigned to programs by their superstep openers (CC
+    first) and to kernels by name; compactions alternate within a superstep."""
+    import json
+    rows, i = [], 0
+
+    def launch(name, dram):
+        nonlocal i
+        for metric, v in (("gpu__time_duration.sum", 1000), ("dram__bytes_read.sum", dram),
+                          ("dram__bytes_write.sum", 0)):
+            rows.append(f'"{i}","1","p","python","0","(1,1,1)","(1,1,1)","{name}","{metric}","byte","{v}"')
+        i += 1
+
+    launch("k_generate", 77)  # before the profiled step
+    for prog_steps, scale in ((2, 1), (3, 10)):
+        for _ in range(prog_steps):
+            launch("ipx_k_begin_superstep()", 1)
+            launch("ipx_k_compute_spread(const unsigned int *, const unsigned int *)", 2 * scale)
+            launch("k_compact(unsigned int *, unsigned long, ...)", 3 * scale)
+            launch("void ipx_k_push<1>(const unsigned int *)".replace("void ", ""), 5 * scale)
+            launch("k_compact(unsigned int *, unsigned long, ...)", 7 * scale)
+    head = ('"ID","Process ID","Process Name","Host Name","Context","Block Size","Grid Size","Kernel Name",'
+            '"Metric Name","Metric Unit","Metric Value"')
+    csv_path = tmp_path / "l.csv"
+    csv_path.write_text("==PROF== x\n" + head + "\n" + "\n".join(rows) + "\n")
+    kern = {"cc:compute": {"launches": 2, "bytes": 8}, "sssp:compute": {"launches": 3, "bytes": 60},
+            "cc:push_warp": {"launches": 2, "bytes": 20}, "sssp:push_warp": {"launches": 3, "bytes": 300},
+            "cc:compact_broadcasters": {"launches": 2, "bytes": 6}, "cc:compact_targets": {"launches": 2, "bytes": 7},
+            "sssp:compact_broadcasters": {"launches": 3, "bytes": 90},
+            "sssp:compact_targets": {"launches": 3, "bytes": 210}}
+    line_path = tmp_path / "line.json"
+    line_path.write_text(json.dumps({"kernels": kern, "config": {"scale": 24}}))
+    out = bench.write_traffic(str(csv_path), str(line_path), str(tmp_path / "t.json"))
+    assert out["_kernel_sources_sha16"] == bench.kernel_sources_sha16()
+    assert out["cc:compute"]["dram_bytes_per_algorithmic_byte"] == 0.5  # 2 launches x 2 / 8
+    assert out["sssp:push_warp"]["dram_bytes_per_algorithmic_byte"] == 0.5  # 3 x 50 / 300
+    assert out["cc:compact_targets"]["dram_bytes_per_algorithmic_byte"] == 2.0  # 2 x 7 / 7
+    assert out["sssp:compact_broadcasters"]["launches"] == 3

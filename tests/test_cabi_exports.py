@@ -58,3 +58,17 @@ def test_product_does_not_import_oracle():
     for path in glob.glob(os.path.join(ROOT, "ipregel_b200", "**", "*.py"), recursive=True):
         src = open(path).read()
         assert "oracle" not in re.sub(r"#.*", "", src).replace('"""', ""), path
+
+
+def test_probe_library_is_apart_from_the_runtime():
+    """The benchmark's measurement probe lives in its own library: the runtime
+    exports none of it, and the probe library exports what its header says."""
+    import ipregel_b200 as ip
+    if not os.path.exists(ip.PROBE_PATH):
+        pytest.skip("probe library not built")
+    declared = _declared("ipregel_b200_probe.h")
+    assert declared == set(ip.PROBE_SYMBOLS)
+    probe = ctypes.CDLL(ip.PROBE_PATH)
+    assert all(hasattr(probe, s) for s in declared)
+    runtime = ctypes.CDLL(ip.RUNTIME_PATH)
+    assert not any(hasattr(runtime, s) for s in declared)

@@ -198,3 +198,41 @@ def test_symmetry_check_and_generator_flag():
     assert u.check_symmetric() == -1
     for x in (und, d, u):
         x.free()
+
+
+@pytest.mark.parametrize("app", ["pagerank", "cc", "sssp"])
+@pytest.mark.parametrize("t0,t1", [(16, 4096), (2, 64), (0, 1), (64, 100000)])
+def test_single_broadcast_degree_classes(app, t0, t1):
+    """The single_broadcast gather fused with the next superstep's compute,
+    over every split of the in-degree classes: hubs in many chunks of 2048
+    in-edges folded by whichever CTA arrives last (t1 = 1, 64), hubs in one
+    chunk, rows of every alignment read 128 bits at a time by warps and
+    blocks; host and captured loops; per-superstep counts identical."""
+    import ipregel_b200 as ip
+    hub = [(0, i) for i in range(1, 9000)] + [(i, 0) for i in range(1, 9000)] + \
+          [(i, i + 1) for i in range(1, 8999)] + [(i + 1, i) for i in range(1, 8999)] + [(5, 7000), (7000, 5)]
+    graphs = [O.gen_rmat(12, 16, seed=21, undirected=False), O.from_edges(9000, hub),
+              O.gen_rmat(11, 16, seed=22, undirected=True)]
+    for g in graphs:
+        graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+        eng = ip.Engine(app, "single_broadcast")
+        try:
+            eng.set_quiet(True)
+            eng.set_tuning(t0=t0, t1=t1)
+            params = {"rounds": 10} if app == "pagerank" else {"source": 3} if app == "sssp" else {}
+            for k, v in params.items():
+                eng.set_param(k, v)
+            want, counts, _ = O.run(g, app, "single_broadcast", source=params.get("source", 0))
+            for loop in (False, True):
+                eng.set_graph_loop(loop)
+                eng.attach(graph)
+                for _ in range(2):  # a second run on the same attachment
+                    res = eng.run()
+                    if app == "pagerank":
+                        assert np.max(np.abs(res.values - want)) <= PR_TOL
+                    else:
+                        np.testing.assert_array_equal(res.values, want)
+                    assert res.counts == [int(c) for c in counts]
+        finally:
+            eng.release()
+            graph.free()
