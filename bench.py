@@ -420,9 +420,12 @@ def batch_row():
     out = {"workload": "4096 directed ER graphs, n log-uniform [1024, 65536], m = 8n, weights U[1,64], seed 1; "
                        "CC + SSSP(0) per graph",
            "vertices": int(bt.union.V), "edges": int(E),
+           "speedup_vs_plain_device": round(dev / fused, 1),
+           "speedup_note": "device time of the fused launch against the device time of the plain per-graph loops; "
+                           "the wall-clock ratio also counts the plain loop's host attach/run calls",
            "fused_launch_ms": round(fused * 1e3, 2), "fused_gteps_2runs": round(2 * E / fused / 1e9, 3),
-           "plain_loop_wall_s": round(wall, 3), "plain_loop_device_s": round(dev, 3),
-           "speedup_vs_plain_wall": round(wall / fused, 1), "speedup_vs_plain_device": round(dev / fused, 1),
+           "plain_loop_device_s": round(dev, 3), "plain_loop_wall_s": round(wall, 3),
+           "speedup_vs_plain_wall": round(wall / fused, 1),
            "results_equal_plain": bool(same),
            "tuning": {k: v[0] for k, v in best.items()}, "supersteps": list(res.supersteps)}
     r.release()

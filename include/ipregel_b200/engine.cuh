@@ -689,6 +689,10 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_PUSH_EXPAND
 #define IPX_PUSH_EXPAND 0
 #endif
+/* Lanes per source in the thread class of push and mark (1, 2, 4 or 8). */
+#ifndef IPX_PUSH_Q
+#define IPX_PUSH_Q 1
+#endif
 
 template <class T>
 __device__ __forceinline__ T ipx_shfl_idx(T x, int src)
@@ -1056,6 +1060,18 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
             ipx_msg m = ipx_msg();
             if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
             ipx_edges_strided(adj, row[u], row[u + 1], 0, 1, m, visit);
+        }
+    } else if constexpr (MODE == 0 && IPX_PUSH_Q > 1) {
+        /* IPX_PUSH_Q consecutive lanes per source: a source's (at most
+         * IPX_T0) ids are read by the group's lanes together, sectors shared */
+        const ipx_vid* __restrict__ adj = ipx_c.adj;
+        const uint64_t* __restrict__ row = ipx_c.row;
+        const uint64_t q = threadIdx.x & (IPX_PUSH_Q - 1);
+        for (uint64_t i = ipx_gtid() / IPX_PUSH_Q; i < n; i += ipx_gstride() / IPX_PUSH_Q) {
+            const uint64_t u = list[i];
+            ipx_msg m = ipx_msg();
+            if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
+            ipx_edges_strided(adj, row[u], row[u + 1], q, IPX_PUSH_Q, m, visit);
         }
     } else if constexpr (MODE == 0) {
         /* the next source's list entry, row bounds and message are loaded
