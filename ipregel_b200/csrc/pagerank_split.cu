@@ -161,13 +161,47 @@ __device__ __forceinline__ void pr_finish(const PrStep& a, uint64_t v, uint64_t 
 }
 
 // Lane-strided compensated sum of b_cur over adj[e0, e1), PR_UNROLL loads in
-// flight per lane.  Ids are loaded evict-first where a warp reads consecutive
+// flight per lane (warps and blocks: pr_gather_v4).  Ids are loaded evict-first where a warp reads consecutive
 // ids in one instruction (lanes >= 32); a thread walking a row alone comes
 // back to the same line in its next loads, so it keeps the line cached.
+template <bool COMP>
+__device__ __forceinline__ void pr_gather_v4(const PrStep& a, uint64_t e0, uint64_t e1, uint64_t lane,
+                                             uint64_t lanes, float& s, float& c)
+{
+    // a warp or block reads four consecutive ids per lane with one 128-bit
+    // load; the up to 3 ids before the first 16-byte boundary and after the
+    // last take a lane each
+    uint64_t al = (e0 + 3) & ~3ULL;
+    if (al > e1) al = e1;
+    const uint64_t b = al + ((e1 - al) & ~3ULL);
+    {
+        const uint64_t nh = al - e0, nt = e1 - b;
+        uint64_t e = e1;
+        if (lane < nh) e = e0 + lane;
+        else if (lane < nh + nt) e = b + (lane - nh);
+        if (e < e1) pr_add<COMP>(s, c, __ldg(&a.b_cur[a.in_adj[e]]));
+    }
+    const uint4* __restrict__ q4 = reinterpret_cast<const uint4*>(a.in_adj + al);
+    const uint64_t groups = (b - al) >> 2;
+    for (uint64_t g = lane; g < groups; g += lanes) {
+        const uint4 id = __ldcs(q4 + g);
+        const float q0 = __ldg(&a.b_cur[id.x]), q1 = __ldg(&a.b_cur[id.y]);
+        const float q2 = __ldg(&a.b_cur[id.z]), q3 = __ldg(&a.b_cur[id.w]);
+        pr_add<COMP>(s, c, q0);
+        pr_add<COMP>(s, c, q1);
+        pr_add<COMP>(s, c, q2);
+        pr_add<COMP>(s, c, q3);
+    }
+}
+
 template <bool COMP>
 __device__ __forceinline__ void pr_gather(const PrStep& a, uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
                                           float& s, float& c)
 {
+    if (lanes >= 32 && (reinterpret_cast<uintptr_t>(a.in_adj) & 15) == 0) {
+        pr_gather_v4<COMP>(a, e0, e1, lane, lanes, s, c);
+        return;
+    }
     for (uint64_t e = e0 + lane; e < e1; e += PR_UNROLL * lanes) {
         uint32_t u[PR_UNROLL];
         float q[PR_UNROLL];

@@ -57,13 +57,22 @@ def test_c1_pagerank_app_library(c1, rounds):
     g, path = c1
     want, want_counts = _ref_or_oracle("pagerank", "single_broadcast", g, path, rounds)
     dg = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)  # directed = false, as pagerank.c loads it
+    eng = ip.Engine("pagerank", "single_broadcast")
     try:
+        eng.set_quiet(True)
+        eng.set_param("rounds", rounds)
         for loop in (False, True):
-            res = ip.run_app("pagerank", "single_broadcast", dg, params={"rounds": rounds}, graph_loop=loop)
+            eng.set_graph_loop(loop)
+            eng.attach(dg)
+            res = eng.run()
             assert float(np.max(np.abs(res.values - want))) <= 1e-12
             assert res.counts == want_counts
             assert len(res.counts) == rounds + 1
     finally:
+        # parameters are globals of the library: back to pagerank.c's ROUND
+        eng.set_param("rounds", 10)
+        eng.set_graph_loop(False)
+        eng.release()
         dg.free()
 
 

@@ -28,6 +28,9 @@ def _engine(app, version):
     eng.set_quiet(True)
     if app in SOURCED:
         eng.set_param("source", 0)
+    if app in ("pagerank", "ppr"):
+        # parameters are globals of the library: state the default explicitly
+        eng.set_param("rounds", 20 if app == "ppr" else 10)
     return eng
 
 
