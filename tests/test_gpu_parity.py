@@ -201,7 +201,7 @@ def test_symmetry_check_and_generator_flag():
 
 
 @pytest.mark.parametrize("app", ["pagerank", "cc", "sssp"])
-@pytest.mark.parametrize("t0,t1", [(16, 4096), (2, 64), (0, 1), (64, 100000)])
+@pytest.mark.parametrize("t0,t1", [(16, 4096), (2, 64), (1, 1), (64, 100000)])
 def test_single_broadcast_degree_classes(app, t0, t1):
     """The single_broadcast gather fused with the next superstep's compute,
     over every split of the in-degree classes: hubs in many chunks of 2048
