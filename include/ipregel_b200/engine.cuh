@@ -552,6 +552,8 @@ struct ipx_consts {
      * has} in a slot, has in the stamp word), per hub the chunks arrived */
     ipx_bslot* hub_part;
     uint32_t* hub_arrived;
+    /* chunk -> index of its hub in the static hub class (built at attach) */
+    const uint32_t* hub_owner;
 };
 
 __constant__ ipx_consts ipx_c;
@@ -950,6 +952,15 @@ __global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restr
         __syncthreads();
     }
     if (threadIdx.x == 0) prefix[n] = carry;
+}
+
+/* owner[c] = i for every chunk c of hub i (prefix as ipx_k_hub_prefix
+ * made it): a chunk finds its hub with one load instead of a binary search
+ * of ~log2(n) dependent loads. */
+__global__ void ipx_k_chunk_owner(const uint32_t* __restrict__ prefix, uint64_t n, uint32_t* __restrict__ owner)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        for (uint32_t c = prefix[i]; c < prefix[i + 1]; c++) owner[c] = (uint32_t)i;
 }
 
 /* Hub index of chunk c: the last i with prefix[i] <= c. */
@@ -1660,7 +1671,7 @@ __device__ __forceinline__ void ipx_locate_chunk(const uint32_t* __restrict__ li
                                                  uint32_t c, ipx_hub_chunk& h)
 {
     h.c = c;
-    h.i = ipx_hub_of_chunk(prefix, n, c);
+    h.i = ipx_c.hub_owner ? ipx_c.hub_owner[c] : ipx_hub_of_chunk(prefix, n, c);
     h.v = list[h.i];
     h.c0 = prefix[h.i];
     h.nch = prefix[h.i + 1] - h.c0;
@@ -1861,14 +1872,31 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_GATHER_CTAS) ipx_k_gather_com
             v = vn;
         }
     } else if constexpr (MODE == 1) {
+        /* the next vertex's list entry and row bounds are loaded while this
+         * vertex's in-edges are folded */
         const int lane = threadIdx.x & 31;
-        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
-            const uint64_t v = list[i];
+        const uint64_t stride = ipx_gstride() >> 5;
+        uint64_t i = ipx_gtid() >> 5, v = 0, r0 = 0, r1 = 0;
+        if (i < n) {
+            v = list[i];
+            r0 = row[v];
+            r1 = row[v + 1];
+        }
+        for (; i < n; i += stride) {
+            uint64_t vn = 0, r0n = 0, r1n = 0;
+            if (i + stride < n) {
+                vn = list[i + stride];
+                r0n = row[vn];
+                r1n = row[vn + 1];
+            }
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], lane, 32, has, acc);
+            ipx_gather_fold_edges(adj, bs, stamp, r0, r1, lane, 32, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
+            v = vn;
+            r0 = r0n;
+            r1 = r1n;
         }
     } else {
         /* hubs in chunks of IPX_HUB_CHUNK in-edges, spread over all CTAs

@@ -373,7 +373,14 @@ static int ipx_setup_state()
         IPX_CU(cudaMemcpy(dcount, &n2u, 4, cudaMemcpyHostToDevice));
         ipx_k_hub_prefix<<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
         IPX_CU(cudaGetLastError());
+        uint32_t total = 0;
+        IPX_CU(cudaMemcpy(&total, ipx_h.pull_prefix + n2, 4, cudaMemcpyDeviceToHost));
+        uint32_t* owner = nullptr;
+        IPX_OK(ipx_alloc(&owner, (uint64_t)total + 1));
+        if (n2) ipx_k_chunk_owner<<<ipx_grid(4), 256>>>(ipx_h.pull_prefix, n2, owner);
+        IPX_CU(cudaGetLastError());
         IPX_CU(cudaDeviceSynchronize());
+        c.hub_owner = owner;
     }
 #endif
 #if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
