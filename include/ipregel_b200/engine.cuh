@@ -90,6 +90,7 @@ static_assert(sizeof(ipx_msg) <= 8, "iPregel-B200: IP_MESSAGE_TYPE must be at mo
 #define IPX_ERR_COMBINE_HINT 2u
 #define IPX_ERR_SUPERSTEP_LIMIT 4u
 #define IPX_ERR_COPY_TIMEOUT 8u
+#define IPX_ERR_RESERVED_MESSAGE 16u
 #define IPX_HIST 65536
 
 /* Default degree-class thresholds for the thread / warp / block kernels
@@ -496,6 +497,14 @@ __device__ __forceinline__ unsigned long long ipx_bslot_bits(const uint4& w)
 __device__ __forceinline__ uint32_t ipx_bslot_stamp(const uint2& w) { return w.y; }
 __device__ __forceinline__ uint32_t ipx_bslot_stamp(const uint4& w) { return w.z; }
 
+/* A slot that holds no broadcast. */
+__device__ __forceinline__ ipx_bslot make_ipx_nobslot()
+{
+    ipx_bslot w;
+    memset(&w, 0xff, sizeof w);
+    return w;
+}
+
 __device__ __forceinline__ void ipx_bslot_put(ipx_bslot* p, const ipx_msg& m, uint32_t stamp)
 {
     ipx_bslot_store(p, (unsigned long long)ipx_to_word(m), stamp);
@@ -507,6 +516,39 @@ __device__ __forceinline__ bool ipx_bslot_take(const ipx_bslot& w, uint32_t stam
 {
     m = ipx_from_word<ipx_msg>((typename ipx_word<ipx_msg>::type)ipx_bslot_bits(w));
     return ipx_bslot_stamp(w) == stamp;
+}
+
+/* The single_broadcast version with FP64 messages (PageRank) keeps 8-byte
+ * slots without a stamp: its fused kernel visits every vertex each
+ * superstep and writes every slot of the next buffer -- the broadcast, or
+ * IPX_ABSENT64 when the vertex does not broadcast -- so a slot never holds
+ * a message of an older superstep.  IPX_ABSENT64 (all bits set) is a NaN
+ * that FP64 arithmetic does not produce; a broadcast of exactly that bit
+ * pattern is reported as an error (IPX_ERR_RESERVED_MESSAGE).  Half the
+ * bytes of a stamped 16-byte slot: twice as many vertices' slots fit in the
+ * L2.  Other message types keep stamped slots. */
+#ifndef IPX_SB_DENSE
+#define IPX_SB_DENSE 1
+#endif
+#define IPX_ABSENT64 0xffffffffffffffffULL
+typedef typename std::conditional<(IPX_SB_DENSE && std::is_same<ipx_msg, double>::value), unsigned long long,
+                                  ipx_bslot>::type ipx_sbslot;
+
+__device__ __forceinline__ bool ipx_slot_take(const ipx_bslot& w, uint32_t stamp, ipx_msg& m)
+{
+    return ipx_bslot_take(w, stamp, m);
+}
+__device__ __forceinline__ bool ipx_slot_take(const unsigned long long& w, uint32_t, ipx_msg& m)
+{
+    m = ipx_from_word<ipx_msg>((typename ipx_word<ipx_msg>::type)w);
+    return w != IPX_ABSENT64;
+}
+template <class S>
+__device__ __forceinline__ S ipx_no_slot()
+{
+    S w;
+    memset(&w, 0xff, sizeof w);
+    return w;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -537,6 +579,7 @@ struct ipx_consts {
      * fused kernel reads superstep s's slots while writing s+1's);
      * spread+single_broadcast uses bslot[0] */
     ipx_bslot* bslot[2];
+    ipx_sbslot* sbslot[2];
     uint32_t* bt;
     /* counters: [0..3] active counts ring, [4] edges, [5] error word */
     unsigned long long* ctr;
@@ -1201,8 +1244,9 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
  * A warp or block (lanes >= 32) with 32-bit ids reads the ids 128 bits at a
  * time instead: four consecutive in-edges per lane and load instruction
  * (ipx_gather_fold_edges_v4). */
+template <class S>
 __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restrict__ adj,
-                                                         const ipx_bslot* __restrict__ bs, uint32_t stamp,
+                                                         const S* __restrict__ bs, uint32_t stamp,
                                                          uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
                                                          bool& has, ipx_msg& acc)
 {
@@ -1218,16 +1262,16 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
         if (lane < nh) e = e0 + lane;
         else if (lane < nh + nt) e = b + (lane - nh);
         if (e < e1) {
-            const ipx_bslot w = __ldg(&bs[adj[e]]);
+            const S w = __ldg(&bs[adj[e]]);
             ipx_msg m;
-            if (ipx_bslot_take(w, stamp, m)) ipx_fold(has, acc, true, m);
+            if (ipx_slot_take(w, stamp, m)) ipx_fold(has, acc, true, m);
         }
     }
     const uint4* __restrict__ q = reinterpret_cast<const uint4*>(adj + a);
     const uint64_t groups = (b - a) >> 2;
     for (uint64_t g = lane; g < groups; g += lanes) {
         const uint4 id = __ldcs(q + g);
-        ipx_bslot w[4];
+        S w[4];
         w[0] = __ldg(&bs[id.x]);
         w[1] = __ldg(&bs[id.y]);
         w[2] = __ldg(&bs[id.z]);
@@ -1235,13 +1279,14 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             ipx_msg m;
-            if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+            if (ipx_slot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
         }
     }
 }
 
+template <class S>
 __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict__ adj,
-                                                      const ipx_bslot* __restrict__ bs, uint32_t stamp, uint64_t e0,
+                                                      const S* __restrict__ bs, uint32_t stamp, uint64_t e0,
                                                       uint64_t e1, uint64_t lane, uint64_t lanes, bool& has,
                                                       ipx_msg& acc)
 {
@@ -1255,22 +1300,17 @@ __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict_
     }
     for (uint64_t e = e0 + lane; e < e1; e += IPX_UNROLL * lanes) {
         uint64_t u[IPX_UNROLL];
-        ipx_bslot w[IPX_UNROLL];
+        S w[IPX_UNROLL];
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++)
             u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_edge(&adj[e + k * lanes], lanes) : 0;
 #pragma unroll
-        for (int k = 0; k < IPX_UNROLL; k++) {
-            if (e + k * lanes < e1) {
-                w[k] = __ldg(&bs[u[k]]);
-            } else {
-                memset(&w[k], 0xff, sizeof w[k]); /* no broadcast */
-            }
-        }
+        for (int k = 0; k < IPX_UNROLL; k++)
+            w[k] = (e + k * lanes < e1) ? __ldg(&bs[u[k]]) : ipx_no_slot<S>();
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             ipx_msg m;
-            if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+            if (ipx_slot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
         }
     }
 }
@@ -1557,6 +1597,23 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32
     }
 }
 
+/* The single_broadcast version's record of a vertex's broadcast (or of
+ * none) for the superstep `stamp`: a stamped slot is written only for a
+ * broadcast; a dense slot every time. */
+__device__ __forceinline__ void ipx_sb_put(ipx_bslot* p, bool out, const ipx_msg& m, uint32_t stamp)
+{
+    if (out) ipx_bslot_put(p, m, stamp);
+}
+__device__ __forceinline__ void ipx_sb_put(unsigned long long* p, bool out, const ipx_msg& m, uint32_t)
+{
+    unsigned long long w = IPX_ABSENT64;
+    if (out) {
+        w = (unsigned long long)ipx_to_word(m);
+        if (w == IPX_ABSENT64) atomicOr(ipx_c.err, IPX_ERR_RESERVED_MESSAGE);
+    }
+    *p = w;
+}
+
 /* Single broadcast (pull), superstep 0's compute phase
  * (combiner_single_broadcast_postamble.h:185-201): every vertex is active and
  * has no message.  A broadcast writes the vertex's slot in buffer 0 stamped
@@ -1568,9 +1625,12 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb0()
 {
     if (ipx_step() != 0) return;
     const uint64_t V = ipx_c.V;
-    ipx_bslot* __restrict__ out = ipx_c.bslot[0];
+    ipx_sbslot* __restrict__ out = ipx_c.sbslot[0];
     for (uint64_t v = ipx_gtid(); v < V; v += ipx_gstride()) {
-        if (!ipx_c.active_b[v]) continue;
+        if (!ipx_c.active_b[v]) {
+            ipx_sb_put(&out[v], false, ipx_msg(), 0u);
+            continue;
+        }
         struct ip_vertex_t x;
         x.id = (ipx_vid)v;
         x.active = true;
@@ -1582,7 +1642,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb0()
         ip_compute(&x);
         if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
         if (!x.active) ipx_c.active_b[v] = 0;
-        if (x.ipx_has_out) ipx_bslot_put(&out[v], x.ipx_out, 0u);
+        ipx_sb_put(&out[v], x.ipx_has_out, x.ipx_out, 0u);
     }
 }
 
@@ -1590,11 +1650,14 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb0()
  * compute(s), or a message reactivates it, :65-71), and if so its compute
  * phase of superstep s+1 (:185-201) with the gathered message; a broadcast
  * goes to `out` stamped s+1.  Returns the activity that superstep s counts. */
-__device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const ipx_msg& acc, ipx_bslot* out,
+__device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const ipx_msg& acc, ipx_sbslot* out,
                                                     uint32_t next_stamp)
 {
     const bool a0 = ipx_c.active_b[v] != 0;
-    if (!a0 && !has) return false;
+    if (!a0 && !has) {
+        ipx_sb_put(&out[v], false, acc, next_stamp);
+        return false;
+    }
     struct ip_vertex_t x;
     x.id = (ipx_vid)v;
     x.active = true;
@@ -1607,7 +1670,7 @@ __device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const 
     ip_compute(&x);
     if (!ipx_same_bits(x.value, v0)) ipx_c.value[v] = x.value;
     if (x.active != a0) ipx_c.active_b[v] = x.active ? 1 : 0;
-    if (x.ipx_has_out) ipx_bslot_put(&out[v], x.ipx_out, next_stamp);
+    ipx_sb_put(&out[v], x.ipx_has_out, x.ipx_out, next_stamp);
     return true;
 }
 
@@ -1687,7 +1750,7 @@ __device__ __forceinline__ void ipx_locate_chunk(const uint32_t* __restrict__ li
  * and runs the vertex's compute phase of the next superstep.  Returns the
  * count the caller adds (thread 0 only). */
 __device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_chunk& h, bool has, ipx_msg acc,
-                                                                 ipx_bslot* out, uint32_t next_stamp)
+                                                                 ipx_sbslot* out, uint32_t next_stamp)
 {
     bool last = h.nch == 1;
     if (!last) {
@@ -1708,6 +1771,107 @@ __device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_c
     return last ? (unsigned long long)ipx_sb_compute_next(h.v, has, acc, out, next_stamp) : 0ULL;
 }
 
+/* 1: the warp class of the fused pull kernel takes 32 vertices per warp and
+ * spreads their concatenated in-edges over its lanes (ipx_gather_expand);
+ * 0: a warp per vertex. */
+#ifndef IPX_GATHER_EXPAND
+#define IPX_GATHER_EXPAND 1
+#endif
+#ifndef IPX_EXPAND_STEPS
+#define IPX_EXPAND_STEPS 4
+#endif
+
+/* The warp class of ipx_k_gather_compute, edge-balanced.  Most vertices of
+ * the class have a few dozen in-edges, so a warp per vertex leaves most
+ * lanes idle and pays the list -> row -> ids -> slots chain once per vertex.
+ * Here a warp takes 32 vertices of the list (lane j owns vertex j), scans
+ * their in-degrees, and walks the concatenated edges 32 per step, lane by
+ * lane: each lane finds its vertex by a 5-step search of the exclusive
+ * degree prefix, loads the id and the slot (IPX_EXPAND_STEPS steps' loads
+ * in flight), the lanes of each vertex fold their messages by a segmented
+ * reduction (a lane folds in its right neighbour's partial while it belongs
+ * to the same vertex), and the vertex's owner lane folds the segment's
+ * result into its own.  A vertex's messages are folded in edge order within
+ * a step, as a tree, and step after step: only the order of the ip_combine
+ * calls differs from the reference's sequential fold.  Then every lane runs
+ * the compute phase of its own vertex.  Degrees are below 2^32 / 32 (the
+ * class bound t1). */
+__device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* __restrict__ list, uint64_t n,
+                                                                const ipx_vid* __restrict__ adj,
+                                                                const uint64_t* __restrict__ row,
+                                                                const ipx_sbslot* __restrict__ bs, uint32_t stamp,
+                                                                ipx_sbslot* __restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ipx_gstride() >> 5;
+    unsigned long long cnt = 0;
+    for (uint64_t base = (ipx_gtid() >> 5) * 32; base < n; base += nwarps * 32) {
+        const bool valid = base + lane < n;
+        uint64_t v = 0, r0 = 0;
+        uint32_t deg = 0;
+        if (valid) {
+            v = list[base + lane];
+            r0 = row[v];
+            deg = (uint32_t)(row[v + 1] - r0);
+        }
+        uint32_t inc = deg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(IPX_FULL, inc, o);
+            if (lane >= o) inc += t;
+        }
+        const uint32_t excl = inc - deg;
+        const uint32_t total = __shfl_sync(IPX_FULL, inc, 31);
+        bool has = false;
+        ipx_msg acc;
+        for (uint32_t t0 = 0; t0 < total; t0 += 32 * IPX_EXPAND_STEPS) {
+            int jk[IPX_EXPAND_STEPS];
+            ipx_sbslot w[IPX_EXPAND_STEPS];
+#pragma unroll
+            for (int k = 0; k < IPX_EXPAND_STEPS; k++) {
+                const uint32_t pos = t0 + (uint32_t)(32 * k + lane);
+                int j = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const uint32_t ex = __shfl_sync(IPX_FULL, excl, j + st);
+                    if (ex <= pos) j += st;
+                }
+                const uint64_t rj = __shfl_sync(IPX_FULL, r0, j);
+                const uint32_t xj = __shfl_sync(IPX_FULL, excl, j);
+                jk[k] = pos < total ? j : 32 + lane; /* past the end: a segment of its own */
+                w[k] = ipx_no_slot<ipx_sbslot>();
+                if (pos < total) {
+                    const uint64_t u = (uint64_t)ipx_ld_stream(&adj[rj + (pos - xj)]);
+                    w[k] = __ldg(&bs[u]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < IPX_EXPAND_STEPS; k++) {
+                ipx_msg m;
+                bool h = ipx_slot_take(w[k], stamp, m);
+                const int j = jk[k];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const bool h2 = __shfl_down_sync(IPX_FULL, h, o);
+                    const ipx_msg m2 = ipx_shfl_down(m, o);
+                    const int j2 = __shfl_down_sync(IPX_FULL, j, o);
+                    if (lane + o < 32 && j2 == j) ipx_fold(h, m, h2, m2);
+                }
+                /* lane j's segment in this step starts at its first edge
+                 * here (or at lane 0 when it began in an earlier step) */
+                const uint32_t ts = t0 + 32u * k;
+                const bool meets = deg && excl < ts + 32 && excl + deg > ts;
+                const int src = meets ? (int)(excl > ts ? excl - ts : 0u) : lane;
+                const bool hs = __shfl_sync(IPX_FULL, h, src);
+                const ipx_msg ms = ipx_shfl_idx(m, src);
+                if (meets) ipx_fold(has, acc, hs, ms);
+            }
+        }
+        if (valid) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
+    }
+    return cnt;
+}
+
 #ifndef IPX_HUB_SMEM
 #define IPX_HUB_SMEM 1
 #endif
@@ -1724,8 +1888,8 @@ __device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_c
  * rest of the launch; results stay exact. */
 __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
     const uint32_t* __restrict__ adj, const uint64_t* __restrict__ row, const uint32_t* __restrict__ list, uint64_t n,
-    const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_bslot* __restrict__ bs, uint32_t stamp,
-    ipx_bslot* __restrict__ out)
+    const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_sbslot* __restrict__ bs, uint32_t stamp,
+    ipx_sbslot* __restrict__ out)
 {
     __shared__ __align__(16) uint32_t s_ids[2][IPX_HUB_CHUNK + 4];
     __shared__ __align__(8) uint64_t s_bar[2];
@@ -1777,7 +1941,7 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
         ipx_msg acc;
         for (uint64_t e = h.e0 + threadIdx.x; e < h.e1; e += IPX_UNROLL * (uint64_t)nthr) {
             uint32_t u[IPX_UNROLL];
-            ipx_bslot w[IPX_UNROLL];
+            ipx_sbslot w[IPX_UNROLL];
 #pragma unroll
             for (int k = 0; k < IPX_UNROLL; k++) {
                 const uint64_t ek = e + (uint64_t)k * nthr;
@@ -1785,16 +1949,12 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
             }
 #pragma unroll
             for (int k = 0; k < IPX_UNROLL; k++) {
-                if (e + (uint64_t)k * nthr < h.e1) {
-                    w[k] = __ldg(&bs[u[k]]);
-                } else {
-                    memset(&w[k], 0xff, sizeof w[k]);
-                }
+                w[k] = (e + (uint64_t)k * nthr < h.e1) ? __ldg(&bs[u[k]]) : ipx_no_slot<ipx_sbslot>();
             }
 #pragma unroll
             for (int k = 0; k < IPX_UNROLL; k++) {
                 ipx_msg m;
-                if (ipx_bslot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
+                if (ipx_slot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
             }
         }
         ipx_warp_fold(has, acc);
@@ -1846,8 +2006,13 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
 #define IPX_GATHER_CTAS 5
 #endif
 
+#ifndef IPX_EXPAND_CTAS
+#define IPX_EXPAND_CTAS 4
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(IPX_THREADS, IPX_GATHER_CTAS) ipx_k_gather_compute(const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) ? IPX_EXPAND_CTAS : IPX_GATHER_CTAS)
+    ipx_k_gather_compute(const uint32_t* __restrict__ list,
                                                                                   uint64_t n,
                                                                                   const uint32_t* __restrict__ prefix)
 {
@@ -1855,8 +2020,8 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_GATHER_CTAS) ipx_k_gather_com
     const uint32_t stamp = (uint32_t)s;
     const ipx_vid* __restrict__ adj = ipx_c.in_adj;
     const uint64_t* __restrict__ row = ipx_c.in_row;
-    const ipx_bslot* __restrict__ bs = ipx_c.bslot[s & 1];
-    ipx_bslot* __restrict__ out = ipx_c.bslot[(s + 1) & 1];
+    const ipx_sbslot* __restrict__ bs = ipx_c.sbslot[s & 1];
+    ipx_sbslot* __restrict__ out = ipx_c.sbslot[(s + 1) & 1];
     unsigned long long cnt = 0;
     if constexpr (MODE == 0) {
         /* the next vertex's list entry is loaded while this vertex's
@@ -1871,6 +2036,8 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_GATHER_CTAS) ipx_k_gather_com
             cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
             v = vn;
         }
+    } else if constexpr (MODE == 1 && IPX_GATHER_EXPAND) {
+        cnt += ipx_gather_expand(list, n, adj, row, bs, stamp, out);
     } else if constexpr (MODE == 1) {
         /* the next vertex's list entry and row bounds are loaded while this
          * vertex's in-edges are folded */

@@ -95,6 +95,7 @@ struct ipx_host_state {
     int tb = IPX_THREADS;      /* CTA size in use */
     uint32_t grid_compute = 0; /* resident CTAs of the compute kernel */
     uint32_t grid_edge = 0;    /* resident CTAs of the edge kernels */
+    uint32_t grid_gather[3] = {0, 0, 0}; /* single_broadcast: of each class's fused kernel */
     std::vector<struct ip_vertex_t> host_vertices;
     bool host_valid = false;
     char err[512] = {0};
@@ -242,8 +243,8 @@ static int ipx_reset_vertex_state()
     IPX_CU(cudaMemsetAsync(c.bcaster, 0, W * 4 + 4, st));
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
     /* every stamp IPX_NO_STAMP: no slot counts in any superstep */
-    IPX_CU(cudaMemsetAsync(c.bslot[0], 0xff, (V ? V : 1) * sizeof(ipx_bslot), st));
-    IPX_CU(cudaMemsetAsync(c.bslot[1], 0xff, (V ? V : 1) * sizeof(ipx_bslot), st));
+    IPX_CU(cudaMemsetAsync(c.sbslot[0], 0xff, (V ? V : 1) * sizeof(ipx_sbslot), st));
+    IPX_CU(cudaMemsetAsync(c.sbslot[1], 0xff, (V ? V : 1) * sizeof(ipx_sbslot), st));
     IPX_CU(cudaMemsetAsync(c.hub_arrived, 0, (ipx_h.gbins.count[2] + 1) * sizeof(uint32_t), st));
 #else
     IPX_CU(cudaMemsetAsync(c.hasmsg_b, 0, V + 1, st));
@@ -354,8 +355,8 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&c.bslot[0], V));
 #endif
 #if IPX_VERSION == IPX_SINGLE_BROADCAST
-    IPX_OK(ipx_alloc(&c.bslot[0], V));
-    IPX_OK(ipx_alloc(&c.bslot[1], V));
+    IPX_OK(ipx_alloc(&c.sbslot[0], V));
+    IPX_OK(ipx_alloc(&c.sbslot[1], V));
     IPX_OK(ipx_alloc(&c.active_b, V + 1));
     IPX_OK(ipg_graph_bins(ipx_h.g, 1, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
     {
@@ -414,6 +415,9 @@ static int ipx_setup_state()
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb0, tb, per_sm);
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather_compute<1>, tb, per_sm);
+        ipx_h.grid_gather[0] = ipx_resident_grid(ipx_k_gather_compute<0>, tb, per_sm);
+        ipx_h.grid_gather[1] = ipx_h.grid_edge;
+        ipx_h.grid_gather[2] = ipx_resident_grid(ipx_k_gather_compute<2>, tb, per_sm);
 #else
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb, tb, per_sm);
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, false>, tb, per_sm);
@@ -625,6 +629,9 @@ static int ipx_end_superstep(uint64_t s, uint64_t* count, uint64_t frontier)
                         "broadcast() should be called, and once per superstep maximum.");
     if (err & IPX_ERR_COPY_TIMEOUT)
         return ipx_fail(IPG_EDEVICE, "a bulk copy into shared memory did not complete in time (results kept exact)");
+    if (err & IPX_ERR_RESERVED_MESSAGE)
+        return ipx_fail(IPG_EDEVICE, "a broadcast FP64 message had all 64 bits set, the pattern the single_broadcast "
+                                     "engine reserves for 'no broadcast' (build with -DIPX_SB_DENSE=0 to allow it)");
     if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
 #if IPX_VERSION == IPX_COMBINER || IPX_VERSION == IPX_SINGLE_BROADCAST
     *count = ipx_h.h_ctr[s & 3];
@@ -704,14 +711,14 @@ static int ipx_enqueue_superstep()
         /* gather of this superstep fused with the next one's compute phase */
         const ipg_bins& b = ipx_h.gbins;
         if (b.count[0])
-            IPX_LAUNCH(IPX_K_GATHER0,
-                       ipx_k_gather_compute<0><<<ge, ipx_h.tb, 0, st>>>(b.d_list[0], b.count[0], nullptr));
+            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather_compute<0><<<ipx_h.grid_gather[0], ipx_h.tb, 0, st>>>(
+                                          b.d_list[0], b.count[0], nullptr));
         if (b.count[1])
-            IPX_LAUNCH(IPX_K_GATHER1,
-                       ipx_k_gather_compute<1><<<ge, ipx_h.tb, 0, st>>>(b.d_list[1], b.count[1], nullptr));
+            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather_compute<1><<<ipx_h.grid_gather[1], ipx_h.tb, 0, st>>>(
+                                          b.d_list[1], b.count[1], nullptr));
         if (b.count[2])
-            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather_compute<2><<<ge, ipx_h.tb, 0, st>>>(b.d_list[2], b.count[2],
-                                                                                          ipx_h.pull_prefix));
+            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather_compute<2><<<ipx_h.grid_gather[2], ipx_h.tb, 0, st>>>(
+                                          b.d_list[2], b.count[2], ipx_h.pull_prefix));
     }
 #else
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);
@@ -895,6 +902,9 @@ static int ipx_loop_collect(double seconds)
     if (err & IPX_ERR_SUPERSTEP_LIMIT) return ipx_fail(IPG_EDEVICE, "superstep limit (IPG_MAX_SUPERSTEPS) reached");
     if (err & IPX_ERR_COPY_TIMEOUT)
         return ipx_fail(IPG_EDEVICE, "a bulk copy into shared memory did not complete in time (results kept exact)");
+    if (err & IPX_ERR_RESERVED_MESSAGE)
+        return ipx_fail(IPG_EDEVICE, "a broadcast FP64 message had all 64 bits set, the pattern the single_broadcast "
+                                     "engine reserves for 'no broadcast' (build with -DIPX_SB_DENSE=0 to allow it)");
     if (err) return ipx_fail(IPG_EDEVICE, "a kernel reported an error");
     return IPG_OK;
 }
@@ -1259,6 +1269,9 @@ int ipg_app_set_tuning(int block, uint64_t t0, uint64_t t1, uint64_t pull_div)
     if (block < 32 || block > IPX_THREADS || (block & 31))
         return ipx_fail(IPG_EINVAL, "ipg_app_set_tuning: block must be a multiple of 32 in [32, 256]");
     if (t0 < 1 || t1 < t0) return ipx_fail(IPG_EINVAL, "ipg_app_set_tuning: need 1 <= t0 <= t1");
+    /* a warp of the pull gather sums the degrees of 32 vertices of the
+     * middle class in 32 bits */
+    if (t1 > (1ULL << 26)) return ipx_fail(IPG_EINVAL, "ipg_app_set_tuning: t1 above 2^26");
     ipx_h.tune.block = block;
     ipx_h.tune.t0 = t0;
     ipx_h.tune.t1 = t1;
