@@ -1773,9 +1773,12 @@ __device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_c
 
 /* 1: the warp class of the fused pull kernel takes 32 vertices per warp and
  * spreads their concatenated in-edges over its lanes (ipx_gather_expand);
- * 0: a warp per vertex. */
+ * 0: a warp per vertex.  Measured on directed R-MAT scale 25 (FP64
+ * PageRank, 30 rounds): 191 ms with the expansion against 135 ms without
+ * (its shuffles and segmented folds cost more than the idle lanes of the
+ * warp per vertex), so it is off. */
 #ifndef IPX_GATHER_EXPAND
-#define IPX_GATHER_EXPAND 1
+#define IPX_GATHER_EXPAND 0
 #endif
 #ifndef IPX_EXPAND_STEPS
 #define IPX_EXPAND_STEPS 4
