@@ -551,6 +551,52 @@ __device__ __forceinline__ S ipx_no_slot()
     return w;
 }
 
+/* ---- L2 eviction policies for the gathered slots ----
+ * The slots of a few million often-gathered vertices would fit the L2, but
+ * the gather's cold accesses (most vertices are gathered a few times per
+ * superstep) evict them.  The single_broadcast version can gather from a
+ * copy of the in-lists whose ids carry a flag in bit 31 for the vertices
+ * gathered most often (ipx_consts::in_adj_hot, built at attach): their
+ * slots are loaded evict-last, all others evict-first. */
+#define IPX_HOT_BIT 0x80000000u
+__device__ __forceinline__ uint64_t ipx_policy(bool hot)
+{
+    uint64_t p;
+    if (hot) asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long ipx_ld_policy(const unsigned long long* p, uint64_t pol)
+{
+    unsigned long long r;
+    asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(r) : "l"(p), "l"(pol));
+    return r;
+}
+__device__ __forceinline__ uint2 ipx_ld_policy(const uint2* p, uint64_t pol)
+{
+    uint2 r;
+    asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(r.x), "=r"(r.y) : "l"(p), "l"(pol));
+    return r;
+}
+__device__ __forceinline__ uint4 ipx_ld_policy(const uint4* p, uint64_t pol)
+{
+    uint4 r;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p), "l"(pol));
+    return r;
+}
+/* The slot of the in-neighbour whose id word is w: HOT ids carry the flag. */
+template <bool HOT, class S>
+__device__ __forceinline__ S ipx_slot_ld(const S* __restrict__ bs, uint64_t w)
+{
+    if constexpr (HOT) {
+        return ipx_ld_policy(&bs[w & (IPX_HOT_BIT - 1u)], ipx_policy((w & IPX_HOT_BIT) != 0));
+    } else {
+        return __ldg(&bs[w]);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Device-resident engine state, read through the constant bank.            */
 /* ------------------------------------------------------------------------ */
@@ -597,6 +643,8 @@ struct ipx_consts {
     uint32_t* hub_arrived;
     /* chunk -> index of its hub in the static hub class (built at attach) */
     const uint32_t* hub_owner;
+    /* the in-lists with the flag of the most gathered vertices (null: none) */
+    const uint32_t* in_adj_hot;
 };
 
 __constant__ ipx_consts ipx_c;
@@ -1006,6 +1054,37 @@ __global__ void ipx_k_chunk_owner(const uint32_t* __restrict__ prefix, uint64_t 
         for (uint32_t c = prefix[i]; c < prefix[i + 1]; c++) owner[c] = (uint32_t)i;
 }
 
+/* ---- the flagged in-lists of the single_broadcast gather (attach time) ---- */
+/* cnt[u] += 1 for every occurrence of u in the in-lists. */
+__global__ void ipx_k_count_occurrences(const uint32_t* __restrict__ adj, uint64_t E, uint32_t* __restrict__ cnt)
+{
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[adj[e]], 1u);
+}
+
+/* hist[b] = vertices whose occurrence count has b significant bits. */
+__global__ void ipx_k_count_hist(const uint32_t* __restrict__ cnt, uint64_t V, unsigned long long* __restrict__ hist)
+{
+    __shared__ unsigned int h[33];
+    if (threadIdx.x < 33) h[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[32 - __clz(cnt[v])], 1u);
+    __syncthreads();
+    if (threadIdx.x < 33 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], (unsigned long long)h[threadIdx.x]);
+}
+
+/* out[e] = adj[e], with IPX_HOT_BIT set when that vertex occurs at least
+ * `threshold` times in the in-lists. */
+__global__ void ipx_k_flag_hot(const uint32_t* __restrict__ adj, uint64_t E, const uint32_t* __restrict__ cnt,
+                               uint32_t threshold, uint32_t* __restrict__ out)
+{
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t u = adj[e];
+        out[e] = u | (cnt[u] >= threshold ? IPX_HOT_BIT : 0u);
+    }
+}
+
 /* Hub index of chunk c: the last i with prefix[i] <= c. */
 __device__ __forceinline__ uint64_t ipx_hub_of_chunk(const uint32_t* __restrict__ prefix, uint64_t n, uint32_t c)
 {
@@ -1244,7 +1323,7 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
  * A warp or block (lanes >= 32) with 32-bit ids reads the ids 128 bits at a
  * time instead: four consecutive in-edges per lane and load instruction
  * (ipx_gather_fold_edges_v4). */
-template <class S>
+template <bool HOT = false, class S>
 __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restrict__ adj,
                                                          const S* __restrict__ bs, uint32_t stamp,
                                                          uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
@@ -1262,7 +1341,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
         if (lane < nh) e = e0 + lane;
         else if (lane < nh + nt) e = b + (lane - nh);
         if (e < e1) {
-            const S w = __ldg(&bs[adj[e]]);
+            const S w = ipx_slot_ld<HOT>(bs, adj[e]);
             ipx_msg m;
             if (ipx_slot_take(w, stamp, m)) ipx_fold(has, acc, true, m);
         }
@@ -1272,10 +1351,10 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
     for (uint64_t g = lane; g < groups; g += lanes) {
         const uint4 id = __ldcs(q + g);
         S w[4];
-        w[0] = __ldg(&bs[id.x]);
-        w[1] = __ldg(&bs[id.y]);
-        w[2] = __ldg(&bs[id.z]);
-        w[3] = __ldg(&bs[id.w]);
+        w[0] = ipx_slot_ld<HOT>(bs, id.x);
+        w[1] = ipx_slot_ld<HOT>(bs, id.y);
+        w[2] = ipx_slot_ld<HOT>(bs, id.z);
+        w[3] = ipx_slot_ld<HOT>(bs, id.w);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             ipx_msg m;
@@ -1284,7 +1363,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
     }
 }
 
-template <class S>
+template <bool HOT = false, class S>
 __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict__ adj,
                                                       const S* __restrict__ bs, uint32_t stamp, uint64_t e0,
                                                       uint64_t e1, uint64_t lane, uint64_t lanes, bool& has,
@@ -1294,7 +1373,8 @@ __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict_
         /* the vector path needs a 16-byte aligned id array (always so for
          * arrays the runtime allocates; a caller's array may not be) */
         if (lanes >= 32 && (reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
-            ipx_gather_fold_edges_v4(reinterpret_cast<const uint32_t*>(adj), bs, stamp, e0, e1, lane, lanes, has, acc);
+            ipx_gather_fold_edges_v4<HOT>(reinterpret_cast<const uint32_t*>(adj), bs, stamp, e0, e1, lane, lanes, has,
+                                          acc);
             return;
         }
     }
@@ -1306,7 +1386,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict_
             u[k] = (e + k * lanes < e1) ? (uint64_t)ipx_ld_edge(&adj[e + k * lanes], lanes) : 0;
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++)
-            w[k] = (e + k * lanes < e1) ? __ldg(&bs[u[k]]) : ipx_no_slot<S>();
+            w[k] = (e + k * lanes < e1) ? ipx_slot_ld<HOT>(bs, u[k]) : ipx_no_slot<S>();
 #pragma unroll
         for (int k = 0; k < IPX_UNROLL; k++) {
             ipx_msg m;
@@ -1889,6 +1969,7 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
  * global memory.  A wait that gives up (never expected) sets
  * IPX_ERR_COPY_TIMEOUT, and the CTA reads ids from global memory for the
  * rest of the launch; results stay exact. */
+template <bool HOT>
 __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
     const uint32_t* __restrict__ adj, const uint64_t* __restrict__ row, const uint32_t* __restrict__ list, uint64_t n,
     const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_sbslot* __restrict__ bs, uint32_t stamp,
@@ -1952,7 +2033,7 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
             }
 #pragma unroll
             for (int k = 0; k < IPX_UNROLL; k++) {
-                w[k] = (e + (uint64_t)k * nthr < h.e1) ? __ldg(&bs[u[k]]) : ipx_no_slot<ipx_sbslot>();
+                w[k] = (e + (uint64_t)k * nthr < h.e1) ? ipx_slot_ld<HOT>(bs, u[k]) : ipx_no_slot<ipx_sbslot>();
             }
 #pragma unroll
             for (int k = 0; k < IPX_UNROLL; k++) {
@@ -2013,7 +2094,7 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
 #define IPX_EXPAND_CTAS 4
 #endif
 
-template <int MODE>
+template <int MODE, bool HOT>
 __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) ? IPX_EXPAND_CTAS : IPX_GATHER_CTAS)
     ipx_k_gather_compute(const uint32_t* __restrict__ list,
                                                                                   uint64_t n,
@@ -2021,7 +2102,8 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
 {
     const uint64_t s = ipx_step();
     const uint32_t stamp = (uint32_t)s;
-    const ipx_vid* __restrict__ adj = ipx_c.in_adj;
+    /* HOT: ids of the in-lists carry the flag of the most gathered vertices */
+    const ipx_vid* __restrict__ adj = HOT ? reinterpret_cast<const ipx_vid*>(ipx_c.in_adj_hot) : ipx_c.in_adj;
     const uint64_t* __restrict__ row = ipx_c.in_row;
     const ipx_sbslot* __restrict__ bs = ipx_c.sbslot[s & 1];
     ipx_sbslot* __restrict__ out = ipx_c.sbslot[(s + 1) & 1];
@@ -2035,11 +2117,11 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             const uint64_t vn = (i + stride < n) ? list[i + stride] : 0;
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, bs, stamp, row[v], row[v + 1], 0, 1, has, acc);
+            ipx_gather_fold_edges<HOT>(adj, bs, stamp, row[v], row[v + 1], 0, 1, has, acc);
             cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
             v = vn;
         }
-    } else if constexpr (MODE == 1 && IPX_GATHER_EXPAND) {
+    } else if constexpr (MODE == 1 && IPX_GATHER_EXPAND && !HOT) {
         cnt += ipx_gather_expand(list, n, adj, row, bs, stamp, out);
     } else if constexpr (MODE == 1) {
         /* the next vertex's list entry and row bounds are loaded while this
@@ -2061,7 +2143,7 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             }
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, bs, stamp, r0, r1, lane, 32, has, acc);
+            ipx_gather_fold_edges<HOT>(adj, bs, stamp, r0, r1, lane, 32, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
             v = vn;
@@ -2082,7 +2164,7 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
         const uint32_t chunks = prefix[n];
         if constexpr (sizeof(ipx_vid) == 4 && IPX_HUB_SMEM) {
             if ((reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
-                cnt += ipx_gather_hubs_staged(reinterpret_cast<const uint32_t*>(adj), row, list, n, prefix, chunks,
+                cnt += ipx_gather_hubs_staged<HOT>(reinterpret_cast<const uint32_t*>(adj), row, list, n, prefix, chunks,
                                               bs, stamp, out);
                 ipx_block_count(cnt, &ipx_c.ctr[s & 3]);
                 return;
@@ -2098,7 +2180,7 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             const ipx_hub_chunk h = s_h;
             bool has = false;
             ipx_msg acc;
-            ipx_gather_fold_edges(adj, bs, stamp, h.e0, h.e1, threadIdx.x, blockDim.x, has, acc);
+            ipx_gather_fold_edges<HOT>(adj, bs, stamp, h.e0, h.e1, threadIdx.x, blockDim.x, has, acc);
             ipx_warp_fold(has, acc);
             if (lane == 0) {
                 s_has[warp] = has;

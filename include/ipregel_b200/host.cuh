@@ -266,6 +266,53 @@ static int ipx_reset_vertex_state()
     return IPG_OK;
 }
 
+#if IPX_VERSION == IPX_SINGLE_BROADCAST
+/* The flagged copy of the in-lists (ipx_consts::in_adj_hot): the vertices
+ * gathered most often, as many as IPG_SB_HOT_KB kilobytes of slots hold
+ * (default 65536, a half of the L2; 0: no copy), have IPX_HOT_BIT set in their ids.  Needs
+ * 32-bit ids and V < 2^31; skipped, not failed, when the copy (4 bytes per
+ * edge) does not fit. */
+static int ipx_build_hot_ids(ipx_consts& c)
+{
+    c.in_adj_hot = nullptr;
+    const uint64_t kb = ipx_env_u64("IPG_SB_HOT_KB", 65536);
+    if (sizeof(ipx_vid) != 4 || kb == 0 || c.V == 0 || c.E == 0 || c.V >= (1ULL << 31)) return IPG_OK;
+    const uint64_t hot_vertices = (kb << 10) / sizeof(ipx_sbslot);
+    void* cnt = nullptr;
+    if (ipg_dev_alloc(&cnt, c.V * 4 + 33 * 8) != IPG_OK) return IPG_OK;
+    unsigned long long* hist = (unsigned long long*)((char*)cnt + ((c.V * 4 + 7) & ~7ULL));
+    uint32_t* out = nullptr;
+    if (ipx_alloc(&out, c.E) != IPG_OK) {
+        ipx_h.err[0] = 0;
+        ipg_dev_free(cnt, c.V * 4 + 33 * 8);
+        return IPG_OK;
+    }
+    int r = IPG_OK;
+    unsigned long long h[33];
+    cudaError_t e = cudaMemset(cnt, 0, c.V * 4 + 33 * 8);
+    if (e == cudaSuccess) {
+        ipx_k_count_occurrences<<<ipx_grid(8), 256>>>((const uint32_t*)c.in_adj, c.E, (uint32_t*)cnt);
+        ipx_k_count_hist<<<ipx_grid(8), 256>>>((const uint32_t*)cnt, c.V, hist);
+        e = cudaMemcpy(h, hist, sizeof h, cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess) {
+        /* the least b whose classes [b, 32] hold at most hot_vertices */
+        int b = 33;
+        uint64_t n = 0;
+        while (b > 1 && n + h[b - 1] <= hot_vertices) n += h[--b];
+        const uint32_t threshold = b > 32 ? 0xffffffffu : (1u << (b - 1));
+        ipx_k_flag_hot<<<ipx_grid(8), 256>>>((const uint32_t*)c.in_adj, c.E, (const uint32_t*)cnt, threshold, out);
+        e = cudaDeviceSynchronize();
+    }
+    ipg_dev_free(cnt, c.V * 4 + 33 * 8);
+    if (e != cudaSuccess) r = ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
+    else c.in_adj_hot = out;
+    return r;
+}
+#else
+static int ipx_build_hot_ids(ipx_consts&) { return IPG_OK; }
+#endif
+
 /* Allocates the version's device state for the attached graph. */
 static int ipx_setup_state()
 {
@@ -383,6 +430,7 @@ static int ipx_setup_state()
         IPX_CU(cudaDeviceSynchronize());
         c.hub_owner = owner;
     }
+    IPX_OK(ipx_build_hot_ids(c));
 #endif
 #if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
     IPX_OK(ipx_alloc(&c.bt, W + 1));
@@ -414,10 +462,16 @@ static int ipx_setup_state()
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_push<1>, tb, per_sm);
 #elif IPX_VERSION == IPX_SINGLE_BROADCAST
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_sb0, tb, per_sm);
-        ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather_compute<1>, tb, per_sm);
-        ipx_h.grid_gather[0] = ipx_resident_grid(ipx_k_gather_compute<0>, tb, per_sm);
+        if (c.in_adj_hot) {
+            ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather_compute<1, true>, tb, per_sm);
+            ipx_h.grid_gather[0] = ipx_resident_grid(ipx_k_gather_compute<0, true>, tb, per_sm);
+            ipx_h.grid_gather[2] = ipx_resident_grid(ipx_k_gather_compute<2, true>, tb, per_sm);
+        } else {
+            ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather_compute<1, false>, tb, per_sm);
+            ipx_h.grid_gather[0] = ipx_resident_grid(ipx_k_gather_compute<0, false>, tb, per_sm);
+            ipx_h.grid_gather[2] = ipx_resident_grid(ipx_k_gather_compute<2, false>, tb, per_sm);
+        }
         ipx_h.grid_gather[1] = ipx_h.grid_edge;
-        ipx_h.grid_gather[2] = ipx_resident_grid(ipx_k_gather_compute<2>, tb, per_sm);
 #else
         ipx_h.grid_compute = ipx_resident_grid(ipx_k_compute_ssb, tb, per_sm);
         ipx_h.grid_edge = ipx_resident_grid(ipx_k_gather<1, false>, tb, per_sm);
@@ -710,15 +764,22 @@ static int ipx_enqueue_superstep()
     {
         /* gather of this superstep fused with the next one's compute phase */
         const ipg_bins& b = ipx_h.gbins;
+        const bool hot = ipx_h.c.in_adj_hot != nullptr;
         if (b.count[0])
-            IPX_LAUNCH(IPX_K_GATHER0, ipx_k_gather_compute<0><<<ipx_h.grid_gather[0], ipx_h.tb, 0, st>>>(
-                                          b.d_list[0], b.count[0], nullptr));
+            IPX_LAUNCH(IPX_K_GATHER0, hot ? ipx_k_gather_compute<0, true><<<ipx_h.grid_gather[0], ipx_h.tb, 0, st>>>(
+                                                b.d_list[0], b.count[0], nullptr)
+                                          : ipx_k_gather_compute<0, false><<<ipx_h.grid_gather[0], ipx_h.tb, 0, st>>>(
+                                                b.d_list[0], b.count[0], nullptr));
         if (b.count[1])
-            IPX_LAUNCH(IPX_K_GATHER1, ipx_k_gather_compute<1><<<ipx_h.grid_gather[1], ipx_h.tb, 0, st>>>(
-                                          b.d_list[1], b.count[1], nullptr));
+            IPX_LAUNCH(IPX_K_GATHER1, hot ? ipx_k_gather_compute<1, true><<<ipx_h.grid_gather[1], ipx_h.tb, 0, st>>>(
+                                                b.d_list[1], b.count[1], nullptr)
+                                          : ipx_k_gather_compute<1, false><<<ipx_h.grid_gather[1], ipx_h.tb, 0, st>>>(
+                                                b.d_list[1], b.count[1], nullptr));
         if (b.count[2])
-            IPX_LAUNCH(IPX_K_GATHER2, ipx_k_gather_compute<2><<<ipx_h.grid_gather[2], ipx_h.tb, 0, st>>>(
-                                          b.d_list[2], b.count[2], ipx_h.pull_prefix));
+            IPX_LAUNCH(IPX_K_GATHER2, hot ? ipx_k_gather_compute<2, true><<<ipx_h.grid_gather[2], ipx_h.tb, 0, st>>>(
+                                                b.d_list[2], b.count[2], ipx_h.pull_prefix)
+                                          : ipx_k_gather_compute<2, false><<<ipx_h.grid_gather[2], ipx_h.tb, 0, st>>>(
+                                                b.d_list[2], b.count[2], ipx_h.pull_prefix));
     }
 #else
     uint64_t* edges_b = (uint64_t*)(c.ctr + 8);

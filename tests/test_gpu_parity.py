@@ -202,13 +202,17 @@ def test_symmetry_check_and_generator_flag():
 
 @pytest.mark.parametrize("app", ["pagerank", "cc", "sssp"])
 @pytest.mark.parametrize("t0,t1", [(16, 4096), (2, 64), (1, 1), (64, 100000)])
-def test_single_broadcast_degree_classes(app, t0, t1):
+@pytest.mark.parametrize("hot_kb", ["0", "4", "65536"])
+def test_single_broadcast_degree_classes(app, t0, t1, hot_kb, monkeypatch):
     """The single_broadcast gather fused with the next superstep's compute,
     over every split of the in-degree classes: hubs in many chunks of 2048
     in-edges folded by whichever CTA arrives last (t1 = 1, 64), hubs in one
     chunk, rows of every alignment read 128 bits at a time by warps and
-    blocks; host and captured loops; per-superstep counts identical."""
+    blocks; with none, some or all in-neighbours flagged for the L2
+    (IPG_SB_HOT_KB); host and captured loops; per-superstep counts
+    identical."""
     import ipregel_b200 as ip
+    monkeypatch.setenv("IPG_SB_HOT_KB", hot_kb)
     hub = [(0, i) for i in range(1, 9000)] + [(i, 0) for i in range(1, 9000)] + \
           [(i, i + 1) for i in range(1, 8999)] + [(i + 1, i) for i in range(1, 8999)] + [(5, 7000), (7000, 5)]
     graphs = [O.gen_rmat(12, 16, seed=21, undirected=False), O.from_edges(9000, hub),
