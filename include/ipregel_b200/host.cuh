@@ -279,17 +279,18 @@ static int ipx_build_hot_ids(ipx_consts& c)
     if (sizeof(ipx_vid) != 4 || kb == 0 || c.V == 0 || c.E == 0 || c.V >= (1ULL << 31)) return IPG_OK;
     const uint64_t hot_vertices = (kb << 10) / sizeof(ipx_sbslot);
     void* cnt = nullptr;
-    if (ipg_dev_alloc(&cnt, c.V * 4 + 33 * 8) != IPG_OK) return IPG_OK;
-    unsigned long long* hist = (unsigned long long*)((char*)cnt + ((c.V * 4 + 7) & ~7ULL));
+    const uint64_t hist_off = (c.V * 4 + 7) & ~7ULL, tmp_bytes = hist_off + 33 * 8;
+    if (ipg_dev_alloc(&cnt, tmp_bytes) != IPG_OK) return IPG_OK;
+    unsigned long long* hist = (unsigned long long*)((char*)cnt + hist_off);
     uint32_t* out = nullptr;
     if (ipx_alloc(&out, c.E) != IPG_OK) {
         ipx_h.err[0] = 0;
-        ipg_dev_free(cnt, c.V * 4 + 33 * 8);
+        ipg_dev_free(cnt, tmp_bytes);
         return IPG_OK;
     }
     int r = IPG_OK;
     unsigned long long h[33];
-    cudaError_t e = cudaMemset(cnt, 0, c.V * 4 + 33 * 8);
+    cudaError_t e = cudaMemset(cnt, 0, tmp_bytes);
     if (e == cudaSuccess) {
         ipx_k_count_occurrences<<<ipx_grid(8), 256>>>((const uint32_t*)c.in_adj, c.E, (uint32_t*)cnt);
         ipx_k_count_hist<<<ipx_grid(8), 256>>>((const uint32_t*)cnt, c.V, hist);
@@ -304,7 +305,7 @@ static int ipx_build_hot_ids(ipx_consts& c)
         ipx_k_flag_hot<<<ipx_grid(8), 256>>>((const uint32_t*)c.in_adj, c.E, (const uint32_t*)cnt, threshold, out);
         e = cudaDeviceSynchronize();
     }
-    ipg_dev_free(cnt, c.V * 4 + 33 * 8);
+    ipg_dev_free(cnt, tmp_bytes);
     if (e != cudaSuccess) r = ipx_fail(IPG_ECUDA, cudaGetErrorString(e));
     else c.in_adj_hot = out;
     return r;
