@@ -1316,6 +1316,20 @@ __device__ __forceinline__ void ipx_warp_fold(bool& has, ipx_msg& acc)
     }
 }
 
+/* The same over the G lanes of one group (G a power of two <= 32); `mask`
+ * holds the group's lanes. */
+template <int G>
+__device__ __forceinline__ void ipx_group_fold(bool& has, ipx_msg& acc, unsigned mask)
+{
+    typedef typename ipx_word<ipx_msg>::type W;
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        const bool oh = __shfl_down_sync(mask, has, o, G);
+        const ipx_msg om = ipx_from_word<ipx_msg>(__shfl_down_sync(mask, ipx_to_word(acc), o, G));
+        ipx_fold(has, acc, oh, om);
+    }
+}
+
 /* Folds the broadcasts of the in-neighbours at edges e0 + lane, e0 + lane +
  * lanes, ... below e1, in that order.  IPX_UNROLL edges a step: their ids,
  * then their broadcast slots are each loaded for all IPX_UNROLL edges before
@@ -1331,7 +1345,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges_v4(const uint32_t* __restr
 {
     /* [e0, a): up to 3 edges before the first 16-byte boundary; [a, b): whole
      * groups of four; [b, e1): up to 3 edges after.  The 6 or fewer edges of
-     * both ends take one lane each (lanes >= 32). */
+     * both ends take one lane each (lanes >= 8). */
     uint64_t a = (e0 + 3) & ~3ULL;
     if (a > e1) a = e1;
     const uint64_t b = a + ((e1 - a) & ~3ULL);
@@ -1372,7 +1386,7 @@ __device__ __forceinline__ void ipx_gather_fold_edges(const ipx_vid* __restrict_
     if constexpr (sizeof(ipx_vid) == 4) {
         /* the vector path needs a 16-byte aligned id array (always so for
          * arrays the runtime allocates; a caller's array may not be) */
-        if (lanes >= 32 && (reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
+        if (lanes >= 8 && (reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
             ipx_gather_fold_edges_v4<HOT>(reinterpret_cast<const uint32_t*>(adj), bs, stamp, e0, e1, lane, lanes, has,
                                           acc);
             return;
@@ -1958,6 +1972,10 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
 #ifndef IPX_HUB_SMEM
 #define IPX_HUB_SMEM 1
 #endif
+/* Lanes per vertex in the middle (warp) class of the fused pull kernel. */
+#ifndef IPX_GATHER_GROUP
+#define IPX_GATHER_GROUP 32
+#endif
 
 /* The hub class of ipx_k_gather_compute with ids staged in shared memory:
  * two id buffers, each filled by one bulk copy per chunk and completed on
@@ -2123,6 +2141,22 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
         }
     } else if constexpr (MODE == 1 && IPX_GATHER_EXPAND && !HOT) {
         cnt += ipx_gather_expand(list, n, adj, row, bs, stamp, out);
+    } else if constexpr (MODE == 1 && IPX_GATHER_GROUP < 32) {
+        /* IPX_GATHER_GROUP lanes per vertex: most vertices of the class have
+         * a few dozen in-edges, which 8 lanes reading four ids each cover
+         * in one or two steps, so a warp works on 32 / G vertices at once */
+        constexpr int G = IPX_GATHER_GROUP;
+        const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+        const unsigned mask = (G == 32) ? IPX_FULL : (((1u << G) - 1u) << (lane & ~(G - 1)));
+        const uint64_t groups = ipx_gstride() / G;
+        for (uint64_t i = ipx_gtid() / G; i < n; i += groups) {
+            const uint64_t v = list[i];
+            bool has = false;
+            ipx_msg acc;
+            ipx_gather_fold_edges<HOT>(adj, bs, stamp, row[v], row[v + 1], gl, G, has, acc);
+            ipx_group_fold<G>(has, acc, mask);
+            if (gl == 0) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
+        }
     } else if constexpr (MODE == 1) {
         /* the next vertex's list entry and row bounds are loaded while this
          * vertex's in-edges are folded */
