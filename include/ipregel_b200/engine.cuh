@@ -774,6 +774,10 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_HUB_CHUNK
 #define IPX_HUB_CHUNK 2048
 #endif
+/* In-edges per chunk of the single_broadcast gather's hub class. */
+#ifndef IPX_GATHER_CHUNK
+#define IPX_GATHER_CHUNK 2048
+#endif
 #ifndef IPX_UNROLL
 #define IPX_UNROLL 4
 #endif
@@ -1016,6 +1020,7 @@ __device__ __forceinline__ void ipx_warp_expand(const uint32_t* __restrict__ lis
 
 /* Chunk prefix of the high-degree class: prefix[i] = chunks of the hubs before
  * i, prefix[n] = total (one block, a carried scan over tiles of its width). */
+template <uint32_t CHUNK = IPX_HUB_CHUNK>
 __global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restrict__ list,
                                                          const uint32_t* __restrict__ count,
                                                          const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix)
@@ -1028,7 +1033,7 @@ __global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restr
         uint32_t c = 0;
         if (i < n) {
             const uint64_t u = list[i];
-            c = (uint32_t)((row[u + 1] - row[u] + IPX_HUB_CHUNK - 1) / IPX_HUB_CHUNK);
+            c = (uint32_t)((row[u + 1] - row[u] + CHUNK - 1) / CHUNK);
         }
         s[threadIdx.x] = c;
         __syncthreads();
@@ -1832,9 +1837,9 @@ __device__ __forceinline__ void ipx_locate_chunk(const uint32_t* __restrict__ li
     h.v = list[h.i];
     h.c0 = prefix[h.i];
     h.nch = prefix[h.i + 1] - h.c0;
-    h.e0 = row[h.v] + (uint64_t)(c - h.c0) * IPX_HUB_CHUNK;
+    h.e0 = row[h.v] + (uint64_t)(c - h.c0) * IPX_GATHER_CHUNK;
     const uint64_t end = row[h.v + 1];
-    h.e1 = (h.e0 + IPX_HUB_CHUNK < end) ? h.e0 + IPX_HUB_CHUNK : end;
+    h.e1 = (h.e0 + IPX_GATHER_CHUNK < end) ? h.e0 + IPX_GATHER_CHUNK : end;
     h.a0 = h.e0 & ~3ULL;
     h.b = h.e1 & ~3ULL;
 }
@@ -1972,9 +1977,12 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
 #ifndef IPX_HUB_SMEM
 #define IPX_HUB_SMEM 1
 #endif
-/* Lanes per vertex in the middle (warp) class of the fused pull kernel. */
+/* Lanes per vertex in the middle class of the fused pull kernel.  On
+ * directed R-MAT scale 25 (FP64 PageRank, 30 rounds) 16 lanes took 118 ms,
+ * 8 lanes 119 ms and a whole warp 135 ms: most vertices of the class have a
+ * few dozen in-edges. */
 #ifndef IPX_GATHER_GROUP
-#define IPX_GATHER_GROUP 32
+#define IPX_GATHER_GROUP 16
 #endif
 
 /* The hub class of ipx_k_gather_compute with ids staged in shared memory:
@@ -1993,7 +2001,7 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
     const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_sbslot* __restrict__ bs, uint32_t stamp,
     ipx_sbslot* __restrict__ out)
 {
-    __shared__ __align__(16) uint32_t s_ids[2][IPX_HUB_CHUNK + 4];
+    __shared__ __align__(16) uint32_t s_ids[2][IPX_GATHER_CHUNK + 4];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ ipx_hub_chunk s_h[2];
     __shared__ bool s_has[IPX_THREADS / 32];
@@ -2185,7 +2193,7 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             r1 = r1n;
         }
     } else {
-        /* hubs in chunks of IPX_HUB_CHUNK in-edges, spread over all CTAs
+        /* hubs in chunks of IPX_GATHER_CHUNK in-edges, spread over all CTAs
          * (one hub's row would otherwise keep one CTA busy long after the
          * others finished): each chunk's fold is stored, and the CTA whose
          * chunk arrives last folds the partials in chunk order, then runs

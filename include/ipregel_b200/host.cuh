@@ -393,7 +393,7 @@ static int ipx_setup_state()
         IPX_OK(ipx_alloc(&dcount, 1));
         const uint32_t n2 = (uint32_t)ipx_h.gbins.count[2];
         IPX_CU(cudaMemcpy(dcount, &n2, 4, cudaMemcpyHostToDevice));
-        ipx_k_hub_prefix<<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
+        ipx_k_hub_prefix<><<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
         IPX_CU(cudaGetLastError());
         IPX_CU(cudaDeviceSynchronize());
     }
@@ -412,7 +412,7 @@ static int ipx_setup_state()
         /* chunks of the hub class: prefix, partial folds, arrival counters */
         const ipg_bins& b = ipx_h.gbins;
         const uint64_t n2 = b.count[2];
-        const uint64_t max_chunks = b.edges[2] / IPX_HUB_CHUNK + n2 + 1;
+        const uint64_t max_chunks = b.edges[2] / IPX_GATHER_CHUNK + n2 + 1;
         IPX_OK(ipx_alloc(&ipx_h.pull_prefix, n2 + 2));
         IPX_OK(ipx_alloc(&c.hub_part, max_chunks));
         IPX_OK(ipx_alloc(&c.hub_arrived, n2 + 1));
@@ -421,7 +421,7 @@ static int ipx_setup_state()
         IPX_OK(ipx_alloc(&dcount, 1));
         const uint32_t n2u = (uint32_t)n2;
         IPX_CU(cudaMemcpy(dcount, &n2u, 4, cudaMemcpyHostToDevice));
-        ipx_k_hub_prefix<<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
+        ipx_k_hub_prefix<IPX_GATHER_CHUNK><<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
         IPX_CU(cudaGetLastError());
         uint32_t total = 0;
         IPX_CU(cudaMemcpy(&total, ipx_h.pull_prefix + n2, 4, cudaMemcpyDeviceToHost));
@@ -566,7 +566,7 @@ static int ipx_push_class(int k, uint32_t g)
     if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre));
     if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre));
     if (k == 2) {
-        IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre));
+        IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre));
         IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre));
     }
     IPX_CU(cudaGetLastError());
@@ -793,7 +793,7 @@ static int ipx_enqueue_superstep()
                                                    ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
     IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
-    IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, ipx_h.tune.t0, ipx_h.tune.t1, ipx_h.tlist[0], ipx_h.tlist[1],
                                                    ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1, st)));
