@@ -1844,30 +1844,55 @@ __device__ __forceinline__ void ipx_locate_chunk(const uint32_t* __restrict__ li
     h.b = h.e1 & ~3ULL;
 }
 
-/* The CTA's fold of one hub chunk is done (thread 0 holds it): store it;
- * the CTA whose chunk arrives last folds the hub's partials in chunk order
- * and runs the vertex's compute phase of the next superstep.  Returns the
- * count the caller adds (thread 0 only). */
+/* The CTA's fold of one hub chunk is done (thread 0 holds it in has/acc;
+ * every thread of the CTA calls this).  The fold is stored; the CTA whose
+ * chunk arrives last folds the hub's partials in chunk order -- each thread
+ * a contiguous run of them, then the runs in order through the warps and
+ * the CTA -- and thread 0 runs the vertex's compute phase of the next
+ * superstep.  s_has / s_acc: the caller's per-warp shared scratch, free
+ * again when this is called.  Returns the count (thread 0). */
 __device__ __forceinline__ unsigned long long ipx_hub_chunk_done(const ipx_hub_chunk& h, bool has, ipx_msg acc,
-                                                                 ipx_sbslot* out, uint32_t next_stamp)
+                                                                 ipx_sbslot* out, uint32_t next_stamp,
+                                                                 bool* s_has, ipx_msg* s_acc)
 {
-    bool last = h.nch == 1;
-    if (!last) {
-        ipx_bslot_put(&ipx_c.hub_part[h.c], acc, has ? 1u : 0u);
-        __threadfence();
-        last = atomicAdd(&ipx_c.hub_arrived[h.i], 1u) == h.nch - 1;
-        if (last) {
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+        int last = 2; /* a hub of one chunk: its fold is the hub's */
+        if (h.nch != 1) {
+            ipx_bslot_put(&ipx_c.hub_part[h.c], acc, has ? 1u : 0u);
             __threadfence();
+            last = atomicAdd(&ipx_c.hub_arrived[h.i], 1u) == h.nch - 1 ? 1 : 0;
+        }
+        s_last = last;
+    }
+    __syncthreads();
+    const int last = s_last;
+    if (last == 1) {
+        __threadfence();
+        const uint32_t nthr = blockDim.x, per = (h.nch + nthr - 1) / nthr;
+        const uint32_t k0 = threadIdx.x * per, k1 = min(k0 + per, h.nch);
+        bool hp = false;
+        ipx_msg ap;
+        for (uint32_t k = k0; k < k1; k++) {
+            const ipx_bslot p = __ldcg(&ipx_c.hub_part[h.c0 + k]);
+            ipx_msg m;
+            if (ipx_bslot_take(p, 1u, m)) ipx_fold(hp, ap, true, m);
+        }
+        ipx_warp_fold(hp, ap);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) {
+            s_has[warp] = hp;
+            s_acc[warp] = ap;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
             has = false;
-            for (uint32_t k = 0; k < h.nch; k++) {
-                const ipx_bslot p = __ldcg(&ipx_c.hub_part[h.c0 + k]);
-                ipx_msg m;
-                if (ipx_bslot_take(p, 1u, m)) ipx_fold(has, acc, true, m);
-            }
+            for (int w = 0; w < (int)(nthr >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
             ipx_c.hub_arrived[h.i] = 0; /* every chunk of the hub has arrived */
         }
     }
-    return last ? (unsigned long long)ipx_sb_compute_next(h.v, has, acc, out, next_stamp) : 0ULL;
+    if (threadIdx.x == 0 && last != 0) return (unsigned long long)ipx_sb_compute_next(h.v, has, acc, out, next_stamp);
+    return 0ULL;
 }
 
 /* 1: the warp class of the fused pull kernel takes 32 vertices per warp and
@@ -1977,6 +2002,10 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
 #ifndef IPX_HUB_SMEM
 #define IPX_HUB_SMEM 1
 #endif
+/* In-edges a thread of the staged hub gather loads per step. */
+#ifndef IPX_HUB_UNROLL
+#define IPX_HUB_UNROLL 4
+#endif
 /* Lanes per vertex in the middle class of the fused pull kernel.  On
  * directed R-MAT scale 25 (FP64 PageRank, 30 rounds) 16 lanes took 118 ms,
  * 8 lanes 119 ms and a whole warp 135 ms: most vertices of the class have a
@@ -2049,20 +2078,20 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
         const uint64_t sb = staged ? h.b : h.e0; /* ids of [e0, sb) from shared memory */
         bool has = false;
         ipx_msg acc;
-        for (uint64_t e = h.e0 + threadIdx.x; e < h.e1; e += IPX_UNROLL * (uint64_t)nthr) {
-            uint32_t u[IPX_UNROLL];
-            ipx_sbslot w[IPX_UNROLL];
+        for (uint64_t e = h.e0 + threadIdx.x; e < h.e1; e += IPX_HUB_UNROLL * (uint64_t)nthr) {
+            uint32_t u[IPX_HUB_UNROLL];
+            ipx_sbslot w[IPX_HUB_UNROLL];
 #pragma unroll
-            for (int k = 0; k < IPX_UNROLL; k++) {
+            for (int k = 0; k < IPX_HUB_UNROLL; k++) {
                 const uint64_t ek = e + (uint64_t)k * nthr;
                 u[k] = (ek < sb) ? s_ids[buf][ek - h.a0] : (ek < h.e1 ? __ldcs(&adj[ek]) : 0u);
             }
 #pragma unroll
-            for (int k = 0; k < IPX_UNROLL; k++) {
+            for (int k = 0; k < IPX_HUB_UNROLL; k++) {
                 w[k] = (e + (uint64_t)k * nthr < h.e1) ? ipx_slot_ld<HOT>(bs, u[k]) : ipx_no_slot<ipx_sbslot>();
             }
 #pragma unroll
-            for (int k = 0; k < IPX_UNROLL; k++) {
+            for (int k = 0; k < IPX_HUB_UNROLL; k++) {
                 ipx_msg m;
                 if (ipx_slot_take(w[k], stamp, m)) ipx_fold(has, acc, true, m);
             }
@@ -2076,8 +2105,8 @@ __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
         if (threadIdx.x == 0) {
             has = false;
             for (int w = 0; w < (int)(nthr >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
-            cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1);
         }
+        cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1, s_has, s_acc);
     }
     /* a copy given up on may still be in flight: wait for it (bounded)
      * before the CTA's shared memory is released */
@@ -2232,8 +2261,8 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             if (threadIdx.x == 0) {
                 has = false;
                 for (int w = 0; w < (int)(blockDim.x >> 5); w++) ipx_fold(has, acc, s_has[w], s_acc[w]);
-                cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1);
             }
+            cnt += ipx_hub_chunk_done(h, has, acc, out, stamp + 1, s_has, s_acc);
             __syncthreads();
         }
     }
