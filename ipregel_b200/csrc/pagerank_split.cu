@@ -42,6 +42,9 @@ extern "C" int ipg_internal_fail(int code, const char* msg);
 #define PR_THREADS 256
 #define PR_UNROLL 4
 #define PR_CHUNK 4096
+#ifndef PR_GROUP
+#define PR_GROUP 16 /* lanes per vertex of the middle degree class */
+#endif
 #define PR_CTAS_PER_SM 8 /* upper bound; the resident count decides */
 
 #define PR_CUDA(call)                                                      \
@@ -198,7 +201,7 @@ template <bool COMP>
 __device__ __forceinline__ void pr_gather(const PrStep& a, uint64_t e0, uint64_t e1, uint64_t lane, uint64_t lanes,
                                           float& s, float& c)
 {
-    if (lanes >= 32 && (reinterpret_cast<uintptr_t>(a.in_adj) & 15) == 0) {
+    if (lanes >= 8 && (reinterpret_cast<uintptr_t>(a.in_adj) & 15) == 0) {
         pr_gather_v4<COMP>(a, e0, e1, lane, lanes, s, c);
         return;
     }
@@ -279,19 +282,28 @@ __global__ void __launch_bounds__(PR_THREADS) k_pr_thread(PrStep a, const uint32
     }
 }
 
-// Class 1: a warp per vertex.
+// Class 1: PR_GROUP lanes per vertex (most vertices of the class have a few
+// dozen in-edges, which 16 lanes reading four ids each cover in a step or
+// two; a whole warp per vertex left most lanes idle).
 template <bool COMP, bool LAST>
 __global__ void __launch_bounds__(PR_THREADS) k_pr_warp(PrStep a, const uint32_t* __restrict__ list, uint64_t n)
 {
-    const int lane = threadIdx.x & 31;
-    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    constexpr int G = PR_GROUP;
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+    const unsigned mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    const uint64_t groups = ((uint64_t)gridDim.x * blockDim.x) / G;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) / G; i < n; i += groups) {
         const uint64_t v = list[i];
         const uint64_t e0 = a.in_row[v], e1 = a.in_row[v + 1];
         float s = 0.0f, c = 0.0f;
-        pr_gather<COMP>(a, e0, e1, lane, 32, s, c);
-        pr_warp_merge<COMP>(s, c);
-        if (lane == 0) pr_finish<LAST>(a, v, pr_deg(a, v, e0, e1), __fadd_rn(s, c));
+        pr_gather<COMP>(a, e0, e1, gl, G, s, c);
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+            const float s2 = __shfl_down_sync(mask, s, o, G);
+            const float c2 = __shfl_down_sync(mask, c, o, G);
+            pr_merge<COMP>(s, c, s2, c2);
+        }
+        if (gl == 0) pr_finish<LAST>(a, v, pr_deg(a, v, e0, e1), __fadd_rn(s, c));
     }
 }
 
