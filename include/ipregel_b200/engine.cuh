@@ -1148,36 +1148,6 @@ __device__ inline void ip_vote_to_halt(struct ip_vertex_t* v)
 
 /* Fills the neighbour fields of the proxy (loads the compiler drops when
  * ip_compute does not read them). */
-/* The same with the out-row bounds (o0, o1) and in-row bounds (q0, q1)
- * already in registers. */
-__device__ __forceinline__ void ipx_fill_topology_known(struct ip_vertex_t& x, uint64_t o0, uint64_t o1, uint64_t q0,
-                                                        uint64_t q1)
-{
-    (void)x;
-    (void)o0;
-    (void)o1;
-    (void)q0;
-    (void)q1;
-#ifdef IP_NEEDS_OUT_NEIGHBOUR_IDS
-    x.out_neighbours = const_cast<ipx_vid*>(ipx_c.adj + o0);
-#endif
-#ifdef IP_NEEDS_OUT_NEIGHBOUR_COUNT
-    x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(o1 - o0);
-#endif
-#if IPX_OUT_WEIGHTS
-    x.out_neighbour_weights = const_cast<ipx_wgt*>(ipx_c.wgt + o0);
-#endif
-#ifdef IP_NEEDS_IN_NEIGHBOUR_IDS
-    x.in_neighbours = const_cast<ipx_vid*>(ipx_c.in_adj + q0);
-#endif
-#ifdef IP_NEEDS_IN_NEIGHBOUR_COUNT
-    x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(q1 - q0);
-#endif
-#if IPX_IN_WEIGHTS
-    x.in_neighbour_weights = const_cast<ipx_wgt*>(ipx_c.in_wgt + q0);
-#endif
-}
-
 __device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_t v)
 {
 #if defined(IP_NEEDS_OUT_NEIGHBOUR_IDS) || defined(IP_NEEDS_OUT_NEIGHBOUR_COUNT) || IPX_OUT_WEIGHTS
@@ -1803,55 +1773,6 @@ __device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const 
     return true;
 }
 
-/* The vertex data its compute phase reads, loaded before its gather so that
- * their latency overlaps the gather's (the vertex's in-row bounds q0, q1
- * are known; with the rows as in-lists they are its out-row bounds too). */
-struct ipx_sb_pre {
-    uint64_t o0, o1;
-    ipx_val v0;
-    bool a0;
-};
-
-__device__ __forceinline__ ipx_sb_pre ipx_sb_preload(uint64_t v, uint64_t q0, uint64_t q1)
-{
-    ipx_sb_pre p;
-    p.a0 = ipx_c.active_b[v] != 0;
-    p.v0 = ipx_c.value[v];
-    p.o0 = q0;
-    p.o1 = q1;
-#if defined(IP_NEEDS_OUT_NEIGHBOUR_IDS) || defined(IP_NEEDS_OUT_NEIGHBOUR_COUNT) || IPX_OUT_WEIGHTS
-    if (ipx_c.in_row != ipx_c.row) {
-        p.o0 = ipx_c.row[v];
-        p.o1 = ipx_c.row[v + 1];
-    }
-#endif
-    return p;
-}
-
-/* ipx_sb_compute_next with the preloaded data. */
-__device__ __forceinline__ bool ipx_sb_compute_next_pre(uint64_t v, bool has, const ipx_msg& acc, ipx_sbslot* out,
-                                                        uint32_t next_stamp, const ipx_sb_pre& p, uint64_t q0,
-                                                        uint64_t q1)
-{
-    if (!p.a0 && !has) {
-        ipx_sb_put(&out[v], false, acc, next_stamp);
-        return false;
-    }
-    struct ip_vertex_t x;
-    x.id = (ipx_vid)v;
-    x.active = true;
-    x.has_message = has;
-    if (has) x.message = acc;
-    x.value = p.v0;
-    x.ipx_has_out = false;
-    ipx_fill_topology_known(x, p.o0, p.o1, q0, q1);
-    ip_compute(&x);
-    if (!ipx_same_bits(x.value, p.v0)) ipx_c.value[v] = x.value;
-    if (x.active != p.a0) ipx_c.active_b[v] = x.active ? 1 : 0;
-    ipx_sb_put(&out[v], x.ipx_has_out, x.ipx_out, next_stamp);
-    return true;
-}
-
 /* ---- bulk copies into shared memory (cp.async.bulk, completed on an
  * mbarrier; one CTA, no cluster, no multicast) ---- */
 __device__ __forceinline__ uint32_t ipx_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -2081,11 +2002,6 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
 #ifndef IPX_HUB_SMEM
 #define IPX_HUB_SMEM 1
 #endif
-/* 1: the fused pull kernel loads a vertex's activity, value and out-row
- * bounds before its gather (the latency overlaps the gather's). */
-#ifndef IPX_SB_PRELOAD
-#define IPX_SB_PRELOAD 1
-#endif
 /* In-edges a thread of the staged hub gather loads per step. */
 #ifndef IPX_HUB_UNROLL
 #define IPX_HUB_UNROLL 4
@@ -2256,15 +2172,8 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             const uint64_t vn = (i + stride < n) ? list[i + stride] : 0;
             bool has = false;
             ipx_msg acc;
-#if IPX_SB_PRELOAD
-            const uint64_t q0 = row[v], q1 = row[v + 1];
-            const ipx_sb_pre pre = ipx_sb_preload(v, q0, q1);
-            ipx_gather_fold_edges<HOT>(adj, bs, stamp, q0, q1, 0, 1, has, acc);
-            cnt += ipx_sb_compute_next_pre(v, has, acc, out, stamp + 1, pre, q0, q1);
-#else
             ipx_gather_fold_edges<HOT>(adj, bs, stamp, row[v], row[v + 1], 0, 1, has, acc);
             cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
-#endif
             v = vn;
         }
     } else if constexpr (MODE == 1 && IPX_GATHER_EXPAND && !HOT) {
@@ -2277,35 +2186,6 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
         const int lane = threadIdx.x & 31, gl = lane & (G - 1);
         const unsigned mask = (G == 32) ? IPX_FULL : (((1u << G) - 1u) << (lane & ~(G - 1)));
         const uint64_t groups = ipx_gstride() / G;
-#if IPX_SB_PRELOAD
-        /* the next vertex's list entry and in-row bounds are loaded during
-         * this vertex's gather, and the data of this vertex's compute phase
-         * before it */
-        uint64_t i = ipx_gtid() / G, v = 0, q0 = 0, q1 = 0;
-        if (i < n) {
-            v = list[i];
-            q0 = row[v];
-            q1 = row[v + 1];
-        }
-        for (; i < n; i += groups) {
-            uint64_t vn = 0, q0n = 0, q1n = 0;
-            if (i + groups < n) {
-                vn = list[i + groups];
-                q0n = row[vn];
-                q1n = row[vn + 1];
-            }
-            ipx_sb_pre pre;
-            if (gl == 0) pre = ipx_sb_preload(v, q0, q1);
-            bool has = false;
-            ipx_msg acc;
-            ipx_gather_fold_edges<HOT>(adj, bs, stamp, q0, q1, gl, G, has, acc);
-            ipx_group_fold<G>(has, acc, mask);
-            if (gl == 0) cnt += ipx_sb_compute_next_pre(v, has, acc, out, stamp + 1, pre, q0, q1);
-            v = vn;
-            q0 = q0n;
-            q1 = q1n;
-        }
-#else
         for (uint64_t i = ipx_gtid() / G; i < n; i += groups) {
             const uint64_t v = list[i];
             bool has = false;
@@ -2314,7 +2194,6 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
             ipx_group_fold<G>(has, acc, mask);
             if (gl == 0) cnt += ipx_sb_compute_next(v, has, acc, out, stamp + 1);
         }
-#endif
     } else if constexpr (MODE == 1) {
         /* the next vertex's list entry and row bounds are loaded while this
          * vertex's in-edges are folded */
