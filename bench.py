@@ -465,10 +465,10 @@ def serving_row():
         runs.append((S.summarize(lat, mk, tr.kind), clk))
     runs.sort(key=lambda r: r[0]["qps"])
     summ, clk = runs[1]
-    # below capacity: arrivals at about half the served rate, so that the
+    # below capacity: arrivals at about an eighth of the served rate, so that the
     # percentiles are service latencies rather than queueing
-    low_rate = 150.0
-    tr_low = S.poisson_trace(600, low_rate, sizes, seed=2)
+    low_rate = 40.0
+    tr_low = S.poisson_trace(200, low_rate, sizes, seed=2)
     _, lat_low, mk_low = srv.run_trace(tr_low)
     low = S.summarize(lat_low, mk_low, tr_low.kind)
     st = srv.stats()
@@ -525,8 +525,8 @@ def serving_row():
             "kernel_launches": st["kernel_launches"], "pull_supersteps": st["pull_supersteps"],
             "peak_hbm_bytes": st["peak_bytes"], "hbm_free_before_trace": free_b, "clocks_during_trace": clk,
             "note": "arrivals exceed capacity: latency includes queueing",
-            "unsaturated": {"workload": f"600 queries of the same mix, Poisson {low_rate:.0f}/s (below the served "
-                                        f"rate), seed 2", "served_qps": round(low["qps"], 1),
+            "unsaturated": {"workload": f"200 queries of the same mix, Poisson {low_rate:.0f}/s (an eighth of the "
+                                        f"served rate), seed 2", "served_qps": round(low["qps"], 1),
                             "p50_ms": round(low["p50_ms"], 2), "p99_ms": round(low["p99_ms"], 2),
                             "per_kind_ms": {k: round(v, 2) for k, v in low.items()
                                             if k.endswith("_ms") and "_" in k[:-3]}}}
@@ -702,6 +702,8 @@ def write_traffic(csv_path, line_path, out_path=TRAFFIC_PATH):
         compacts = 0
         for x in order[b:end]:
             nm = x["name"]
+            if nm.startswith("void "):  # templated kernels carry their return type
+                nm = nm[5:]
             key = None
             for pref, short in NCU_KERNEL_NAMES:
                 if nm.startswith(pref):
@@ -815,6 +817,7 @@ def main():
             prof[f"{tag}:{k}"] = v
     for eng in (cc, sp):
         eng.set_profile(False)
+        eng.set_graph_loop(True)  # every later run (same-work row, e2e) is one captured launch again
 
     # dominant kernel and its roofline
     peak, peak_kind = measured_peaks()
