@@ -786,6 +786,10 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_PUSH_EXPAND
 #define IPX_PUSH_EXPAND 0
 #endif
+/* Lanes per source in the warp class of push and mark (8, 16 or 32). */
+#ifndef IPX_PUSH_GROUP
+#define IPX_PUSH_GROUP 32
+#endif
 /* Lanes per source in the thread class of push and mark (1, 2, 4 or 8). */
 #ifndef IPX_PUSH_Q
 #define IPX_PUSH_Q 1
@@ -940,7 +944,7 @@ __device__ __forceinline__ void ipx_edges_strided(const ipx_vid* __restrict__ ad
                                                   uint64_t lane, uint64_t lanes, ipx_msg m, const Visit& visit)
 {
     if constexpr (sizeof(ipx_vid) == 4) {
-        if (lanes >= 32 && ipx_v4_ok(adj)) {
+        if (lanes >= 8 && ipx_v4_ok(adj)) {
             ipx_edges_v4(reinterpret_cast<const uint32_t*>(adj), e0, e1, lane, lanes, m, visit);
             return;
         }
@@ -1240,14 +1244,17 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
             m = mn;
         }
     } else if constexpr (MODE == 1) {
+        /* IPX_PUSH_GROUP lanes per source (a warp's worth, or fewer: most
+         * sources of the class have a few dozen out-edges) */
+        constexpr int G = IPX_PUSH_GROUP;
         const ipx_vid* __restrict__ adj = ipx_c.adj;
         const uint64_t* __restrict__ row = ipx_c.row;
-        const uint64_t lane = threadIdx.x & 31;
-        for (uint64_t i = ipx_gtid() >> 5; i < n; i += ipx_gstride() >> 5) {
+        const uint64_t lane = threadIdx.x & (G - 1);
+        for (uint64_t i = ipx_gtid() / G; i < n; i += ipx_gstride() / G) {
             const uint64_t u = list[i];
             ipx_msg m = ipx_msg();
             if constexpr (Visit::kNeedsMessage) m = ipx_c.outbox[u];
-            ipx_edges_strided(adj, row[u], row[u + 1], lane, 32, m, visit);
+            ipx_edges_strided(adj, row[u], row[u + 1], lane, G, m, visit);
         }
     } else {
         if (n == 0) return;
