@@ -2031,6 +2031,57 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
  * global memory.  A wait that gives up (never expected) sets
  * IPX_ERR_COPY_TIMEOUT, and the CTA reads ids from global memory for the
  * rest of the launch; results stay exact. */
+/* 1: the hub class of the fused pull kernel takes a warp per chunk instead
+ * of a CTA (no CTA-wide barriers per chunk). */
+#ifndef IPX_HUB_WARP
+#define IPX_HUB_WARP 0
+#endif
+
+/* The hub class with a warp per chunk: the warp folds its chunk, lane 0
+ * stores the fold, and the warp whose chunk arrives last folds the hub's
+ * partials -- each lane a contiguous run of them, then the runs in order by
+ * shuffles -- and lane 0 runs the vertex's compute phase. */
+template <bool HOT>
+__device__ __forceinline__ unsigned long long ipx_gather_hubs_warp(
+    const ipx_vid* __restrict__ adj, const uint64_t* __restrict__ row, const uint32_t* __restrict__ list, uint64_t n,
+    const uint32_t* __restrict__ prefix, uint32_t chunks, const ipx_sbslot* __restrict__ bs, uint32_t stamp,
+    ipx_sbslot* __restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ipx_gstride() >> 5;
+    unsigned long long cnt = 0;
+    for (uint64_t c = ipx_gtid() >> 5; c < chunks; c += nwarps) {
+        ipx_hub_chunk h;
+        ipx_locate_chunk(list, n, prefix, row, (uint32_t)c, h);
+        bool has = false;
+        ipx_msg acc;
+        ipx_gather_fold_edges<HOT>(adj, bs, stamp, h.e0, h.e1, lane, 32, has, acc);
+        ipx_warp_fold(has, acc);
+        int last = 2; /* a hub of one chunk: its fold is the hub's */
+        if (lane == 0 && h.nch != 1) {
+            ipx_bslot_put(&ipx_c.hub_part[h.c], acc, has ? 1u : 0u);
+            __threadfence();
+            last = atomicAdd(&ipx_c.hub_arrived[h.i], 1u) == h.nch - 1 ? 1 : 0;
+        }
+        last = __shfl_sync(IPX_FULL, last, 0);
+        if (last == 1) {
+            __threadfence();
+            const uint32_t per = (h.nch + 31) / 32;
+            const uint32_t k0 = (uint32_t)lane * per, k1 = min(k0 + per, h.nch);
+            has = false;
+            for (uint32_t k = k0; k < k1; k++) {
+                const ipx_bslot p = __ldcg(&ipx_c.hub_part[h.c0 + k]);
+                ipx_msg m;
+                if (ipx_bslot_take(p, 1u, m)) ipx_fold(has, acc, true, m);
+            }
+            ipx_warp_fold(has, acc);
+            if (lane == 0) ipx_c.hub_arrived[h.i] = 0; /* every chunk of the hub has arrived */
+        }
+        if (lane == 0 && last != 0) cnt += ipx_sb_compute_next(h.v, has, acc, out, stamp + 1);
+    }
+    return cnt;
+}
+
 template <bool HOT>
 __device__ __forceinline__ unsigned long long ipx_gather_hubs_staged(
     const uint32_t* __restrict__ adj, const uint64_t* __restrict__ row, const uint32_t* __restrict__ list, uint64_t n,
@@ -2240,6 +2291,11 @@ __global__ void __launch_bounds__(IPX_THREADS, (MODE == 1 && IPX_GATHER_EXPAND) 
          * instead of behind a global id load each. */
         if (n == 0) return;
         const uint32_t chunks = prefix[n];
+        if constexpr (IPX_HUB_WARP) {
+            cnt += ipx_gather_hubs_warp<HOT>(adj, row, list, n, prefix, chunks, bs, stamp, out);
+            ipx_block_count(cnt, &ipx_c.ctr[s & 3]);
+            return;
+        }
         if constexpr (sizeof(ipx_vid) == 4 && IPX_HUB_SMEM) {
             if ((reinterpret_cast<uintptr_t>(adj) & 15) == 0) {
                 cnt += ipx_gather_hubs_staged<HOT>(reinterpret_cast<const uint32_t*>(adj), row, list, n, prefix, chunks,
