@@ -774,9 +774,24 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_HUB_CHUNK
 #define IPX_HUB_CHUNK 2048
 #endif
-/* In-edges per chunk of the single_broadcast gather's hub class. */
+/* 1: the hub class of the fused pull kernel takes a warp per chunk instead
+ * of a CTA (no CTA-wide barriers per chunk); 0: a CTA per chunk, its ids
+ * staged in shared memory (IPX_HUB_SMEM).  On directed R-MAT scale 25
+ * (FP64 PageRank, 30 rounds) a warp per 4,096-edge chunk took 109 ms, a CTA
+ * per 2,048-edge chunk, staged or not, 118.7 ms: the CTA version waits at
+ * two barriers per chunk. */
+#ifndef IPX_HUB_WARP
+#define IPX_HUB_WARP 1
+#endif
+/* In-edges per chunk of the single_broadcast gather's hub class (a warp's
+ * with IPX_HUB_WARP; 2,048 for a CTA's: the staging buffers of larger
+ * chunks do not fit the 48 KB of static shared memory). */
 #ifndef IPX_GATHER_CHUNK
+#if IPX_HUB_WARP
+#define IPX_GATHER_CHUNK 4096
+#else
 #define IPX_GATHER_CHUNK 2048
+#endif
 #endif
 #ifndef IPX_UNROLL
 #define IPX_UNROLL 4
@@ -2031,11 +2046,6 @@ __device__ __forceinline__ unsigned long long ipx_gather_expand(const uint32_t* 
  * global memory.  A wait that gives up (never expected) sets
  * IPX_ERR_COPY_TIMEOUT, and the CTA reads ids from global memory for the
  * rest of the launch; results stay exact. */
-/* 1: the hub class of the fused pull kernel takes a warp per chunk instead
- * of a CTA (no CTA-wide barriers per chunk). */
-#ifndef IPX_HUB_WARP
-#define IPX_HUB_WARP 0
-#endif
 
 /* The hub class with a warp per chunk: the warp folds its chunk, lane 0
  * stores the fold, and the warp whose chunk arrives last folds the hub's

@@ -418,8 +418,11 @@ class RunResult:
     supersteps: int = 0
 
 
-def app_library(app: str, version: str, id_bits: int = 32, generic: bool = False) -> str:
-    prefix = "appgeneric" if generic else "app"
+def app_library(app: str, version: str, id_bits: int = 32, generic: bool = False, variant: str = "") -> str:
+    """Path of an application library; `variant` names a build of other
+    kernel switches ("staged": the pull gather's hub chunks a CTA each, ids
+    staged in shared memory)."""
+    prefix = "appgeneric" if generic else f"app{variant}"
     return os.path.join(LIB_DIR, f"{prefix}_{app}_{version}_{id_bits}.so")
 
 
@@ -432,10 +435,11 @@ class Engine:
     # attach must not run after another (its kernels hold the old state)
     _generation = {}
 
-    def __init__(self, app: str, version: str = "combiner", id_bits: int = 32, generic: bool = False):
+    def __init__(self, app: str, version: str = "combiner", id_bits: int = 32, generic: bool = False,
+                 variant: str = ""):
         if version not in VERSIONS:
             raise ValueError(f"unknown version {version!r}; expected one of {VERSIONS}")
-        path = app_library(app, version, id_bits, generic)
+        path = app_library(app, version, id_bits, generic, variant)
         if not os.path.exists(path):
             raise IPregelError(f"{path} is missing: build it with `make -C {HERE}`")
         runtime()

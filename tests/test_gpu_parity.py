@@ -240,3 +240,35 @@ def test_single_broadcast_degree_classes(app, t0, t1, hot_kb, monkeypatch):
         finally:
             eng.release()
             graph.free()
+
+
+@pytest.mark.parametrize("app", ["pagerank", "cc"])
+def test_single_broadcast_staged_hub_chunks(app):
+    """The build whose pull gather takes a CTA per hub chunk with the chunk's
+    ids staged in shared memory by bulk copies (appstaged_*): the same
+    results as the oracle, with many chunks per hub (t1 = 64) and one."""
+    import ipregel_b200 as ip
+    hub = [(0, i) for i in range(1, 9000)] + [(i, 0) for i in range(1, 9000)] + \
+          [(i, i + 1) for i in range(1, 8999)] + [(i + 1, i) for i in range(1, 8999)]
+    for g in (O.gen_rmat(12, 16, seed=31, undirected=False), O.from_edges(9000, hub)):
+        graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+        eng = ip.Engine(app, "single_broadcast", variant="staged")
+        try:
+            eng.set_quiet(True)
+            if app == "pagerank":
+                eng.set_param("rounds", 10)
+            want, counts, _ = O.run(g, app, "single_broadcast")
+            for t1 in (64, 4096):
+                eng.set_tuning(t0=16, t1=t1)
+                for loop in (False, True):
+                    eng.set_graph_loop(loop)
+                    eng.attach(graph)
+                    res = eng.run()
+                    if app == "pagerank":
+                        assert np.max(np.abs(res.values - want)) <= PR_TOL
+                    else:
+                        np.testing.assert_array_equal(res.values, want)
+                    assert res.counts == [int(c) for c in counts]
+        finally:
+            eng.release()
+            graph.free()
