@@ -777,9 +777,9 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 /* 1: the hub class of the fused pull kernel takes a warp per chunk instead
  * of a CTA (no CTA-wide barriers per chunk); 0: a CTA per chunk, its ids
  * staged in shared memory (IPX_HUB_SMEM).  On directed R-MAT scale 25
- * (FP64 PageRank, 30 rounds) a warp per 4,096-edge chunk took 109 ms, a CTA
- * per 2,048-edge chunk, staged or not, 118.7 ms: the CTA version waits at
- * two barriers per chunk. */
+ * (FP64 PageRank, 30 rounds) a warp per 4,096-edge chunk took 109 ms (8,192:
+ * 105.9 ms), a CTA per 2,048-edge chunk, staged or not, 118.7 ms: the CTA
+ * version waits at two barriers per chunk. */
 #ifndef IPX_HUB_WARP
 #define IPX_HUB_WARP 1
 #endif
@@ -788,7 +788,7 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
  * chunks do not fit the 48 KB of static shared memory). */
 #ifndef IPX_GATHER_CHUNK
 #if IPX_HUB_WARP
-#define IPX_GATHER_CHUNK 4096
+#define IPX_GATHER_CHUNK 8192
 #else
 #define IPX_GATHER_CHUNK 2048
 #endif
