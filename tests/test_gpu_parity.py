@@ -272,3 +272,35 @@ def test_single_broadcast_staged_hub_chunks(app):
         finally:
             eng.release()
             graph.free()
+
+
+def test_reserved_fp64_pattern_is_refused():
+    """The single_broadcast engine's 8-byte FP64 slots keep the all-ones bit
+    pattern for "no broadcast": a program that broadcasts exactly that
+    pattern gets an error (host and captured loops), a program that does not
+    gets its results, and the engine stays usable after the error."""
+    import ipregel_b200 as ip
+    g = O.gen_rmat(9, 8, seed=3, undirected=True)
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj)
+    eng = ip.Engine("reserved", "single_broadcast")
+    try:
+        eng.set_quiet(True)
+        src = int(np.argmax(np.diff(g.row_ptr())))  # a vertex with edges
+        eng.set_param("source", src)
+        row = g.row_ptr().astype(np.int64)
+        want = np.array([float(np.count_nonzero(g.adj[row[v]:row[v + 1]] == src)) for v in range(g.V)])
+        for loop in (False, True):
+            eng.set_graph_loop(loop)
+            eng.attach(graph)
+            eng.set_param("allones", 0)
+            res = eng.run()
+            np.testing.assert_array_equal(res.values, want)
+            eng.set_param("allones", 1)
+            with pytest.raises(ip.IPregelError, match="all 64 bits set"):
+                eng.run()
+            eng.set_param("allones", 0)
+            np.testing.assert_array_equal(eng.run().values, want)
+    finally:
+        eng.set_graph_loop(False)
+        eng.release()
+        graph.free()
