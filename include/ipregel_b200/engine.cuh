@@ -645,6 +645,9 @@ struct ipx_consts {
     const uint32_t* hub_owner;
     /* the in-lists with the flag of the most gathered vertices (null: none) */
     const uint32_t* in_adj_hot;
+    /* push / mark: chunk -> index of its hub in this superstep's hub list
+     * (null: found by a binary search over the prefix) */
+    const uint32_t* push_owner;
 };
 
 __constant__ ipx_consts ipx_c;
@@ -1038,11 +1041,14 @@ __device__ __forceinline__ void ipx_warp_expand(const uint32_t* __restrict__ lis
 }
 
 /* Chunk prefix of the high-degree class: prefix[i] = chunks of the hubs before
- * i, prefix[n] = total (one block, a carried scan over tiles of its width). */
+ * i, prefix[n] = total (one block, a carried scan over tiles of its width).
+ * With owner, also owner[c] = i for every chunk c of hub i, so that a chunk
+ * finds its hub with one load instead of a binary search over the prefix. */
 template <uint32_t CHUNK = IPX_HUB_CHUNK>
 __global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restrict__ list,
                                                          const uint32_t* __restrict__ count,
-                                                         const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix)
+                                                         const uint64_t* __restrict__ row, uint32_t* __restrict__ prefix,
+                                                         uint32_t* __restrict__ owner = nullptr)
 {
     __shared__ uint32_t s[1024];
     const uint64_t n = *count;
@@ -1062,20 +1068,16 @@ __global__ void __launch_bounds__(1024) ipx_k_hub_prefix(const uint32_t* __restr
             s[threadIdx.x] += x;
             __syncthreads();
         }
-        if (i < n) prefix[i] = carry + s[threadIdx.x] - c;
+        if (i < n) {
+            const uint32_t p = carry + s[threadIdx.x] - c;
+            prefix[i] = p;
+            if (owner)
+                for (uint32_t k = 0; k < c; k++) owner[p + k] = (uint32_t)i;
+        }
         carry += s[1023];
         __syncthreads();
     }
     if (threadIdx.x == 0) prefix[n] = carry;
-}
-
-/* owner[c] = i for every chunk c of hub i (prefix as ipx_k_hub_prefix
- * made it): a chunk finds its hub with one load instead of a binary search
- * of ~log2(n) dependent loads. */
-__global__ void ipx_k_chunk_owner(const uint32_t* __restrict__ prefix, uint64_t n, uint32_t* __restrict__ owner)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        for (uint32_t c = prefix[i]; c < prefix[i + 1]; c++) owner[c] = (uint32_t)i;
 }
 
 /* ---- the flagged in-lists of the single_broadcast gather (attach time) ---- */
@@ -1277,7 +1279,7 @@ __device__ __forceinline__ void ipx_over_sources(const uint32_t* __restrict__ li
         const uint64_t* __restrict__ row = ipx_c.row;
         const uint32_t chunks = prefix[n];
         for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-            const uint64_t i = ipx_hub_of_chunk(prefix, n, c);
+            const uint64_t i = ipx_c.push_owner ? ipx_c.push_owner[c] : ipx_hub_of_chunk(prefix, n, c);
             const uint64_t u = list[i];
             const uint64_t e0 = row[u] + (uint64_t)(c - prefix[i]) * IPX_HUB_CHUNK;
             const uint64_t end = row[u + 1];
@@ -1600,7 +1602,7 @@ __global__ void __launch_bounds__(IPX_THREADS, IPX_EDGE_CTAS) ipx_k_pull_deliver
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const uint32_t chunks = prefix[n];
         for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-            const uint64_t i = ipx_hub_of_chunk(prefix, n, c);
+            const uint64_t i = ipx_c.hub_owner ? ipx_c.hub_owner[c] : ipx_hub_of_chunk(prefix, n, c);
             const uint64_t v = list[i];
             const uint64_t e0 = row[v] + (uint64_t)(c - prefix[i]) * IPX_HUB_CHUNK;
             const uint64_t e1 = (e0 + IPX_HUB_CHUNK < row[v + 1]) ? e0 + IPX_HUB_CHUNK : row[v + 1];

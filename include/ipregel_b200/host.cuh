@@ -350,6 +350,15 @@ static int ipx_setup_state()
     c.lcnt = ipx_h.lcnt;
     IPX_OK(ipx_alloc(&c.hist, (uint64_t)IPX_HIST * 4));
     IPX_OK(ipx_alloc(&ipx_h.hub_prefix, gv.E / (ipx_h.tune.t1 + 1) + 2));
+#if !IPX_PULL || IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
+    {
+        /* the chunks of this superstep's broadcaster hubs: at most E / chunk
+         * + one partial chunk per hub */
+        uint32_t* owner = nullptr;
+        IPX_OK(ipx_alloc(&owner, gv.E / IPX_HUB_CHUNK + gv.E / (ipx_h.tune.t1 + 1) + 2));
+        c.push_owner = owner;
+    }
+#endif
 #if IPX_VERSION == IPX_COMBINER
     IPX_OK(ipx_alloc(&c.active_bm, W + 1));
     IPX_OK(ipx_alloc(&c.hasmsg_bm, W + 1));
@@ -393,9 +402,12 @@ static int ipx_setup_state()
         IPX_OK(ipx_alloc(&dcount, 1));
         const uint32_t n2 = (uint32_t)ipx_h.gbins.count[2];
         IPX_CU(cudaMemcpy(dcount, &n2, 4, cudaMemcpyHostToDevice));
-        ipx_k_hub_prefix<><<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
+        uint32_t* owner = nullptr;
+        IPX_OK(ipx_alloc(&owner, ipx_h.gbins.edges[2] / IPX_HUB_CHUNK + n2 + 1));
+        ipx_k_hub_prefix<><<<1, 1024>>>(ipx_h.gbins.d_list[2], dcount, c.in_row, ipx_h.pull_prefix, owner);
         IPX_CU(cudaGetLastError());
         IPX_CU(cudaDeviceSynchronize());
+        c.hub_owner = owner;
     }
 #endif
 #if IPX_VERSION == IPX_SPREAD_SINGLE_BROADCAST
@@ -421,13 +433,9 @@ static int ipx_setup_state()
         IPX_OK(ipx_alloc(&dcount, 1));
         const uint32_t n2u = (uint32_t)n2;
         IPX_CU(cudaMemcpy(dcount, &n2u, 4, cudaMemcpyHostToDevice));
-        ipx_k_hub_prefix<IPX_GATHER_CHUNK><<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix);
-        IPX_CU(cudaGetLastError());
-        uint32_t total = 0;
-        IPX_CU(cudaMemcpy(&total, ipx_h.pull_prefix + n2, 4, cudaMemcpyDeviceToHost));
         uint32_t* owner = nullptr;
-        IPX_OK(ipx_alloc(&owner, (uint64_t)total + 1));
-        if (n2) ipx_k_chunk_owner<<<ipx_grid(4), 256>>>(ipx_h.pull_prefix, n2, owner);
+        IPX_OK(ipx_alloc(&owner, max_chunks));
+        ipx_k_hub_prefix<IPX_GATHER_CHUNK><<<1, 1024>>>(b.d_list[2], dcount, c.in_row, ipx_h.pull_prefix, owner);
         IPX_CU(cudaGetLastError());
         IPX_CU(cudaDeviceSynchronize());
         c.hub_owner = owner;
@@ -566,7 +574,8 @@ static int ipx_push_class(int k, uint32_t g)
     if (k == 0) IPX_LAUNCH(IPX_K_PUSH0, ipx_k_push<0><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, pre));
     if (k == 1) IPX_LAUNCH(IPX_K_PUSH1, ipx_k_push<1><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, pre));
     if (k == 2) {
-        IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre));
+        IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.c.row, pre,
+                                                                       (uint32_t*)ipx_h.c.push_owner));
         IPX_LAUNCH(IPX_K_PUSH2, ipx_k_push<2><<<g, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, pre));
     }
     IPX_CU(cudaGetLastError());
@@ -793,7 +802,8 @@ static int ipx_enqueue_superstep()
                                                    ipx_h.blist[1], ipx_h.blist[2], ipx_h.lcnt, edges_b, 1, st)));
     IPX_LAUNCH(IPX_K_MARK0, ipx_k_mark<0><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[0], ipx_h.lcnt + 0, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_MARK1, ipx_k_mark<1><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[1], ipx_h.lcnt + 1, ipx_h.hub_prefix));
-    IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix));
+    IPX_LAUNCH(IPX_K_CTRL, ipx_k_hub_prefix<><<<1, 1024, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, c.row, ipx_h.hub_prefix,
+                                                                   (uint32_t*)c.push_owner));
     IPX_LAUNCH(IPX_K_MARK2, ipx_k_mark<2><<<ge, ipx_h.tb, 0, st>>>(ipx_h.blist[2], ipx_h.lcnt + 2, ipx_h.hub_prefix));
     IPX_LAUNCH(IPX_K_COMPACT_T, IPX_OK(ipg_compact(c.bt, V, c.in_row, ipx_h.tune.t0, ipx_h.tune.t1, ipx_h.tlist[0], ipx_h.tlist[1],
                                                    ipx_h.tlist[2], ipx_h.lcnt + 4, edges_t, 1, st)));

@@ -66,6 +66,7 @@ struct ipg_pr_plan {
     float* b[2] = {nullptr, nullptr};  // broadcast quotients, by superstep parity
     float* xs = nullptr;               // values of every other superstep
     uint32_t* hub_prefix = nullptr;    // first chunk of each hub, then the total
+    uint32_t* hub_owner = nullptr;     // chunk -> index of its hub
     float2* partial = nullptr;         // (sum, compensation) of every hub chunk
     uint64_t chunks = 0;
     int sms = 148;
@@ -307,23 +308,12 @@ __global__ void __launch_bounds__(PR_THREADS) k_pr_warp(PrStep a, const uint32_t
     }
 }
 
-// Index of the hub owning chunk c: the last i with prefix[i] <= c.
-__device__ __forceinline__ uint64_t pr_hub_of(const uint32_t* __restrict__ prefix, uint64_t n, uint32_t c)
-{
-    uint64_t lo = 0, hi = n;  // prefix[lo] <= c < prefix[hi]
-    while (hi - lo > 1) {
-        const uint64_t mid = (lo + hi) >> 1;
-        if (prefix[mid] <= c) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // Class 2, pass 1: a warp per chunk of PR_CHUNK edges of a hub (no CTA-wide
 // barriers per chunk: 15 - 20 % shorter in the FP64 engine's gather).
 template <bool COMP>
 __global__ void __launch_bounds__(PR_THREADS) k_pr_hub_chunks(PrStep a, const uint32_t* __restrict__ list, uint64_t n,
                                                               const uint32_t* __restrict__ prefix,
+                                                              const uint32_t* __restrict__ owner,
                                                               float2* __restrict__ partial)
 {
     if (n == 0) return;
@@ -331,7 +321,7 @@ __global__ void __launch_bounds__(PR_THREADS) k_pr_hub_chunks(PrStep a, const ui
     const int lane = threadIdx.x & 31;
     const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t ch = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; ch < chunks; ch += warps) {
-        const uint64_t i = pr_hub_of(prefix, n, (uint32_t)ch);
+        const uint64_t i = owner[ch];  // one load, not a binary search over the prefix
         const uint64_t v = list[i];
         const uint64_t end = a.in_row[v + 1];
         const uint64_t e0 = a.in_row[v] + (ch - prefix[i]) * (uint64_t)PR_CHUNK;
@@ -380,7 +370,8 @@ int pr_superstep(ipg_pr_plan* p, const PrStep& a, cudaStream_t st)
     if (b.count[0]) k_pr_thread<COMP, LAST><<<grid, PR_THREADS, 0, st>>>(a, b.d_list[0], b.count[0]);
     if (b.count[1]) k_pr_warp<COMP, LAST><<<grid, PR_THREADS, 0, st>>>(a, b.d_list[1], b.count[1]);
     if (b.count[2]) {
-        k_pr_hub_chunks<COMP><<<grid, PR_THREADS, 0, st>>>(a, b.d_list[2], b.count[2], p->hub_prefix, p->partial);
+        k_pr_hub_chunks<COMP><<<grid, PR_THREADS, 0, st>>>(a, b.d_list[2], b.count[2], p->hub_prefix, p->hub_owner,
+                                                             p->partial);
         const uint32_t g2 = (uint32_t)((b.count[2] * 32 + PR_THREADS - 1) / PR_THREADS);
         k_pr_hub_finish<COMP, LAST><<<g2 < grid ? g2 : grid, PR_THREADS, 0, st>>>(a, b.d_list[2], b.count[2],
                                                                                   p->hub_prefix, p->partial);
@@ -520,6 +511,17 @@ extern "C" int ipg_pr_plan_create(ipg_graph* g, ipg_pr_plan** out)
             break;
         }
         if ((r = pr_alloc(p, &p->partial, total)) != IPG_OK) break;
+        std::vector<uint32_t> owner(total);
+        for (uint64_t i = 0; i < nh; i++)
+            for (uint32_t ch = cnt[i]; ch < cnt[i + 1]; ch++) owner[ch] = (uint32_t)i;
+        if ((r = pr_alloc(p, &p->hub_owner, total + 1)) != IPG_OK) break;
+        if (total) {
+            e = cudaMemcpy(p->hub_owner, owner.data(), total * 4, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                r = ipg_internal_fail(IPG_ECUDA, cudaGetErrorString(e));
+                break;
+            }
+        }
     } while (0);
     if (r != IPG_OK) {
         ipg_pr_plan_free(p);
