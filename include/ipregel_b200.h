@@ -185,6 +185,25 @@ int ipg_graph_check_symmetric(const ipg_graph* g, int* result);
 int ipg_graph_set_directed(ipg_graph* g, int directed);
 /* Builds the in-CSR if it is missing (no-op for undirected graphs). */
 int ipg_graph_build_in(ipg_graph* g);
+/* A renamed copy of g (no reference counterpart: an internal layout of the
+ * engine).  Vertex n of the copy is vertex d_old_of_new[n] of g; the
+ * vertices are numbered by descending count of occurrences in the rows
+ * (ties by ascending id), so the most pushed-to or gathered-from vertices
+ * share cache lines (every s-th edge counted when IPG_ORDER_SAMPLE sets
+ * s; default every edge).  Every row keeps its edge order and weights, its ids
+ * renamed; in-lists (present on g, or built first when need_in is set) are
+ * renamed the same way, and degrees are unchanged.  d_new_of_old is the
+ * inverse map (both 4-byte device arrays of V entries).  Row n of the copy
+ * lists the same edges, in the same order, as row d_old_of_new[n] of g, so
+ * a program reading neighbour ids reads g's row.  The copy and its maps are
+ * cached on g and belong to it: a later call after a refill rebuilds them
+ * in place (same size), ipg_graph_free frees them.  Needs V < 2^31. */
+typedef struct ipg_order {
+    ipg_graph* graph;
+    const uint32_t* d_old_of_new;
+    const uint32_t* d_new_of_old;
+} ipg_order;
+int ipg_graph_degree_order(ipg_graph* g, int need_in, ipg_order* out);
 /* Copies the CSR back to host buffers in the file layout (idx: V x u64). */
 int ipg_graph_to_host(const ipg_graph* g, uint64_t* idx, void* adj, void* wgt);
 /* Writes <path>.config/.idx/.adj(/.wgt) in the reference loader's format. */

@@ -648,9 +648,27 @@ struct ipx_consts {
     /* push / mark: chunk -> index of its hub in this superstep's hub list
      * (null: found by a binary search over the prefix) */
     const uint32_t* push_owner;
+    /* The kernels run on a degree-ordered copy of the graph: vid_of[v] is
+     * the id of vertex v in the caller's numbering, vindex_of its inverse
+     * (both null when the graph is not renamed). */
+    const uint32_t* vid_of;
+    const uint32_t* vindex_of;
+    /* the caller's graph, whose row vid_of[v] holds the same edges in the
+     * same order as row v of the copy: the neighbour ids ip_compute reads
+     * (null when not renamed) */
+    const uint64_t* user_row;
+    const ipx_vid* user_adj;
+    const uint64_t* user_in_row;
+    const ipx_vid* user_in_adj;
 };
 
 __constant__ ipx_consts ipx_c;
+
+/* The id ip_compute sees for vertex v (the caller's numbering). */
+__device__ __forceinline__ ipx_vid ipx_user_id(uint64_t v)
+{
+    return (ipx_vid)(ipx_c.vid_of ? (uint64_t)__ldg(&ipx_c.vid_of[v]) : v);
+}
 
 /* The current superstep, from device memory: the host writes it before each
  * superstep (host loop), or the previous superstep's last kernel advances it
@@ -1154,7 +1172,9 @@ __device__ inline void ip_send_message(IP_VERTEX_ID_TYPE id, IP_MESSAGE_TYPE mes
     (void)message;
     atomicOr(ipx_c.err, IPX_ERR_SEND_IN_BROADCAST);
 #else
-    ipx_deliver((int)(ip_get_superstep() & 1), (uint64_t)id, message);
+    uint64_t w = (uint64_t)id;
+    if (ipx_c.vindex_of && w < ipx_c.V) w = ipx_c.vindex_of[w]; /* the caller's id -> the copy's vertex */
+    ipx_deliver((int)(ip_get_superstep() & 1), w, message);
 #endif
 }
 
@@ -1175,7 +1195,8 @@ __device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_
     const uint64_t r0 = ipx_c.row[v], r1 = ipx_c.row[v + 1];
 #endif
 #ifdef IP_NEEDS_OUT_NEIGHBOUR_IDS
-    x.out_neighbours = const_cast<ipx_vid*>(ipx_c.adj + r0);
+    x.out_neighbours = const_cast<ipx_vid*>(ipx_c.user_adj ? ipx_c.user_adj + ipx_c.user_row[ipx_c.vid_of[v]]
+                                                           : ipx_c.adj + r0);
 #endif
 #ifdef IP_NEEDS_OUT_NEIGHBOUR_COUNT
     x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(r1 - r0);
@@ -1187,7 +1208,8 @@ __device__ __forceinline__ void ipx_fill_topology(struct ip_vertex_t& x, uint64_
     const uint64_t q0 = ipx_c.in_row[v], q1 = ipx_c.in_row[v + 1];
 #endif
 #ifdef IP_NEEDS_IN_NEIGHBOUR_IDS
-    x.in_neighbours = const_cast<ipx_vid*>(ipx_c.in_adj + q0);
+    x.in_neighbours = const_cast<ipx_vid*>(ipx_c.user_in_adj ? ipx_c.user_in_adj + ipx_c.user_in_row[ipx_c.vid_of[v]]
+                                                             : ipx_c.in_adj + q0);
 #endif
 #ifdef IP_NEEDS_IN_NEIGHBOUR_COUNT
     x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(q1 - q0);
@@ -1652,7 +1674,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_combiner()
         const bool r = rw & bit;
         if (v < V && (a || h || r)) {
             struct ip_vertex_t x;
-            x.id = (ipx_vid)v;
+            x.id = ipx_user_id(v);
             x.active = true;
             if (r) {
                 x.has_message = true;
@@ -1703,7 +1725,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_spread(const uint32
         const uint64_t v = vn;
         vn = (i + stride < n) ? (s ? frontier[i + stride] : i + stride) : 0;
         struct ip_vertex_t x;
-        x.id = (ipx_vid)v;
+        x.id = ipx_user_id(v);
         x.active = true;
         x.has_message = s != 0;
         if (s) x.message = ipx_mb::take(&ipx_c.mbox[pprev][v]);
@@ -1755,7 +1777,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_sb0()
             continue;
         }
         struct ip_vertex_t x;
-        x.id = (ipx_vid)v;
+        x.id = ipx_user_id(v);
         x.active = true;
         x.has_message = false;
         const ipx_val v0 = ipx_c.value[v];
@@ -1782,7 +1804,7 @@ __device__ __forceinline__ bool ipx_sb_compute_next(uint64_t v, bool has, const 
         return false;
     }
     struct ip_vertex_t x;
-    x.id = (ipx_vid)v;
+    x.id = ipx_user_id(v);
     x.active = true;
     x.has_message = has;
     if (has) x.message = acc;
@@ -2357,7 +2379,7 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(const uint32_t*
     for (uint64_t i = ipx_gtid(); i < n; i += ipx_gstride()) {
         const uint64_t v = !s ? i : (i < c0 ? l0[i] : (i < c0 + c1 ? l1[i - c0] : l2[i - c0 - c1]));
         struct ip_vertex_t x;
-        x.id = (ipx_vid)v;
+        x.id = ipx_user_id(v);
         x.active = true;
         x.has_message = ipx_c.hasmsg_b[v];
         if (x.has_message) x.message = ipx_c.msg[v];
@@ -2379,7 +2401,15 @@ __global__ void __launch_bounds__(IPX_THREADS) ipx_k_compute_ssb(const uint32_t*
 /* ------------------------------------------------------------------------ */
 __global__ void ipx_k_init_values(uint64_t first, uint64_t last)
 {
-    for (uint64_t v = first + ipx_gtid(); v <= last && v < ipx_c.V; v += ipx_gstride()) {
+    /* [first, last] are ids in the caller's numbering: on a renamed graph
+     * every vertex checks its own id */
+    const bool renamed = ipx_c.vid_of != nullptr;
+    const uint64_t lo = renamed ? 0 : first, hi = renamed ? ~0ULL : last;
+    for (uint64_t v = lo + ipx_gtid(); v <= hi && v < ipx_c.V; v += ipx_gstride()) {
+        if (renamed) {
+            const uint64_t id = ipx_c.vid_of[v];
+            if (id < first || id > last) continue;
+        }
         ipx_c.value[v] = ipx_val();
 #if IPX_VERSION == IPX_SINGLE_BROADCAST
         ipx_c.active_b[v] = 1;
@@ -2389,6 +2419,12 @@ __global__ void ipx_k_init_values(uint64_t first, uint64_t last)
         ipx_c.mbox[1][v] = ipx_mb::empty();
 #endif
     }
+}
+
+/* out[i] = value of the vertex whose id is i in the caller's numbering. */
+__global__ void ipx_k_values_by_id(ipx_val* __restrict__ out)
+{
+    for (uint64_t i = ipx_gtid(); i < ipx_c.V; i += ipx_gstride()) out[i] = ipx_c.value[ipx_c.vindex_of[i]];
 }
 
 __global__ void ipx_k_fill_bits(uint32_t* bm, uint64_t V, uint64_t W)

@@ -54,8 +54,17 @@ static double ipx_wtime()
 
 /* ---- engine host state ---- */
 struct ipx_host_state {
-    ipg_graph* g = nullptr;
+    ipg_graph* g = nullptr;  /* the caller's graph (contents checks, ownership) */
     bool own_graph = false;
+    /* the graph the kernels run on: g, or its degree-ordered copy (owned by
+     * g), with the id maps of the copy (null for g) */
+    ipg_graph* gw = nullptr;
+    const uint32_t* vid_of = nullptr;
+    const uint32_t* vindex_of = nullptr;
+    /* run on the degree-ordered copy (ipg_app_set_order; IPG_ORDER=0 turns
+     * the default off) */
+    bool order = ipx_env_u64("IPG_ORDER", 1) != 0;
+    ipx_val* values_by_id = nullptr; /* the values in the caller's numbering */
     ipg_graph_view gv;
     uint64_t graph_generation = 0; /* the graph's contents generation at attach */
     ipx_consts c;
@@ -197,6 +206,9 @@ static void ipx_release_state(bool keep = false)
     }
     if (ipx_h.g && ipx_h.own_graph) ipg_graph_free(ipx_h.g);
     ipx_h.g = nullptr;
+    ipx_h.gw = nullptr;
+    ipx_h.vid_of = ipx_h.vindex_of = nullptr;
+    ipx_h.values_by_id = nullptr;
     ipx_h.ready = false;
     ipx_h.host_valid = false;
     ipx_h.host_vertices.clear();
@@ -333,6 +345,17 @@ static int ipx_setup_state()
     c.in_row = gv.has_in ? gv.d_in_row : gv.d_row;
     c.in_adj = (const ipx_vid*)(gv.has_in ? gv.d_in_adj : gv.d_adj);
     c.in_wgt = (const ipx_wgt*)(gv.has_in ? gv.d_in_wgt : gv.d_wgt);
+    c.vid_of = ipx_h.vid_of;
+    c.vindex_of = ipx_h.vindex_of;
+    if (ipx_h.vid_of) {
+        /* the caller's rows, for the neighbour ids ip_compute reads */
+        ipg_graph_view u;
+        IPX_OK(ipg_graph_view_get(ipx_h.g, &u));
+        c.user_row = u.d_row;
+        c.user_adj = (const ipx_vid*)u.d_adj;
+        c.user_in_row = u.has_in ? u.d_in_row : u.d_row;
+        c.user_in_adj = (const ipx_vid*)(u.has_in ? u.d_in_adj : u.d_adj);
+    }
     if (IPX_WEIGHT_BYTES && !gv.d_wgt)
         return ipx_fail(IPG_EINVAL, "the application needs edge weights: load the graph with weighted = true");
     if (IPX_WEIGHT_BYTES && gv.weight_bytes != IPX_WEIGHT_BYTES)
@@ -344,6 +367,7 @@ static int ipx_setup_state()
         IPX_CU(cudaHostAlloc((void**)&ipx_h.h_ctr, IPX_NCTR * sizeof(unsigned long long), cudaHostAllocDefault));
     if (!ipx_h.h_lcnt) IPX_CU(cudaHostAlloc((void**)&ipx_h.h_lcnt, 8 * sizeof(uint32_t), cudaHostAllocDefault));
     IPX_OK(ipx_alloc(&c.value, V));
+    if (ipx_h.vindex_of) IPX_OK(ipx_alloc(&ipx_h.values_by_id, V));
     IPX_OK(ipx_alloc(&c.ctr, IPX_NCTR));
     c.err = (uint32_t*)(c.ctr + IPX_CTR_ERR);
     IPX_OK(ipx_alloc(&ipx_h.lcnt, 8));
@@ -396,7 +420,7 @@ static int ipx_setup_state()
         ipx_h.pull_threshold = div ? gv.E / div : ~0ULL;
     }
     if (c.pull_ok) {
-        IPX_OK(ipg_graph_bins(ipx_h.g, gv.directed ? 1 : 0, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
+        IPX_OK(ipg_graph_bins(ipx_h.gw, gv.directed ? 1 : 0, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
         IPX_OK(ipx_alloc(&ipx_h.pull_prefix, ipx_h.gbins.count[2] + 2));
         uint32_t* dcount = nullptr;
         IPX_OK(ipx_alloc(&dcount, 1));
@@ -419,7 +443,7 @@ static int ipx_setup_state()
     IPX_OK(ipx_alloc(&c.sbslot[0], V));
     IPX_OK(ipx_alloc(&c.sbslot[1], V));
     IPX_OK(ipx_alloc(&c.active_b, V + 1));
-    IPX_OK(ipg_graph_bins(ipx_h.g, 1, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
+    IPX_OK(ipg_graph_bins(ipx_h.gw, 1, ipx_h.tune.t0, ipx_h.tune.t1, &ipx_h.gbins));
     {
         /* chunks of the hub class: prefix, partial folds, arrival counters */
         const ipg_bins& b = ipx_h.gbins;
@@ -512,10 +536,22 @@ static int ipx_attach(ipg_graph* g, bool own)
         ;
     /* the push versions pull over the transpose of a directed graph */
     if (!IPX_PULL && ipx_h.tune.pull_div > 0 && ipx_h.gv.directed) need_in = true;
-    if (need_in && !ipx_h.gv.has_in) {
-        IPX_OK(ipg_graph_build_in(g));
-        IPX_OK(ipg_graph_view_get(g, &ipx_h.gv));
+    ipx_h.gw = g;
+    if (ipx_h.order && ipx_h.gv.V < (1ULL << 31)) {
+        /* the kernels run on the degree-ordered copy; a copy that does not
+         * fit the HBM budget leaves the graph's own numbering */
+        ipg_order o;
+        const int r = ipg_graph_degree_order(g, need_in ? 1 : 0, &o);
+        if (r == IPG_OK) {
+            ipx_h.gw = o.graph;
+            ipx_h.vid_of = o.d_old_of_new;
+            ipx_h.vindex_of = o.d_new_of_old;
+        } else if (r != IPG_EBUDGET && r != IPG_ENOMEM) {
+            return ipx_fail(r, ipg_last_error());
+        }
     }
+    if (need_in && ipx_h.gw == g && !ipx_h.gv.has_in) IPX_OK(ipg_graph_build_in(g));
+    IPX_OK(ipg_graph_view_get(ipx_h.gw, &ipx_h.gv));
     ip_set_vertices_count(ipx_h.gv.V);
     ip_set_edges_count(ipx_h.gv.E);
     int r = ipx_setup_state();
@@ -1025,6 +1061,22 @@ void ip_increment_superstep() { ip_superstep++; }
 void ip_set_vertices_count(size_t vertices_count) { ip_vertices_count = vertices_count; }
 void ip_set_edges_count(size_t edges_count) { ip_edges_count = edges_count; }
 
+/* The values in the caller's numbering, on the device: the engine's own
+ * array, or a copy gathered from it when the kernels run renamed. */
+static int ipx_values_by_id(const ipx_val** out)
+{
+    if (!ipx_h.vindex_of || !ipx_h.c.V) {
+        *out = ipx_h.c.value;
+        return IPG_OK;
+    }
+    if (!ipx_h.values_by_id) IPX_OK(ipx_alloc(&ipx_h.values_by_id, ipx_h.c.V));
+    ipx_k_values_by_id<<<ipx_grid(), IPX_THREADS, 0, ipx_h.st>>>(ipx_h.values_by_id);
+    IPX_CU(cudaGetLastError());
+    IPX_CU(cudaStreamSynchronize(ipx_h.st));
+    *out = ipx_h.values_by_id;
+    return IPG_OK;
+}
+
 /* Host copies of the vertices, filled from the device on first use. */
 static int ipx_materialise()
 {
@@ -1032,10 +1084,14 @@ static int ipx_materialise()
     const uint64_t V = ipx_h.c.V;
     std::vector<ipx_val> vals(V);
     std::vector<uint64_t> row(V + 1), in_row(V + 1);
+    std::vector<uint32_t> index_of(ipx_h.vindex_of ? V : 0); /* id -> vertex of the renamed copy */
     if (V) {
-        IPX_CU(cudaMemcpy(vals.data(), ipx_h.c.value, V * sizeof(ipx_val), cudaMemcpyDeviceToHost));
+        const ipx_val* v = nullptr;
+        IPX_OK(ipx_values_by_id(&v));
+        IPX_CU(cudaMemcpy(vals.data(), v, V * sizeof(ipx_val), cudaMemcpyDeviceToHost));
         IPX_CU(cudaMemcpy(row.data(), ipx_h.c.row, (V + 1) * 8, cudaMemcpyDeviceToHost));
         IPX_CU(cudaMemcpy(in_row.data(), ipx_h.c.in_row, (V + 1) * 8, cudaMemcpyDeviceToHost));
+        if (ipx_h.vindex_of) IPX_CU(cudaMemcpy(index_of.data(), ipx_h.vindex_of, V * 4, cudaMemcpyDeviceToHost));
     }
     ipx_h.host_vertices.resize(V);
     for (uint64_t i = 0; i < V; i++) {
@@ -1043,11 +1099,12 @@ static int ipx_materialise()
         memset(&x, 0, sizeof x);
         x.id = (ipx_vid)i;
         x.value = vals[i];
+        [[maybe_unused]] const uint64_t n = ipx_h.vindex_of ? index_of[i] : i;
 #ifdef IP_NEEDS_OUT_NEIGHBOUR_COUNT
-        x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(row[i + 1] - row[i]);
+        x.out_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(row[n + 1] - row[n]);
 #endif
 #ifdef IP_NEEDS_IN_NEIGHBOUR_COUNT
-        x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(in_row[i + 1] - in_row[i]);
+        x.in_neighbour_count = (IP_NEIGHBOUR_COUNT_TYPE)(in_row[n + 1] - in_row[n]);
 #endif
     }
     ip_all_vertices = ipx_h.host_vertices.data();
@@ -1267,14 +1324,19 @@ int ipg_app_values(void* out, uint64_t cap_bytes)
     const uint64_t bytes = ipx_h.c.V * sizeof(ipx_val);
     if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "no graph attached");
     if (cap_bytes < bytes) return ipx_fail(IPG_EINVAL, "output buffer too small");
-    if (bytes) IPX_CU(cudaMemcpy(out, ipx_h.c.value, bytes, cudaMemcpyDeviceToHost));
+    const ipx_val* v = nullptr;
+    IPX_OK(ipx_values_by_id(&v));
+    if (bytes) IPX_CU(cudaMemcpy(out, v, bytes, cudaMemcpyDeviceToHost));
     return IPG_OK;
 }
 
+/* Valid until the next run, attach or release of this library. */
 int ipg_app_values_device(void** ptr)
 {
     if (!ipx_h.ready) return ipx_fail(IPG_EINVAL, "no graph attached");
-    *ptr = ipx_h.c.value;
+    const ipx_val* v = nullptr;
+    IPX_OK(ipx_values_by_id(&v));
+    *ptr = (void*)v;
     return IPG_OK;
 }
 
@@ -1331,6 +1393,21 @@ int ipg_app_set_graph_loop(int on)
 }
 
 int ipg_app_graph_loop(void) { return ipx_h.graph_loop ? 1 : 0; }
+
+/* 1 (the default, unless IPG_ORDER=0): the next attach runs the kernels on
+ * the graph's degree-ordered copy (ipg_graph_degree_order).  ip_compute
+ * still sees the graph's own numbering (its id, its neighbours' ids, the
+ * order of its edges), and so do ip_send_message, the values and ip_dump:
+ * every result is the same.  A copy that does not fit the HBM budget leaves
+ * the graph's own numbering.  ipg_app_order reports whether the attached
+ * graph runs renamed. */
+int ipg_app_set_order(int on)
+{
+    ipx_h.order = on != 0;
+    return IPG_OK;
+}
+
+int ipg_app_order(void) { return (ipx_h.ready && ipx_h.vid_of) ? 1 : 0; }
 
 /* Tuning of the superstep kernels, applied at the next attach: CTA size
  * (a multiple of 32, at most 256), degree-class thresholds t0 <= t1 (thread

@@ -47,7 +47,7 @@ RUNTIME_SYMBOLS = (
     "ipg_fused_free", "ipg_server_create", "ipg_server_free", "ipg_server_add_graph", "ipg_server_submit",
     "ipg_server_poll", "ipg_server_query", "ipg_server_result", "ipg_server_result_device", "ipg_server_release",
     "ipg_server_get_stats", "ipg_server_run_trace", "ipg_server_group_stats",
-    "ipg_server_reserve", "ipg_graph_refill_host", "ipg_graph_contents",
+    "ipg_server_reserve", "ipg_graph_refill_host", "ipg_graph_contents", "ipg_graph_degree_order",
 )
 # The reference interface (src/iPregel_preamble.h:66-317) and the ipg_app_*
 # ABI (include/ipregel_b200/host.cuh), exported by every application library.
@@ -63,6 +63,7 @@ APP_SYMBOLS = (
     "ipg_app_set_profile", "ipg_app_profile_reset", "ipg_app_launches", "ipg_app_profile", "ipg_app_main",
     "ipg_app_set_graph_loop", "ipg_app_graph_loop", "ipg_app_set_tuning", "ipg_app_get_tuning",
     "ipg_app_loop_add", "ipg_app_loop_prepare", "ipg_app_loop_collect", "ipg_app_set_param_ptr",
+    "ipg_app_set_order", "ipg_app_order",
 )
 
 
@@ -77,6 +78,10 @@ class _View(ctypes.Structure):
                 ("d_in_row", ctypes.c_void_p), ("d_in_adj", ctypes.c_void_p), ("d_in_wgt", ctypes.c_void_p),
                 ("max_out_degree", ctypes.c_uint64), ("max_in_degree", ctypes.c_uint64),
                 ("device_bytes", ctypes.c_uint64), ("symmetric", ctypes.c_int)]
+
+
+class _Order(ctypes.Structure):
+    _fields_ = [("graph", ctypes.c_void_p), ("d_old_of_new", ctypes.c_void_p), ("d_new_of_old", ctypes.c_void_p)]
 
 
 def build():
@@ -107,6 +112,7 @@ def runtime():
         L.ipg_graph_generate_er.argtypes = [u64, u64, u64, i32, ctypes.c_uint32, i32, ctypes.POINTER(vp)]
         L.ipg_graph_view_get.argtypes = [vp, ctypes.POINTER(_View)]
         L.ipg_graph_build_in.argtypes = [vp]
+        L.ipg_graph_degree_order.argtypes = [vp, i32, ctypes.POINTER(_Order)]
         L.ipg_graph_set_symmetric.argtypes = [vp, i32]
         L.ipg_graph_set_directed.argtypes = [vp, i32]
         L.ipg_graph_check_symmetric.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
@@ -271,6 +277,29 @@ class Graph:
 
     def refresh(self):
         _check(runtime().ipg_graph_view_get(self._h, ctypes.byref(self.view)), where="ipg_graph_view_get")
+
+    def degree_order(self, need_in=False) -> dict:
+        """The degree-ordered copy the engine runs on (ipg_graph_degree_order),
+        read back to the host: old_of_new, new_of_old, the copy's row / adj /
+        wgt and, when it has in-lists, in_row / in_adj."""
+        rt = runtime()
+        o = _Order()
+        _check(rt.ipg_graph_degree_order(self._h, int(need_in), ctypes.byref(o)), where="ipg_graph_degree_order")
+        V = self.V
+        view = _View()
+        _check(rt.ipg_graph_view_get(o.graph, ctypes.byref(view)), where="ipg_graph_view_get")
+        idt = np.uint32 if view.id_bytes == 4 else np.uint64
+        out = {"old_of_new": DeviceArray.wrap(o.d_old_of_new, V, np.uint32).to_host(),
+               "new_of_old": DeviceArray.wrap(o.d_new_of_old, V, np.uint32).to_host(),
+               "row": DeviceArray.wrap(view.d_row, V + 1, np.uint64).to_host(),
+               "adj": DeviceArray.wrap(view.d_adj, view.E, idt).to_host(),
+               "wgt": (DeviceArray.wrap(view.d_wgt, view.E, _WEIGHT_DTYPES[int(view.weight_bytes)]).to_host()
+                       if view.d_wgt else None),
+               "has_in": bool(view.has_in), "in_alias": bool(view.has_in and view.d_in_row == view.d_row)}
+        if view.has_in:
+            out["in_row"] = DeviceArray.wrap(view.d_in_row, V + 1, np.uint64).to_host()
+            out["in_adj"] = DeviceArray.wrap(view.d_in_adj, view.E, idt).to_host()
+        return out
 
     @classmethod
     def from_csr(cls, V, E, idx, adj, wgt=None, directed=False, need_in=False, id_bytes=4):
@@ -557,6 +586,16 @@ class Engine:
     def graph_loop(self) -> bool:
         return bool(self.lib.ipg_app_graph_loop())
 
+    def set_order(self, on=True):
+        """Run the kernels on the graph's degree-ordered copy (the default)
+        or on its own numbering; applied at the next attach.  Results are
+        the same either way."""
+        self._check(self.lib.ipg_app_set_order(int(on)), "ipg_app_set_order")
+
+    def order(self) -> bool:
+        """Whether the attached graph runs renamed."""
+        return bool(self.lib.ipg_app_order())
+
     def set_tuning(self, block=256, t0=16, t1=4096, pull_div=0):
         """CTA size, degree-class thresholds and pull switch of the superstep
         kernels; applied at the next attach."""
@@ -626,14 +665,18 @@ def _ptr(a):
 
 
 def run_app(app, version, graph: Graph, id_bits=32, params=None, generic=False, quiet=True,
-            graph_loop=None) -> RunResult:
+            graph_loop=None, order=None) -> RunResult:
     """Attach + set params + run, returning values and per-superstep counts.
     graph_loop: None keeps the library's mode (IPG_GRAPH_LOOP), True/False
-    selects the captured or the host-driven superstep loop."""
+    selects the captured or the host-driven superstep loop; order: None
+    keeps the library's mode, True/False runs on the degree-ordered copy or
+    on the graph's own numbering (both modes are library-wide and stay set)."""
     eng = Engine(app, version, id_bits, generic)
     eng.set_quiet(quiet)
     if graph_loop is not None:
         eng.set_graph_loop(graph_loop)
+    if order is not None:
+        eng.set_order(order)
     for k, v in (params or {}).items():
         eng.set_param(k, v)
     eng.attach(graph)

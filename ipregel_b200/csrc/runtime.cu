@@ -231,8 +231,30 @@ struct ipg_graph {
     // to run after it changed or while the contents are bad
     uint64_t generation = 0;
     bool bad = false;
+    // the degree-ordered copy (ipg_graph_degree_order) of the contents of
+    // generation ord_generation, its 4-byte id maps and its build scratch
+    ipg_graph* ord = nullptr;
+    void* ord_old_of_new = nullptr;
+    void* ord_new_of_old = nullptr;
+    uint64_t ord_map_bytes = 0;
+    void* ord_scratch = nullptr;
+    uint64_t ord_scratch_bytes = 0;
+    uint64_t ord_generation = 0;
+    bool ord_valid = false;
+    void drop_order()
+    {
+        delete ord;
+        ord = nullptr;
+        ipg_dev_free(ord_old_of_new, ord_map_bytes);
+        ipg_dev_free(ord_new_of_old, ord_map_bytes);
+        ipg_dev_free(ord_scratch, ord_scratch_bytes);
+        ord_old_of_new = ord_new_of_old = ord_scratch = nullptr;
+        ord_map_bytes = ord_scratch_bytes = 0;
+        ord_valid = false;
+    }
     ~ipg_graph()
     {
+        drop_order();
         ipg_dev_free(refill_dev, 64);
         ipg_dev_free(refill_stage, refill_stage_bytes);
         if (refill_host) cudaFreeHost(refill_host);
@@ -408,6 +430,174 @@ static int bits_for(uint64_t n)
     return b;
 }
 
+// ---- degree order ----
+// occ[v] = occurrences of v among the edges e = 0, s, 2s, ... of the rows (its
+// in-degree over the stored rows, sampled every s-th edge)
+template <class T>
+__global__ void k_occurrences(const T* __restrict__ adj, uint64_t E, uint64_t s, uint32_t* __restrict__ occ)
+{
+    const uint64_t n = (E + s - 1) / s;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&occ[(uint64_t)adj[i * s]], 1u);
+}
+
+// occ[v] = length of row v: the occurrences of v in the rows when every edge
+// has its reverse (symmetric rows), or its in-degree when row = the in-lists
+__global__ void k_occurrences_from_rows(const uint64_t* __restrict__ row, uint64_t V, uint32_t* __restrict__ occ)
+{
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t d = row[v + 1] - row[v];
+        occ[v] = d < 0xFFFFFFFFull ? (uint32_t)d : 0xFFFFFFFFu;
+    }
+}
+
+__global__ void k_invert_perm(const uint32_t* __restrict__ old_of_new, uint64_t V, uint32_t* __restrict__ new_of_old)
+{
+    for (uint64_t n = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; n < V; n += (uint64_t)gridDim.x * blockDim.x)
+        new_of_old[old_of_new[n]] = (uint32_t)n;
+}
+
+// deg[n] = length of row old_of_new[n], deg[V] = 0 (an exclusive scan makes the new rows)
+__global__ void k_perm_degrees(const uint64_t* __restrict__ row, const uint32_t* __restrict__ old_of_new, uint64_t V,
+                               uint64_t* __restrict__ deg)
+{
+    for (uint64_t n = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; n <= V; n += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t d = 0;
+        if (n < V) {
+            const uint64_t o = old_of_new[n];
+            d = row[o + 1] - row[o];
+        }
+        deg[n] = d;
+    }
+}
+
+// Row n of the copy = row old_of_new[n] of the source, in the same edge order,
+// each neighbour id renamed by new_of_old.  The copy's edges are cut into
+// tiles of ORD_TILE; tile_lo[t] is the row holding the tile's first edge.
+#define ORD_TILE 2048
+#define ORD_TILE_ROWS 2048
+#define ORD_PER_THREAD (ORD_TILE / 256) /* k_perm_rows runs 256 threads */
+
+__global__ void k_tile_rows(const uint64_t* __restrict__ nrow, uint64_t V, uint64_t tiles, uint32_t* __restrict__ tile_lo)
+{
+    for (uint64_t n = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; n < V; n += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t a = nrow[n], b = nrow[n + 1];
+        for (uint64_t t = (a + ORD_TILE - 1) / ORD_TILE; t * ORD_TILE < b; t++) tile_lo[t] = (uint32_t)n;
+        if (n == V - 1) tile_lo[tiles] = (uint32_t)n;
+    }
+}
+
+// A CTA per tile: the rows the tile touches staged in shared memory (copy
+// and source starts) with the row of every tile position (each non-empty
+// row marks its first position, a block-wide running max fills the rest);
+// reads follow the source rows, writes are coalesced.  A tile of more rows
+// than the stage holds (long runs of empty rows) searches the copy's row
+// starts instead.
+template <class T, class W>
+__global__ void __launch_bounds__(256) k_perm_rows(const uint64_t* __restrict__ row, const T* __restrict__ adj,
+                                                   const W* __restrict__ wgt, const uint32_t* __restrict__ old_of_new,
+                                                   const uint32_t* __restrict__ new_of_old, uint64_t E,
+                                                   const uint64_t* __restrict__ nrow,
+                                                   const uint32_t* __restrict__ tile_lo, T* __restrict__ nadj,
+                                                   W* __restrict__ nwgt)
+{
+    __shared__ uint64_t s_dst[ORD_TILE_ROWS + 1];
+    __shared__ uint64_t s_src[ORD_TILE_ROWS];
+    __shared__ uint16_t s_rowof[ORD_TILE];
+    __shared__ uint32_t s_warp[8];
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t tiles = (E + ORD_TILE - 1) / ORD_TILE;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t p0 = t * ORD_TILE, p1 = (p0 + ORD_TILE < E) ? p0 + ORD_TILE : E;
+        const uint64_t lo = tile_lo[t], cnt = (uint64_t)tile_lo[t + 1] - lo + 1;
+        const bool staged = cnt <= ORD_TILE_ROWS;
+        if (staged) {
+            for (uint64_t i = tid; i <= cnt; i += 256) {
+                s_dst[i] = nrow[lo + i];  // lo + cnt <= V: nrow holds V + 1 starts
+                if (i < cnt) s_src[i] = row[old_of_new[lo + i]];
+            }
+#pragma unroll
+            for (int j = 0; j < ORD_PER_THREAD; j++) s_rowof[tid * ORD_PER_THREAD + j] = 0;
+        }
+        __syncthreads();
+        if (staged) {
+            // row 0 holds p0; every later non-empty row starts inside (p0, p1]
+            for (uint64_t i = 1 + tid; i < cnt; i += 256) {
+                const uint64_t d = s_dst[i];
+                if (s_dst[i + 1] > d && d < p1) s_rowof[d - p0] = (uint16_t)i;
+            }
+        }
+        __syncthreads();
+        if (staged) {
+            // running max over the positions: ORD_PER_THREAD consecutive ones a thread
+            uint32_t m = 0, v[ORD_PER_THREAD];
+#pragma unroll
+            for (int j = 0; j < ORD_PER_THREAD; j++) {
+                const uint32_t x = s_rowof[tid * ORD_PER_THREAD + j];
+                m = x > m ? x : m;
+                v[j] = m;
+            }
+            uint32_t inc = m;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= (uint32_t)o) inc = y > inc ? y : inc;
+            }
+            if (lane == 31) s_warp[warp] = inc;
+            uint32_t before = __shfl_up_sync(0xffffffffu, inc, 1);
+            if (lane == 0) before = 0;
+            __syncthreads();
+            for (uint32_t w = 0; w < warp; w++) before = s_warp[w] > before ? s_warp[w] : before;
+#pragma unroll
+            for (int j = 0; j < ORD_PER_THREAD; j++)
+                s_rowof[tid * ORD_PER_THREAD + j] = (uint16_t)(v[j] > before ? v[j] : before);
+        }
+        __syncthreads();
+        // a thread's ORD_PER_THREAD edges: every source position first, then
+        // every load, then every store (independent loads in flight together)
+        uint64_t src[ORD_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < ORD_PER_THREAD; k++) {
+            const uint64_t p = p0 + tid + (uint64_t)k * 256;
+            src[k] = ~0ULL;
+            if (p < p1) {
+                if (staged) {
+                    const uint32_t a = s_rowof[p - p0];
+                    src[k] = s_src[a] + (p - s_dst[a]);
+                } else {
+                    // the last row of [lo, lo + cnt) with start <= p holds p
+                    uint64_t a = 0, b = cnt;
+                    while (b - a > 1) {
+                        const uint64_t m = (a + b) >> 1;
+                        if (nrow[lo + m] <= p) a = m;
+                        else b = m;
+                    }
+                    src[k] = row[old_of_new[lo + a]] + (p - nrow[lo + a]);
+                }
+            }
+        }
+        T u[ORD_PER_THREAD];
+        W w[ORD_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < ORD_PER_THREAD; k++) {
+            u[k] = src[k] != ~0ULL ? adj[src[k]] : (T)0;
+            w[k] = (wgt && src[k] != ~0ULL) ? wgt[src[k]] : (W)0;
+        }
+        uint32_t r[ORD_PER_THREAD];
+#pragma unroll
+        for (int k = 0; k < ORD_PER_THREAD; k++) r[k] = src[k] != ~0ULL ? new_of_old[(uint64_t)u[k]] : 0u;
+#pragma unroll
+        for (int k = 0; k < ORD_PER_THREAD; k++) {
+            const uint64_t p = p0 + tid + (uint64_t)k * 256;
+            if (src[k] != ~0ULL) {
+                nadj[p] = (T)r[k];
+                if (wgt) nwgt[p] = w[k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 extern "C" int ipg_graph_build_in(ipg_graph* g)
 {
     if (!g) return fail(IPG_EINVAL, "ipg_graph_build_in: null graph");
@@ -538,6 +728,177 @@ static int finalize(ipg_graph* g, int need_in, ipg_graph** out)
         return r;
     }
     *out = g;
+    return IPG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Degree-ordered copy
+// ---------------------------------------------------------------------------
+template <class T>
+static void launch_perm_rows(const uint64_t* row, const void* adj, const void* wgt, int weight_bytes,
+                             const uint32_t* old_of_new, const uint32_t* new_of_old, uint64_t E, const uint64_t* nrow,
+                             const uint32_t* tile_lo, void* nadj, void* nwgt, cudaStream_t st)
+{
+    const uint32_t grid = grid_for(E, ORD_TILE);
+    const T* a = (const T*)adj;
+    T* na = (T*)nadj;
+    switch (wgt ? weight_bytes : 0) {
+    case 1: k_perm_rows<<<grid, 256, 0, st>>>(row, a, (const uint8_t*)wgt, old_of_new, new_of_old, E, nrow, tile_lo, na, (uint8_t*)nwgt); break;
+    case 2: k_perm_rows<<<grid, 256, 0, st>>>(row, a, (const uint16_t*)wgt, old_of_new, new_of_old, E, nrow, tile_lo, na, (uint16_t*)nwgt); break;
+    case 4: k_perm_rows<<<grid, 256, 0, st>>>(row, a, (const uint32_t*)wgt, old_of_new, new_of_old, E, nrow, tile_lo, na, (uint32_t*)nwgt); break;
+    case 8: k_perm_rows<<<grid, 256, 0, st>>>(row, a, (const uint64_t*)wgt, old_of_new, new_of_old, E, nrow, tile_lo, na, (uint64_t*)nwgt); break;
+    default: k_perm_rows<<<grid, 256, 0, st>>>(row, a, (const uint8_t*)nullptr, old_of_new, new_of_old, E, nrow, tile_lo, na, (uint8_t*)nullptr); break;
+    }
+}
+
+// New rows (degree scan) and their edges, for the out- or the in-CSR.
+static int perm_csr(const ipg_graph* g, const uint64_t* row, const void* adj, const void* wgt, uint64_t* nrow,
+                    void* nadj, void* nwgt, const uint32_t* old_of_new, const uint32_t* new_of_old,
+                    uint64_t* deg, uint32_t* tile_lo, void* temp, size_t temp_bytes, cudaStream_t st)
+{
+    const uint64_t V = g->v.V, E = g->v.E;
+    k_perm_degrees<<<grid_for(V + 1, 256), 256, 0, st>>>(row, old_of_new, V, deg);
+    size_t tb = temp_bytes;
+    IPG_CUDA(cub::DeviceScan::ExclusiveSum(temp, tb, deg, nrow, (int)(V + 1), st));
+    if (E && V) {
+        const uint64_t tiles = (E + ORD_TILE - 1) / ORD_TILE;
+        k_tile_rows<<<grid_for(V, 256), 256, 0, st>>>(nrow, V, tiles, tile_lo);
+        if (g->v.id_bytes == 4)
+            launch_perm_rows<uint32_t>(row, adj, wgt, g->v.weight_bytes, old_of_new, new_of_old, E, nrow, tile_lo,
+                                       nadj, nwgt, st);
+        else
+            launch_perm_rows<uint64_t>(row, adj, wgt, g->v.weight_bytes, old_of_new, new_of_old, E, nrow, tile_lo,
+                                       nadj, nwgt, st);
+    }
+    IPG_CUDA(cudaGetLastError());
+    return IPG_OK;
+}
+
+static uint64_t align256(uint64_t x) { return (x + 255) & ~255ULL; }
+
+// Every s-th edge is counted for the order: 1 (every edge) unless
+// IPG_ORDER_SAMPLE sets s.  On undirected R-MAT scale 24 a sample of every
+// 8th edge took 1.2 instead of 5.3 ms, but ordered the many low-degree
+// vertices by noise and left CC + SSSP 6 % slower than exact counts.
+static uint64_t ord_sample_stride()
+{
+    const char* env = getenv("IPG_ORDER_SAMPLE");
+    const uint64_t s = (env && *env) ? strtoull(env, nullptr, 10) : 1;
+    return s ? s : 1;
+}
+
+extern "C" int ipg_graph_degree_order(ipg_graph* g, int need_in, ipg_order* out)
+{
+    if (!g || !out) return fail(IPG_EINVAL, "ipg_graph_degree_order: null argument");
+    memset(out, 0, sizeof *out);
+    if (g->bad) return fail(IPG_EINVAL, "the graph's contents failed validation at its last refill");
+    const uint64_t V = g->v.V, E = g->v.E;
+    if (V >= (1ULL << 31)) return fail(IPG_EINVAL, "ipg_graph_degree_order: supports fewer than 2^31 vertices");
+    if (need_in && !g->v.has_in) IPG_TRY(ipg_graph_build_in(g));
+    const bool with_in = g->v.has_in != 0;
+    const bool in_alias = with_in && g->v.d_in_row == g->v.d_row;
+    ipg_graph* o = g->ord;
+    const bool shape = o && o->v.V == V && o->v.E == E && o->v.id_bytes == g->v.id_bytes &&
+                       o->v.weight_bytes == g->v.weight_bytes && o->v.directed == g->v.directed &&
+                       (o->v.has_in != 0) == with_in && (with_in && o->v.d_in_row == o->v.d_row) == in_alias;
+    if (!(shape && g->ord_valid && g->ord_generation == g->generation)) {
+        const uint64_t deg_bytes = align256((V + 1) * 8), map_bytes = (V ? V : 1) * 4;
+        size_t sort_tb = 0, scan_tb = 0;
+        IPG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tb, (const uint32_t*)nullptr,
+                                                           (uint32_t*)nullptr, (const uint32_t*)nullptr,
+                                                           (uint32_t*)nullptr, (int)V, 0, 32, 0));
+        IPG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_tb, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                               (int)(V + 1), 0));
+        const uint64_t temp_bytes = align256(std::max(sort_tb, scan_tb) + 1);
+        const uint64_t tile_bytes = align256(((E + ORD_TILE - 1) / ORD_TILE + 1) * 4);
+        const uint64_t scratch_bytes = deg_bytes + 2 * align256(map_bytes) + temp_bytes + tile_bytes;
+        if (!shape || g->ord_scratch_bytes < scratch_bytes) {
+            g->drop_order();
+            o = new ipg_graph();
+            o->v.directed = g->v.directed;
+            int r = alloc_out(o, V, E, g->v.id_bytes, g->v.weight_bytes);
+            if (r == IPG_OK && with_in && !in_alias) {
+                o->in_row_bytes = (V + 1) * 8;
+                o->in_adj_bytes = (E ? E : 1) * (uint64_t)g->v.id_bytes;
+                r = ipg_dev_alloc(&o->in_row, o->in_row_bytes);
+                if (r == IPG_OK) r = ipg_dev_alloc(&o->in_adj, o->in_adj_bytes);
+                if (r == IPG_OK && g->v.d_in_wgt) {
+                    o->in_wgt_bytes = (E ? E : 1) * (uint64_t)g->v.weight_bytes;
+                    r = ipg_dev_alloc(&o->in_wgt, o->in_wgt_bytes);
+                }
+                o->v.device_bytes += o->in_row_bytes + o->in_adj_bytes + o->in_wgt_bytes;
+            }
+            g->ord = o;
+            g->ord_map_bytes = map_bytes;  // sizes first: drop_order frees what was allocated
+            g->ord_scratch_bytes = scratch_bytes;
+            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_old_of_new, map_bytes);
+            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_new_of_old, map_bytes);
+            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_scratch, scratch_bytes);
+            if (r != IPG_OK) {
+                g->drop_order();
+                return r;
+            }
+        } else {
+            for (auto& b : o->bins) {  // derived from the old contents
+                ipg_dev_free(b.lists, b.bytes);
+                b = ipg_graph::BinCache();
+            }
+        }
+        g->ord_valid = false;
+        cudaStream_t st = 0;
+        uint32_t* old_of_new = (uint32_t*)g->ord_old_of_new;
+        uint32_t* new_of_old = (uint32_t*)g->ord_new_of_old;
+        char* sc = (char*)g->ord_scratch;
+        uint64_t* deg = (uint64_t*)sc;  // the occurrence counts (u32) before the sort
+        uint32_t* occ_sorted = (uint32_t*)(sc + deg_bytes);
+        uint32_t* iota = (uint32_t*)(sc + deg_bytes + align256(map_bytes));
+        void* temp = sc + deg_bytes + 2 * align256(map_bytes);
+        uint32_t* tile_lo = (uint32_t*)(sc + deg_bytes + 2 * align256(map_bytes) + temp_bytes);
+        if (V) {
+            uint32_t* occ = (uint32_t*)deg;
+            const uint64_t s = ord_sample_stride();
+            if (s == 1 && g->v.symmetric) {
+                k_occurrences_from_rows<<<grid_for(V, 256), 256, 0, st>>>(g->v.d_row, V, occ);
+            } else if (s == 1 && with_in && !in_alias) {
+                k_occurrences_from_rows<<<grid_for(V, 256), 256, 0, st>>>(g->v.d_in_row, V, occ);
+            } else {
+                IPG_CUDA(cudaMemsetAsync(occ, 0, V * 4, st));
+                if (E && g->v.id_bytes == 4)
+                    k_occurrences<<<grid_for(E / s + 1, 256), 256, 0, st>>>((const uint32_t*)g->v.d_adj, E, s, occ);
+                else if (E)
+                    k_occurrences<<<grid_for(E / s + 1, 256), 256, 0, st>>>((const uint64_t*)g->v.d_adj, E, s, occ);
+            }
+            k_iota<<<grid_for(V, 256), 256, 0, st>>>(iota, V);
+            IPG_CUDA(cudaGetLastError());
+            // descending occurrences; the sort is stable, so ties keep ascending ids
+            size_t tb = temp_bytes;
+            const int end_bit = E + 1 >= (1ULL << 32) ? 32 : bits_for(E + 1);
+            IPG_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp, tb, occ, occ_sorted, iota, old_of_new, (int)V, 0,
+                                                               end_bit, st));
+            k_invert_perm<<<grid_for(V, 256), 256, 0, st>>>(old_of_new, V, new_of_old);
+            IPG_CUDA(cudaGetLastError());
+        }
+        IPG_TRY(perm_csr(g, g->v.d_row, g->v.d_adj, g->v.d_wgt, (uint64_t*)o->row, o->adj, o->wgt, old_of_new,
+                         new_of_old, deg, tile_lo, temp, temp_bytes, st));
+        if (with_in && !in_alias)
+            IPG_TRY(perm_csr(g, g->v.d_in_row, g->v.d_in_adj, g->v.d_in_wgt, (uint64_t*)o->in_row, o->in_adj,
+                             o->in_wgt, old_of_new, new_of_old, deg, tile_lo, temp, temp_bytes, st));
+        IPG_CUDA(cudaStreamSynchronize(st));
+        if (with_in) {
+            o->v.has_in = 1;
+            o->v.d_in_row = in_alias ? o->v.d_row : (const uint64_t*)o->in_row;
+            o->v.d_in_adj = in_alias ? o->v.d_adj : o->in_adj;
+            o->v.d_in_wgt = in_alias ? o->v.d_wgt : o->in_wgt;
+        }
+        o->v.max_out_degree = g->v.max_out_degree;  // a renaming keeps every degree
+        o->v.max_in_degree = g->v.max_in_degree;
+        g->ord_generation = g->generation;
+        g->ord_valid = true;
+    }
+    o->v.symmetric = g->v.symmetric;
+    out->graph = o;
+    out->d_old_of_new = (const uint32_t*)g->ord_old_of_new;
+    out->d_new_of_old = (const uint32_t*)g->ord_new_of_old;
     return IPG_OK;
 }
 
