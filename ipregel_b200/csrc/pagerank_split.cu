@@ -65,6 +65,11 @@ struct ipg_pr_plan {
     ipg_bins bins{};
     float* b[2] = {nullptr, nullptr};  // broadcast quotients, by superstep parity
     float* xs = nullptr;               // values of every other superstep
+    // on the graph's degree-ordered copy (ipg_graph_degree_order): the
+    // supersteps write xs / xs2 in the copy's numbering, and a last gather
+    // writes the values in the caller's (null: the graph's own numbering)
+    const uint32_t* new_of_old = nullptr;
+    float* xs2 = nullptr;
     uint32_t* hub_prefix = nullptr;    // first chunk of each hub, then the total
     uint32_t* hub_owner = nullptr;     // chunk -> index of its hub
     float2* partial = nullptr;         // (sum, compensation) of every hub chunk
@@ -252,6 +257,14 @@ __global__ void __launch_bounds__(PR_THREADS) k_pr_diag(const float* __restrict_
         if (x_prev) r += fabs(xv - (double)x_prev[v]);
     }
     pr_block_diag(m, d, r, diag);
+}
+
+// out[i] = x[new_of_old[i]]: the values in the caller's numbering.
+__global__ void k_pr_by_id(const float* __restrict__ x, const uint32_t* __restrict__ new_of_old, uint64_t V,
+                           float* __restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = x[new_of_old[i]];
 }
 
 // Class 0: a thread per vertex.
@@ -474,14 +487,31 @@ extern "C" int ipg_pr_plan_create(ipg_graph* g, ipg_pr_plan** out)
         const char* t1s = getenv("IPG_PR_T1");
         const uint64_t t0 = (t0s && *t0s) ? strtoull(t0s, nullptr, 10) : 16;
         const uint64_t t1 = (t1s && *t1s) ? strtoull(t1s, nullptr, 10) : 4096;
+        // the gathers run on the degree-ordered copy unless IPG_ORDER=0 (or
+        // the copy does not fit the HBM budget): the most gathered
+        // quotients share cache lines
+        ipg_graph* gw = g;
+        const char* ord = getenv("IPG_ORDER");
+        if (!(ord && *ord && strtoull(ord, nullptr, 10) == 0) && p->gv.V < (1ULL << 31)) {
+            ipg_order o;
+            const int ro = ipg_graph_degree_order(g, 1, &o);
+            if (ro == IPG_OK) {
+                gw = o.graph;
+                p->new_of_old = o.d_new_of_old;
+            } else if (ro != IPG_EBUDGET && ro != IPG_ENOMEM) {
+                r = ro;
+                break;
+            }
+        }
         // classes over the gather lists (builds the in-lists of a directed graph)
-        if ((r = ipg_graph_bins(g, 1, t0, t1, &p->bins)) != IPG_OK) break;
-        if ((r = ipg_graph_view_get(g, &p->gv)) != IPG_OK) break;
+        if ((r = ipg_graph_bins(gw, 1, t0, t1, &p->bins)) != IPG_OK) break;
+        if ((r = ipg_graph_view_get(gw, &p->gv)) != IPG_OK) break;
         p->grid = (uint32_t)p->sms * (uint32_t)pr_min_occupancy();
         const uint64_t V = p->gv.V, nh = p->bins.count[2];
         if ((r = pr_alloc(p, &p->b[0], V)) != IPG_OK) break;
         if ((r = pr_alloc(p, &p->b[1], V)) != IPG_OK) break;
         if ((r = pr_alloc(p, &p->xs, V)) != IPG_OK) break;
+        if (p->new_of_old && (r = pr_alloc(p, &p->xs2, V)) != IPG_OK) break;
         if ((r = pr_alloc(p, &p->hub_prefix, nh + 1)) != IPG_OK) break;
         std::vector<uint32_t> cnt(nh + 1, 0);
         if (nh) {
@@ -551,8 +581,10 @@ extern "C" int ipg_pr_run_f32(ipg_pr_plan* p, uint32_t rounds, double damping, i
     a.row = p->gv.d_row;
     a.in_row = p->gv.d_in_row;
     a.in_adj = (const uint32_t*)p->gv.d_in_adj;
-    // superstep s writes its values to xbuf(s), so that the last one lands in d_values
-    auto xbuf = [&](uint32_t s) { return ((rounds - s) & 1) ? p->xs : d_values; };
+    // superstep s writes its values to xbuf(s), so that the last one lands in
+    // d_values (on the renamed copy: in xs2, gathered into d_values at the end)
+    float* last = p->new_of_old ? p->xs2 : d_values;
+    auto xbuf = [&](uint32_t s) { return ((rounds - s) & 1) ? p->xs : last; };
     a.ratio = (float)((1.0 - damping) / (double)V);  // pagerank.c:98 (0.15 / V)
     a.damping = (float)damping;
     a.b_cur = nullptr;
@@ -571,6 +603,10 @@ extern "C" int ipg_pr_run_f32(ipg_pr_plan* p, uint32_t rounds, double damping, i
         else r = last ? pr_superstep<false, true>(p, a, st) : pr_superstep<false, false>(p, a, st);
         PR_TRY(r);
         k_pr_diag<<<p->grid, PR_THREADS, 0, st>>>(a.x_out, xbuf(s - 1), a.row, V, d_diag + (uint64_t)s * 3);
+        PR_CUDA(cudaGetLastError());
+    }
+    if (p->new_of_old) {
+        k_pr_by_id<<<p->grid, PR_THREADS, 0, st>>>(last, p->new_of_old, V, d_values);
         PR_CUDA(cudaGetLastError());
     }
     return IPG_OK;
