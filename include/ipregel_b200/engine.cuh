@@ -822,9 +822,12 @@ __device__ __forceinline__ void ipx_deliver(int p, uint64_t w, ipx_msg m)
 #ifndef IPX_PUSH_EXPAND
 #define IPX_PUSH_EXPAND 0
 #endif
-/* Lanes per source in the warp class of push and mark (8, 16 or 32). */
+/* Lanes per source in the warp class of push and mark (8, 16 or 32).  On
+ * the degree-ordered copy of undirected R-MAT scale 24 (most sources of the
+ * class have a few dozen out-edges), CC + SSSP ran at 63.7 - 63.9 GTEPS with
+ * 16, 62.0 with 8 and 61.5 - 61.6 with 32. */
 #ifndef IPX_PUSH_GROUP
-#define IPX_PUSH_GROUP 32
+#define IPX_PUSH_GROUP 16
 #endif
 /* Lanes per source in the thread class of push and mark (1, 2, 4 or 8). */
 #ifndef IPX_PUSH_Q
