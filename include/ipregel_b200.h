@@ -181,7 +181,9 @@ int ipg_graph_check_symmetric(const ipg_graph* g, int* result);
 /* The `directed` argument of ip_init (iPregel_preamble.h:298) for a graph
  * already resident: 0 makes the in-lists alias the rows (what the reference's
  * benchmarks load, pagerank.c:91), 1 makes them the transpose, built on the
- * next ipg_graph_build_in.  In-lists built for the other meaning are freed. */
+ * next ipg_graph_build_in.  In-lists built for the other meaning are freed,
+ * and a change bumps the contents generation (ipg_graph_contents): engines
+ * attached before must attach again. */
 int ipg_graph_set_directed(ipg_graph* g, int directed);
 /* Builds the in-CSR if it is missing (no-op for undirected graphs). */
 int ipg_graph_build_in(ipg_graph* g);
@@ -197,7 +199,9 @@ int ipg_graph_build_in(ipg_graph* g);
  * lists the same edges, in the same order, as row d_old_of_new[n] of g, so
  * a program reading neighbour ids reads g's row.  The copy and its maps are
  * cached on g and belong to it: a later call after a refill rebuilds them
- * in place (same size), ipg_graph_free frees them.  Needs V < 2^31. */
+ * in place (same size), one that asks for in-lists the copy lacks adds them
+ * in place, and ipg_graph_free frees them; after ipg_graph_set_directed
+ * changed the meaning the next call makes a new copy.  Needs V < 2^31. */
 typedef struct ipg_order {
     ipg_graph* graph;
     const uint32_t* d_old_of_new;

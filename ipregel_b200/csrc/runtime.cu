@@ -797,63 +797,79 @@ extern "C" int ipg_graph_degree_order(ipg_graph* g, int need_in, ipg_order* out)
     if (need_in && !g->v.has_in) IPG_TRY(ipg_graph_build_in(g));
     const bool with_in = g->v.has_in != 0;
     const bool in_alias = with_in && g->v.d_in_row == g->v.d_row;
+    // scratch: degrees (the occurrence counts before the sort), sorted
+    // counts, ids, the sort / scan temporaries, the tile rows of the copy
+    const uint64_t deg_bytes = align256((V + 1) * 8), map_bytes = (V ? V : 1) * 4;
+    size_t sort_tb = 0, scan_tb = 0;
+    IPG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tb, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                                       (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)V, 0, 32, 0));
+    IPG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_tb, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                           (int)(V + 1), 0));
+    const uint64_t temp_bytes = align256(std::max(sort_tb, scan_tb) + 1);
+    const uint64_t tile_bytes = align256(((E + ORD_TILE - 1) / ORD_TILE + 1) * 4);
+    const uint64_t scratch_bytes = deg_bytes + 2 * align256(map_bytes) + temp_bytes + tile_bytes;
+
+    // The copy is only ever dropped when the graph's shape or meaning
+    // changed (set_directed bumps the generation, so engines attached to it
+    // re-attach first); in-lists asked for later are added to it in place.
     ipg_graph* o = g->ord;
     const bool shape = o && o->v.V == V && o->v.E == E && o->v.id_bytes == g->v.id_bytes &&
                        o->v.weight_bytes == g->v.weight_bytes && o->v.directed == g->v.directed &&
-                       (o->v.has_in != 0) == with_in && (with_in && o->v.d_in_row == o->v.d_row) == in_alias;
-    if (!(shape && g->ord_valid && g->ord_generation == g->generation)) {
-        const uint64_t deg_bytes = align256((V + 1) * 8), map_bytes = (V ? V : 1) * 4;
-        size_t sort_tb = 0, scan_tb = 0;
-        IPG_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tb, (const uint32_t*)nullptr,
-                                                           (uint32_t*)nullptr, (const uint32_t*)nullptr,
-                                                           (uint32_t*)nullptr, (int)V, 0, 32, 0));
-        IPG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_tb, (const uint64_t*)nullptr, (uint64_t*)nullptr,
-                                               (int)(V + 1), 0));
-        const uint64_t temp_bytes = align256(std::max(sort_tb, scan_tb) + 1);
-        const uint64_t tile_bytes = align256(((E + ORD_TILE - 1) / ORD_TILE + 1) * 4);
-        const uint64_t scratch_bytes = deg_bytes + 2 * align256(map_bytes) + temp_bytes + tile_bytes;
-        if (!shape || g->ord_scratch_bytes < scratch_bytes) {
+                       g->ord_scratch_bytes >= scratch_bytes;
+    if (!shape) {
+        g->drop_order();
+        o = new ipg_graph();
+        o->v.directed = g->v.directed;
+        int r = alloc_out(o, V, E, g->v.id_bytes, g->v.weight_bytes);
+        g->ord = o;
+        g->ord_map_bytes = map_bytes;  // sizes first: drop_order frees what was allocated
+        g->ord_scratch_bytes = scratch_bytes;
+        if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_old_of_new, map_bytes);
+        if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_new_of_old, map_bytes);
+        if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_scratch, scratch_bytes);
+        if (r != IPG_OK) {
             g->drop_order();
-            o = new ipg_graph();
-            o->v.directed = g->v.directed;
-            int r = alloc_out(o, V, E, g->v.id_bytes, g->v.weight_bytes);
-            if (r == IPG_OK && with_in && !in_alias) {
-                o->in_row_bytes = (V + 1) * 8;
-                o->in_adj_bytes = (E ? E : 1) * (uint64_t)g->v.id_bytes;
-                r = ipg_dev_alloc(&o->in_row, o->in_row_bytes);
-                if (r == IPG_OK) r = ipg_dev_alloc(&o->in_adj, o->in_adj_bytes);
-                if (r == IPG_OK && g->v.d_in_wgt) {
-                    o->in_wgt_bytes = (E ? E : 1) * (uint64_t)g->v.weight_bytes;
-                    r = ipg_dev_alloc(&o->in_wgt, o->in_wgt_bytes);
-                }
-                o->v.device_bytes += o->in_row_bytes + o->in_adj_bytes + o->in_wgt_bytes;
-            }
-            g->ord = o;
-            g->ord_map_bytes = map_bytes;  // sizes first: drop_order frees what was allocated
-            g->ord_scratch_bytes = scratch_bytes;
-            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_old_of_new, map_bytes);
-            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_new_of_old, map_bytes);
-            if (r == IPG_OK) r = ipg_dev_alloc(&g->ord_scratch, scratch_bytes);
-            if (r != IPG_OK) {
-                g->drop_order();
-                return r;
-            }
-        } else {
-            for (auto& b : o->bins) {  // derived from the old contents
-                ipg_dev_free(b.lists, b.bytes);
-                b = ipg_graph::BinCache();
-            }
+            return r;
         }
+    }
+    if (with_in && !in_alias && !o->in_row) {
+        int r = IPG_OK;
+        o->in_row_bytes = (V + 1) * 8;
+        o->in_adj_bytes = (E ? E : 1) * (uint64_t)g->v.id_bytes;
+        r = ipg_dev_alloc(&o->in_row, o->in_row_bytes);
+        if (r == IPG_OK) r = ipg_dev_alloc(&o->in_adj, o->in_adj_bytes);
+        if (r == IPG_OK && g->v.d_in_wgt) {
+            o->in_wgt_bytes = (E ? E : 1) * (uint64_t)g->v.weight_bytes;
+            r = ipg_dev_alloc(&o->in_wgt, o->in_wgt_bytes);
+        }
+        if (r != IPG_OK) {  // the copy stays as it was, without in-lists
+            ipg_dev_free(o->in_row, o->in_row_bytes);
+            ipg_dev_free(o->in_adj, o->in_adj_bytes);
+            ipg_dev_free(o->in_wgt, o->in_wgt_bytes);
+            o->in_row = o->in_adj = o->in_wgt = nullptr;
+            o->in_row_bytes = o->in_adj_bytes = o->in_wgt_bytes = 0;
+            return r;
+        }
+        o->v.device_bytes += o->in_row_bytes + o->in_adj_bytes + o->in_wgt_bytes;
+    }
+    cudaStream_t st = 0;
+    uint32_t* old_of_new = (uint32_t*)g->ord_old_of_new;
+    uint32_t* new_of_old = (uint32_t*)g->ord_new_of_old;
+    char* sc = (char*)g->ord_scratch;
+    uint64_t* deg = (uint64_t*)sc;
+    uint32_t* occ_sorted = (uint32_t*)(sc + deg_bytes);
+    uint32_t* iota = (uint32_t*)(sc + deg_bytes + align256(map_bytes));
+    void* temp = sc + deg_bytes + 2 * align256(map_bytes);
+    uint32_t* tile_lo = (uint32_t*)(sc + deg_bytes + 2 * align256(map_bytes) + temp_bytes);
+    const bool fresh = g->ord_valid && g->ord_generation == g->generation;
+    const bool add_in = with_in && !o->v.has_in;
+    if (!fresh) {
         g->ord_valid = false;
-        cudaStream_t st = 0;
-        uint32_t* old_of_new = (uint32_t*)g->ord_old_of_new;
-        uint32_t* new_of_old = (uint32_t*)g->ord_new_of_old;
-        char* sc = (char*)g->ord_scratch;
-        uint64_t* deg = (uint64_t*)sc;  // the occurrence counts (u32) before the sort
-        uint32_t* occ_sorted = (uint32_t*)(sc + deg_bytes);
-        uint32_t* iota = (uint32_t*)(sc + deg_bytes + align256(map_bytes));
-        void* temp = sc + deg_bytes + 2 * align256(map_bytes);
-        uint32_t* tile_lo = (uint32_t*)(sc + deg_bytes + 2 * align256(map_bytes) + temp_bytes);
+        o->v.has_in = 0;  // rebuilt below with the rows
+        for (auto& b : o->bins) {  // derived from the old contents
+            ipg_dev_free(b.lists, b.bytes);
+            b = ipg_graph::BinCache();
+        }
         if (V) {
             uint32_t* occ = (uint32_t*)deg;
             const uint64_t s = ord_sample_stride();
@@ -880,22 +896,22 @@ extern "C" int ipg_graph_degree_order(ipg_graph* g, int need_in, ipg_order* out)
         }
         IPG_TRY(perm_csr(g, g->v.d_row, g->v.d_adj, g->v.d_wgt, (uint64_t*)o->row, o->adj, o->wgt, old_of_new,
                          new_of_old, deg, tile_lo, temp, temp_bytes, st));
-        if (with_in && !in_alias)
+    }
+    if ((!fresh || add_in) && with_in) {
+        if (!in_alias)
             IPG_TRY(perm_csr(g, g->v.d_in_row, g->v.d_in_adj, g->v.d_in_wgt, (uint64_t*)o->in_row, o->in_adj,
                              o->in_wgt, old_of_new, new_of_old, deg, tile_lo, temp, temp_bytes, st));
-        IPG_CUDA(cudaStreamSynchronize(st));
-        if (with_in) {
-            o->v.has_in = 1;
-            o->v.d_in_row = in_alias ? o->v.d_row : (const uint64_t*)o->in_row;
-            o->v.d_in_adj = in_alias ? o->v.d_adj : o->in_adj;
-            o->v.d_in_wgt = in_alias ? o->v.d_wgt : o->in_wgt;
-        }
-        o->v.max_out_degree = g->v.max_out_degree;  // a renaming keeps every degree
-        o->v.max_in_degree = g->v.max_in_degree;
-        g->ord_generation = g->generation;
-        g->ord_valid = true;
+        o->v.d_in_row = in_alias ? o->v.d_row : (const uint64_t*)o->in_row;
+        o->v.d_in_adj = in_alias ? o->v.d_adj : o->in_adj;
+        o->v.d_in_wgt = in_alias ? o->v.d_wgt : o->in_wgt;
     }
+    IPG_CUDA(cudaStreamSynchronize(st));
+    if (with_in) o->v.has_in = 1;
+    o->v.max_out_degree = g->v.max_out_degree;  // a renaming keeps every degree
+    o->v.max_in_degree = g->v.max_in_degree;
     o->v.symmetric = g->v.symmetric;
+    g->ord_generation = g->generation;
+    g->ord_valid = true;
     out->graph = o;
     out->d_old_of_new = (const uint32_t*)g->ord_old_of_new;
     out->d_new_of_old = (const uint32_t*)g->ord_new_of_old;
@@ -1619,6 +1635,7 @@ extern "C" int ipg_graph_set_directed(ipg_graph* g, int directed)
     g->v.d_in_wgt = nullptr;
     g->v.max_in_degree = directed ? 0 : g->v.max_out_degree;  // 0: unknown until ipg_graph_build_in
     g->v.directed = directed;
+    g->generation++;  // engines attached to the old meaning (and its in-lists) must attach again
     return IPG_OK;
 }
 

@@ -199,3 +199,55 @@ def test_degree_order_of_a_symmetric_graph():
     ties = k[:-1] == k[1:]
     assert np.all(o2n[:-1][ties] < o2n[1:][ties])
     assert c["in_alias"] or not c["has_in"]
+
+
+@pytest.mark.parametrize("undirected,directed", [(True, False), (False, True)])
+def test_copy_gains_in_lists_in_place(undirected, directed):
+    """A push program attached first (no in-lists), then a pull program on
+    the same graph: the copy gains in-lists without moving what the first
+    engine runs on, which still gives the oracle's labels."""
+    import ipregel_b200 as ip
+    g = O.gen_rmat(11, 16, seed=17, undirected=undirected)
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, directed=directed)
+    cc = ip.Engine("cc", "combiner")
+    pr = ip.Engine("pagerank", "single_broadcast")
+    try:
+        for e in (cc, pr):
+            e.set_quiet(True)
+            e.set_order(True)
+        pr.set_param("rounds", 10)
+        cc.attach(graph)
+        first = cc.run()
+        pr.attach(graph)
+        res_pr = pr.run()
+        again = cc.run()
+        want_cc, counts, _ = O.run(g, "cc", "combiner", directed=directed)
+        np.testing.assert_array_equal(again.values.astype(np.uint64), want_cc.astype(np.uint64))
+        np.testing.assert_array_equal(first.values, again.values)
+        assert again.counts == [int(c) for c in counts]
+        want_pr, _, _ = O.run(g, "pagerank", "single_broadcast", rounds=10, directed=directed)
+        assert np.max(np.abs(res_pr.values - want_pr)) <= PR_TOL
+    finally:
+        for e in (cc, pr):
+            e.set_order(ORDER_DEFAULT)
+        graph.free()
+
+
+def test_set_directed_makes_attached_engines_attach_again():
+    import ipregel_b200 as ip
+    g = O.gen_rmat(10, 16, seed=18, undirected=False)
+    graph = ip.Graph.from_csr(g.V, g.E, g.idx, g.adj, directed=False)
+    try:
+        eng = ip.Engine("cc", "spread")
+        eng.set_quiet(True)
+        eng.attach(graph)
+        eng.run()
+        graph.set_directed(True)
+        with pytest.raises(ip.IPregelError):
+            eng.run()
+        eng.attach(graph)
+        res = eng.run()
+        want, _, _ = O.run(g, "cc", "spread", directed=True)
+        np.testing.assert_array_equal(res.values.astype(np.uint64), want.astype(np.uint64))
+    finally:
+        graph.free()
