@@ -1225,7 +1225,7 @@ struct Group {
     uint32_t hchunks = 0;                 // hub chunks of list 2
     uint32_t appended = 0;                // sources appended since
     uint64_t wmask = 0;
-    int cc_lane = -1;  // label-propagation CC lane admitted in this round
+    int cc_lane = -1;  // label-propagation CC lane admitted in this admission pass
     // PPR
     float* b[2] = {nullptr, nullptr};
     float2* partial = nullptr;
@@ -1513,7 +1513,7 @@ void admit(ipg_server* S, Group* G, double now)
     const uint64_t full = K == 64 ? ~0ULL : ((1ULL << K) - 1);
     G->cc_lane = -1;
     bool rebuild = false;
-    void* cc_first = nullptr;  // result of this round's union-find pass
+    void* cc_first = nullptr;  // result of this admission pass's union-find run
     for (auto it = queue.begin(); it != queue.end();) {
         Query& q = S->queries[*it];
         const bool union_find = q.kind == IPG_QUERY_CC && G->G->gv.symmetric;
